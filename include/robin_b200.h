@@ -1,0 +1,172 @@
+/*
+ * robin_b200.h -- C-ABI of the B200 hierarchical Poincare-Steklov (HPS) factor/solve.
+ *
+ * Drop-in boundary for robinsolver's hot path.  Every entry point takes plain
+ * pointers and sizes; complex numbers are interleaved (re, im) double pairs, the
+ * layout of C99 `double _Complex` and Fortran `complex(c_double_complex)`.
+ * Arrays handed in by the caller are read before the call returns (host arrays)
+ * or are device arrays the caller keeps alive until the call returns.
+ *
+ * The reference's callbacks (elliptic_operator%k, elliptic_rhs%f, bndry_rhs%g_face)
+ * are evaluated by the caller on the host at points this library reports
+ * (rb_tree_sample_points); the library never calls back into user code.
+ *
+ * Status codes: 0 on success, a negative RB_ERR_* value on failure; the message of
+ * the last failure on a handle is returned by rb_last_error(handle), and
+ * rb_last_error(NULL) reports the last failure of rb_tree_create on this thread.
+ * The reference stops the process instead ("stop '<message>'"); the messages below
+ * carry the reference's wording where one exists.
+ *
+ * Threading: one host thread at a time per handle.  Different handles are
+ * independent.  All device work of a handle runs on the handle's CUDA stream.
+ */
+#ifndef ROBIN_B200_H
+#define ROBIN_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------------------------------- */
+#define RB_OK                  0
+#define RB_ERR_INVALID        -1  /* bad argument (null pointer, size, index)                        */
+#define RB_ERR_DOMAIN         -2  /* "Invalid operator domain format." / "Dimension must be 2 or 3."  */
+#define RB_ERR_BNDRY_PARAMS   -3  /* "Boundary parameter matrix is nearly singular."                  */
+#define RB_ERR_NOT_FACTORED   -4  /* "Robin Tree must be factored first."                            */
+#define RB_ERR_DIM_MISMATCH   -5  /* "Dimensions of Robin Tree and RHS do not match."                */
+#define RB_ERR_GEOMETRY       -6  /* "Interface sizes of node children do not match." (non-uniform)   */
+#define RB_ERR_UNSUPPORTED    -7  /* a valid request this build does not implement (d = 3, ...)       */
+#define RB_ERR_CUDA           -8  /* CUDA runtime failure (message carries cudaGetErrorString)        */
+#define RB_ERR_OUT_OF_MEMORY  -9  /* device allocation refused or over the handle's byte budget       */
+#define RB_ERR_NUMERIC       -10  /* zero pivot / non-finite value met during the factorization       */
+#define RB_ERR_NO_SOLUTION   -11  /* get_solution before any solve, or irhs out of range              */
+
+/* ---- precision modes for rb_tree_factor ----------------------------------------------------- */
+#define RB_PREC_FP64  0           /* every operation in complex128                                    */
+#define RB_PREC_MIXED 1           /* reserved: split-BF16 lower levels + FP64 refinement              */
+
+/* ---- sample-point kinds for rb_tree_sample_points ------------------------------------------- */
+#define RB_POINTS_POTENTIAL 0     /* interior cell centres where elliptic_operator%k is sampled       */
+#define RB_POINTS_SOURCE    1     /* interior cell centres where elliptic_rhs%f is sampled            */
+#define RB_POINTS_BOUNDARY  2     /* face-local coordinates where bndry_rhs%g_face is sampled         */
+#define RB_POINTS_SOLUTION  3     /* every point of every leaf's u vector (check_solution's points)   */
+
+/* ---- flags in rb_geom.flags ----------------------------------------------------------------- */
+#define RB_FLAG_SKIP_ROOT_RTR 1   /* do not form the root's own RtR (the solve never reads it)         */
+#define RB_FLAG_VERBOSE       2   /* print the reference's progress lines to stdout                   */
+
+typedef struct rb_tree rb_tree;
+
+/* Problem geometry and options: type(elliptic_operator) (derived_type_module.f90:72-84),
+ * type(solve_opts) (derived_type_module.f90:309-320), robin_tree%bndry_params
+ * (robin_tree_module.f90:61) and the level count L of robin_tree%factor. */
+typedef struct rb_geom {
+    int32_t d;                 /* elliptic_operator%d; 2 (3 returns RB_ERR_UNSUPPORTED)             */
+    int32_t L;                 /* tree levels; leaves sit at level L                                */
+    double  domain[6];         /* elliptic_operator%domain(1:2,1:3), Fortran column-major:
+                                  [x_lo, x_hi, y_lo, y_hi, z_lo, z_hi]                              */
+    double  h_tgt;             /* solve_opts%h_tgt                                                  */
+    double  kb;                /* solve_opts%kb: FD boundary row is u_n + i*kb*u                    */
+    double  bndry_params[8];   /* robin_tree%bndry_params(1:2,1:2), complex, column-major,
+                                  interleaved: [re11, im11, re21, im21, re12, im12, re22, im22]     */
+    int32_t ordering;          /* solve_opts%ordering; only 1 is defined by the reference           */
+    int32_t flags;             /* RB_FLAG_*                                                         */
+    int64_t device_budget;     /* bytes of device memory the handle may hold; 0 = no limit          */
+} rb_geom;
+
+/* Sizes of a created tree. */
+typedef struct rb_info {
+    int32_t nleaves;           /* 2^L                                                               */
+    int32_t leaf_a, leaf_b;    /* leaf grid (ptbox) in x and y                                      */
+    int32_t leaf_n;            /* unknowns per leaf = 2(a+b) + a*b, the length of leaf_solution%u   */
+    int32_t leaf_nb;           /* boundary points per leaf = 2(a+b)                                 */
+    int32_t root_nb;           /* boundary points of the whole domain (length of one g_faces RHS)   */
+    int64_t n_interior;        /* nleaves * a * b: length of one potential or source sample array   */
+    int64_t device_bytes;      /* device memory currently held by the handle                        */
+    int32_t factored;          /* robin_tree%factored                                               */
+    int32_t nrhs;              /* right-hand sides held from the last solve                         */
+} rb_info;
+
+/* Builds the tree (robin_tree_factor's setup and bin_tree, robin_tree_module.f90:114-159):
+ * validates domain, dimension and det(bndry_params) >= 1e-3, bisects L times, sizes the leaf
+ * grids (get_h, fd_module.f90:1060-1084) and allocates device memory.  No factorization yet. */
+int rb_tree_create(const rb_geom* geom, rb_tree** out);
+
+/* Releases the handle and all its device memory. */
+int rb_tree_destroy(rb_tree* tree);
+
+/* Message of the last failure on `tree` (or of rb_tree_create on this thread when NULL). */
+const char* rb_last_error(const rb_tree* tree);
+
+int rb_tree_info(const rb_tree* tree, rb_info* info);
+
+/* Coordinates (x, y, z triples) at which the caller evaluates its callbacks, in the order the
+ * corresponding sample arrays must use:
+ *  RB_POINTS_POTENTIAL: nleaves*a*b points, leaves in DFS order (child1 first), each leaf's
+ *                       interior cell centres x-fastest; each leaf uses its own h, as
+ *                       FD_matrix_row does (fd_module.f90:134-145).
+ *  RB_POINTS_SOURCE:    the same points computed with robin_tree%opts%h as it stands after the
+ *                       factorization (the last leaf's h), as fd_leaf_solve does
+ *                       (fd_module.f90:427-431).
+ *  RB_POINTS_BOUNDARY:  root_nb face-local coordinates, faces x1 x2 y1 y2 in turn, each face in
+ *                       ascending order: the concatenation apply_bc builds at the root
+ *                       (robin_tree_module.f90:1186-1237) of fd_make_bndry_vec's points
+ *                       (fd_module.f90:636-651).  x-faces carry (y, 0, 0), y-faces (x, 0, 0).
+ *                       The face a point belongs to follows from its index.
+ *  RB_POINTS_SOLUTION:  nleaves*leaf_n points of proc2vec (robin_output_module.f90:258-265).
+ * `xyz` holds 3 doubles per point.  Requires the tree to be created (not factored). */
+int rb_tree_sample_points(const rb_tree* tree, int which, double* xyz);
+
+/* robin_tree%factor(L, op, opts) (robin_tree_module.f90:96-185) with the potential already
+ * sampled: `k_centres` = nleaves*a*b complex values at RB_POINTS_POTENTIAL (host memory).
+ * Blocks until the factorization is done; robin_tree%f_time is set from device events. */
+int rb_tree_factor(rb_tree* tree, const double* k_centres, int precision);
+
+/* As rb_tree_factor, with `d_k_centres` already in device memory.  Asynchronous on the
+ * handle's stream when `sync` is 0. */
+int rb_tree_factor_device(rb_tree* tree, const double* d_k_centres, int precision, int sync);
+
+/* robin_tree%solve(rhs) (robin_tree_module.f90:198-233) for `nrhs` right-hand sides at once:
+ *  f_centres: nrhs * nleaves*a*b complex, RHS-major, each at RB_POINTS_SOURCE;
+ *  g_faces:   nrhs * root_nb complex, RHS-major, each at RB_POINTS_BOUNDARY.
+ * Every call applies its own boundary data (the reference applies boundary data only on the
+ * first solve of a process, robin_tree_module.f90:1014-1029).  Blocks until done; sets
+ * robin_tree%s_time. */
+int rb_tree_solve(rb_tree* tree, int nrhs, const double* f_centres, const double* g_faces);
+
+/* As rb_tree_solve with device arrays; asynchronous on the handle's stream when `sync` is 0. */
+int rb_tree_solve_device(rb_tree* tree, int nrhs, const double* d_f_centres,
+                         const double* d_g_faces, int sync);
+
+/* get_solution(T, u) (robin_output_module.f90:48-75) for right-hand side `irhs`:
+ *  u:     nleaves * leaf_n complex (host), leaves in DFS order, each in lin2fgrid order;
+ *  boxes: nleaves * 6 doubles (host, may be NULL), each leaf's box(1:2,1:3) column-major. */
+int rb_get_solution(const rb_tree* tree, int irhs, double* u, double* boxes);
+
+/* All right-hand sides' solutions into device memory: nrhs * nleaves * leaf_n complex,
+ * RHS-major.  Asynchronous on the handle's stream when `sync` is 0. */
+int rb_get_solution_device(const rb_tree* tree, double* d_u, int sync);
+
+/* robin_tree%f_time and robin_tree%s_time in seconds (device-event timing). */
+int rb_tree_times(const rb_tree* tree, double* f_time, double* s_time);
+
+/* The handle's CUDA stream (a cudaStream_t), for callers that order their own work with it. */
+void* rb_tree_stream(const rb_tree* tree);
+
+/* Per-stage device times (milliseconds) of the last factor and solve, when stage timing was
+ * enabled with rb_tree_set_timing(tree, 1).  Writes min(n, count) values and returns the count;
+ * names[i] (may be NULL) receives a static string per stage. */
+int rb_tree_set_timing(rb_tree* tree, int enable);
+int rb_tree_stage_times(const rb_tree* tree, double* ms, const char** names, int n);
+
+/* Number of this library's kernels launched by the last factor and the last solve. */
+int rb_tree_launch_counts(const rb_tree* tree, int64_t* factor_launches, int64_t* solve_launches);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ROBIN_B200_H */

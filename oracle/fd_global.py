@@ -1,0 +1,141 @@
+"""Oracle: independent global sparse FD system behind robinsolver's HPS factor/solve.
+
+TEST INFRASTRUCTURE ONLY (same import rule as ``hps_ref.py``).
+
+The HPS tree of the reference eliminates, leaf by leaf and merge by merge, one
+global finite-difference system.  This module writes that system out directly:
+
+* unknowns: every leaf's cornerless grid (its ``u`` vector in lin2fgrid order,
+  fd_module.f90:867-939), leaves in DFS order.  Interface points appear once per
+  adjacent leaf, as in the reference;
+* per leaf: the interior PDE rows of FD_matrix_row (fd_module.f90:140-181);
+* boundary rows on the domain boundary: the Robin row i*kb*u + u_n = g
+  (fd_module.f90:187-216);
+* boundary rows on an interface: the transmission conditions the merge solves
+  (robin_tree_module.f90:425-467 with ``apply_invm`` :1252-1322):
+  h1 = zeta*g1 + nu*g2 and h2 = nu*g1 + zeta*g2, where g is a leaf's incoming
+  data (its own Robin row) and h = -i*kb*u + u_n its outgoing data
+  (RTR_update, robin_tree_module.f90:683-713).
+
+``solve`` factors it with SuperLU (``scipy.sparse.linalg.spsolve``); ``residual``
+applies it to a candidate solution, which checks a full-size result without
+running the HPS restatement.
+"""
+from __future__ import annotations
+
+import numpy as np
+import scipy.sparse as sp
+import scipy.sparse.linalg as spla
+
+from . import hps_ref as H
+
+
+def _leaf_rows(a, b, h, kb):
+    """COO triplets of one leaf matrix without the potential (structure + constants),
+    the diagonal increments of the interior rows, and the outgoing rows R."""
+    A0 = H.fd_matrix(a, b, h, np.zeros(a * b, dtype=np.complex128), kb)
+    nb = 2 * (a + b)
+    n = A0.shape[0]
+    R = H.outgoing_rows(np.eye(n, dtype=np.complex128), a, b, h, kb)   # nb x n
+    return A0, R, nb, n
+
+
+class GlobalFD:
+    """Assemble the global system for a tree geometry (from ``hps_ref.build_tree``)."""
+
+    def __init__(self, L, domain, h_tgt, kb, bndry_params, kfun):
+        self.root, self.levels = H.build_tree(L, np.asarray(domain, dtype=np.float64), 2)
+        leaves = self.levels[-1]
+        self.leaves = leaves
+        h, grid = H.get_h(h_tgt, leaves[0].box, 2)
+        a, b = grid[0], grid[1]
+        for lf in leaves:
+            h2, g2 = H.get_h(h_tgt, lf.box, 2)
+            if g2[:2] != grid[:2]:
+                raise ValueError("non-uniform leaf grids")
+        self.a, self.b, self.h, self.kb = a, b, h, kb
+        bp = np.asarray(bndry_params, dtype=np.complex128)
+        nu = (-bp[0, 0] * bp[1, 1] + bp[0, 1] * bp[1, 0]) / (2 * bp[0, 0] * bp[0, 1])
+        zeta = (bp[0, 0] * bp[1, 1] + bp[0, 1] * bp[1, 0]) / (2 * bp[0, 0] * bp[0, 1])
+        A0, R, nb, n = _leaf_rows(a, b, h, kb)
+        self.nb, self.n = nb, n
+        nl = len(leaves)
+        # leaf positions on the regular leaf lattice
+        w = leaves[0].box[1] - leaves[0].box[0]
+        lo = self.root.box[0]
+        pos = {}
+        where = {}
+        for li, lf in enumerate(leaves):
+            ix = int(round((lf.box[0, 0] - lo[0]) / w[0]))
+            iy = int(round((lf.box[0, 1] - lo[1]) / w[1]))
+            pos[(ix, iy)] = li
+            where[li] = (ix, iy)
+        self.pos = pos
+        pf = H.get_pt_face((a, b))
+        off = H.face_offsets(pf)
+        A0c = sp.coo_matrix(A0)
+        Rc = sp.csr_matrix(R)
+        rows, cols, vals = [], [], []
+        diag_rows = []
+        kval = []
+        for li, lf in enumerate(leaves):
+            base = li * n
+            pts = H.interior_points(a, b, h, lf.box)
+            kval.append(np.asarray(kfun(pts), dtype=np.complex128))
+            # interior rows + boundary Robin rows (interface rows replaced below)
+            keep = A0c.row >= nb
+            rows.append(base + A0c.row[keep]); cols.append(base + A0c.col[keep]); vals.append(A0c.data[keep])
+            diag_rows.append(base + np.arange(nb, n))
+            ix, iy = where[li]
+            for f in range(1, 5):
+                rr = np.arange(off[f - 1], off[f - 1] + pf[f - 1])
+                nbr = {1: (ix - 1, iy), 2: (ix + 1, iy), 3: (ix, iy - 1), 4: (ix, iy + 1)}[f]
+                if nbr not in pos:
+                    sub = sp.coo_matrix(A0[rr])
+                    rows.append(base + rr[sub.row]); cols.append(base + sub.col); vals.append(sub.data)
+                    continue
+                lj = pos[nbr]
+                fo = {1: 2, 2: 1, 3: 4, 4: 3}[f]
+                rn = np.arange(off[fo - 1], off[fo - 1] + pf[fo - 1])
+                # row for (leaf li, face f point p): its own h1 equation
+                #   h_li(p) - zeta*g_li(p) - nu*g_lj(p') = 0
+                for t in range(len(rr)):
+                    r_own, r_nb = rr[t], rn[t]
+                    ro = Rc.getrow(r_own).tocoo()
+                    go = sp.coo_matrix(A0[r_own:r_own + 1])
+                    gn = sp.coo_matrix(A0[r_nb:r_nb + 1])
+                    rows.append(np.full(ro.nnz, base + r_own)); cols.append(base + ro.col); vals.append(ro.data)
+                    rows.append(np.full(go.nnz, base + r_own)); cols.append(base + go.col); vals.append(-zeta * go.data)
+                    rows.append(np.full(gn.nnz, base + r_own)); cols.append(lj * n + gn.col); vals.append(-nu * gn.data)
+        rows = np.concatenate(rows); cols = np.concatenate(cols); vals = np.concatenate(vals)
+        diag_rows = np.concatenate(diag_rows)
+        kval = np.concatenate(kval)
+        rows = np.concatenate([rows, diag_rows]); cols = np.concatenate([cols, diag_rows]); vals = np.concatenate([vals, kval])
+        N = nl * n
+        self.A = sp.csc_matrix((vals, (rows, cols)), shape=(N, N))
+
+    def rhs(self, f, gfaces):
+        """Right-hand side for source ``f`` and face data ``gfaces`` (4 callbacks)."""
+        a, b, h, nb, n = self.a, self.b, self.h, self.nb, self.n
+        pf = H.get_pt_face((a, b))
+        off = H.face_offsets(pf)
+        out = np.zeros(len(self.leaves) * n, dtype=np.complex128)
+        for li, lf in enumerate(self.leaves):
+            base = li * n
+            out[base + nb:base + n] = f(H.interior_points(a, b, h, lf.box))
+            for fc in range(1, 5):
+                if lf.isbndry[fc - 1]:
+                    pts = H.face_points(a, b, h, lf.box, fc)
+                    out[base + off[fc - 1]:base + off[fc - 1] + pf[fc - 1]] = gfaces[fc - 1](pts)
+        return out
+
+    def solve(self, f, gfaces):
+        """Global solution, split per leaf (DFS order) like get_solution."""
+        x = spla.spsolve(self.A, self.rhs(f, gfaces))
+        return x.reshape(len(self.leaves), self.n)
+
+    def residual(self, u_leaves, f, gfaces):
+        """max|A u - b| / max|b| for a per-leaf solution array (nleaves, n)."""
+        b = self.rhs(f, gfaces)
+        r = self.A @ np.asarray(u_leaves).reshape(-1) - b
+        return float(np.max(np.abs(r)) / max(np.max(np.abs(b)), 1e-300))
