@@ -84,6 +84,8 @@ typedef struct rb_info {
     int32_t leaf_n;            /* unknowns per leaf = 2(a+b) + a*b, the length of leaf_solution%u   */
     int32_t leaf_nb;           /* boundary points per leaf = 2(a+b)                                 */
     int32_t root_nb;           /* boundary points of the whole domain (length of one g_faces RHS)   */
+    int32_t root_a, root_b;    /* grid of the whole domain in x and y: root_nb = 2(root_a + root_b)  */
+    double  h_last[3];         /* robin_tree%opts%h after the factorization (the last leaf's h)     */
     int64_t n_interior;        /* nleaves * a * b: length of one potential or source sample array   */
     int64_t device_bytes;      /* device memory currently held by the handle                        */
     int32_t factored;          /* robin_tree%factored                                               */
@@ -91,8 +93,10 @@ typedef struct rb_info {
 } rb_info;
 
 /* Builds the tree (robin_tree_factor's setup and bin_tree, robin_tree_module.f90:114-159):
- * validates domain, dimension and det(bndry_params) >= 1e-3, bisects L times, sizes the leaf
- * grids (get_h, fd_module.f90:1060-1084) and allocates device memory.  No factorization yet. */
+ * validates domain, dimension and det(bndry_params) >= 1e-3, bisects L times and sizes the leaf
+ * grids (get_h, fd_module.f90:1060-1084).  Host work only: device memory is allocated by the
+ * first factorization.  With geom->device_budget > 0 a tree whose factorization storage cannot
+ * fit the budget is refused here with RB_ERR_OUT_OF_MEMORY. */
 int rb_tree_create(const rb_geom* geom, rb_tree** out);
 
 /* Releases the handle and all its device memory. */
@@ -156,11 +160,27 @@ int rb_tree_times(const rb_tree* tree, double* f_time, double* s_time);
 /* The handle's CUDA stream (a cudaStream_t), for callers that order their own work with it. */
 void* rb_tree_stream(const rb_tree* tree);
 
-/* Per-stage device times (milliseconds) of the last factor and solve, when stage timing was
- * enabled with rb_tree_set_timing(tree, 1).  Writes min(n, count) values and returns the count;
- * names[i] (may be NULL) receives a static string per stage. */
-int rb_tree_set_timing(rb_tree* tree, int enable);
-int rb_tree_stage_times(const rb_tree* tree, double* ms, const char** names, int n);
+/* Device-event timing.  mode 0: off.  mode 1: per stage (leaf stage, each merge level, forward,
+ * backward, leaf recovery) of the last factor and solve.  mode 2: one entry per kernel launch
+ * (a whole Gauss-Jordan batch counts as one), accumulated over calls until
+ * rb_tree_clear_stage_times, with each entry's algorithmic flop count (8mnk for a complex GEMM,
+ * 8m^3 per Gauss-Jordan inverse, 0 for data-movement kernels).  rb_tree_stage_times writes
+ * min(n, count) entries (any output pointer may be NULL) and returns the count; names point to
+ * strings owned by the handle.  Entries are complete after the handle's stream is synchronized. */
+int rb_tree_set_timing(rb_tree* tree, int mode);
+int rb_tree_stage_times(const rb_tree* tree, double* ms, double* flops, const char** names, int n);
+int rb_tree_clear_stage_times(rb_tree* tree);
+
+/* Shape of level `level` (0 = root, L = leaves): shape[0] = nodes, shape[1], shape[2] = the grid
+ * (ptbox) of each node in x and y (robin_tree_module.f90:404-407 for merged nodes). */
+int rb_tree_level_shape(const rb_tree* tree, int level, int32_t* shape);
+
+/* Robin-to-Robin matrix of node `node` (0-based, left to right; leaves in DFS order) of level
+ * `level` (0 = root, L = leaves) after the factorization, into `out`: nb x nb complex,
+ * column-major, rows/columns in face order x1 x2 y1 y2 -- the blocks node%RtR(row,col)
+ * (robin_tree_module.f90:782-793 for leaves, :538-615 for merges) assembled into one matrix.
+ * RB_ERR_INVALID for the root when RB_FLAG_SKIP_ROOT_RTR is set. */
+int rb_tree_get_rtr(const rb_tree* tree, int level, int node, double* out);
 
 /* Number of this library's kernels launched by the last factor and the last solve. */
 int rb_tree_launch_counts(const rb_tree* tree, int64_t* factor_launches, int64_t* solve_launches);

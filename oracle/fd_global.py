@@ -139,3 +139,67 @@ class GlobalFD:
         b = self.rhs(f, gfaces)
         r = self.A @ np.asarray(u_leaves).reshape(-1) - b
         return float(np.max(np.abs(r)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def backward_error(L, domain, h_tgt, kb, bndry_params, kvals, U, F, G):
+    """Normwise backward error of a candidate solution of the global FD system, vectorised over
+    leaves so that it runs at the full benchmark sizes:
+
+        eta = max|A u - b| / (||A||_inf * max|u| + max|b|)
+
+    kvals, F: (nleaves, a*b) potential and source samples (leaf DFS order, x fastest);
+    U: (nleaves, n) solution in get_solution order; G: (root_nb,) boundary data in the root's
+    face order (faces x1 x2 y1 y2, each ascending).  The rows are the ones ``GlobalFD``
+    assembles: leaf PDE rows, Robin rows on the domain boundary, transmission rows
+    h1 - zeta*g1 - nu*g2 = 0 on every interface point."""
+    root, levels = H.build_tree(L, np.asarray(domain, dtype=np.float64), 2)
+    leaves = levels[-1]
+    h, grid = H.get_h(h_tgt, leaves[0].box, 2)
+    a, b = grid[0], grid[1]
+    nb = 2 * (a + b)
+    n = nb + a * b
+    bp = np.asarray(bndry_params, dtype=np.complex128)
+    nu = (-bp[0, 0] * bp[1, 1] + bp[0, 1] * bp[1, 0]) / (2 * bp[0, 0] * bp[0, 1])
+    zeta = (bp[0, 0] * bp[1, 1] + bp[0, 1] * bp[1, 0]) / (2 * bp[0, 0] * bp[0, 1])
+    A0 = sp.csr_matrix(H.fd_matrix(a, b, h, np.zeros(a * b, dtype=np.complex128), kb))
+    R = sp.csr_matrix(H.outgoing_rows(np.eye(n, dtype=np.complex128), a, b, h, kb))
+    U = np.asarray(U, dtype=np.complex128)
+    kvals = np.asarray(kvals, dtype=np.complex128).reshape(len(leaves), a * b)
+    F = np.asarray(F, dtype=np.complex128).reshape(len(leaves), a * b)
+    G = np.asarray(G, dtype=np.complex128).reshape(-1)
+    AU = np.asarray((A0 @ U.T).T)
+    AU[:, nb:] += kvals * U[:, nb:]
+    hout = np.asarray((R @ U.T).T)
+    gin = AU[:, :nb]
+    res = np.zeros_like(AU)
+    res[:, nb:] = AU[:, nb:] - F
+    pf = H.get_pt_face((a, b))
+    off = H.face_offsets(pf)
+    w = leaves[0].box[1] - leaves[0].box[0]
+    lo = root.box[0]
+    ix = np.array([int(round((lf.box[0, 0] - lo[0]) / w[0])) for lf in leaves])
+    iy = np.array([int(round((lf.box[0, 1] - lo[1]) / w[1])) for lf in leaves])
+    nx, ny = ix.max() + 1, iy.max() + 1
+    at = -np.ones((nx, ny), dtype=np.int64)
+    at[ix, iy] = np.arange(len(leaves))
+    rootpf = [ny * b, ny * b, nx * a, nx * a]
+    rootoff = H.face_offsets(rootpf)
+    for f in range(1, 5):
+        sl = slice(off[f - 1], off[f - 1] + pf[f - 1])
+        fo = {1: 2, 2: 1, 3: 4, 4: 3}[f]
+        so = slice(off[fo - 1], off[fo - 1] + pf[fo - 1])
+        jx, jy = {1: (ix - 1, iy), 2: (ix + 1, iy), 3: (ix, iy - 1), 4: (ix, iy + 1)}[f]
+        inside = (jx >= 0) & (jx < nx) & (jy >= 0) & (jy < ny)
+        li = np.nonzero(inside)[0]
+        lj = at[jx[li], jy[li]]
+        res[li, sl] = hout[li, sl] - zeta * gin[li, sl] - nu * gin[lj, so]
+        lb = np.nonzero(~inside)[0]
+        pos = iy[lb] if f in (1, 2) else ix[lb]          # position along the face
+        idx = rootoff[f - 1] + pos[:, None] * pf[f - 1] + np.arange(pf[f - 1])[None, :]
+        res[lb, sl] = gin[lb, sl] - G[idx]
+    A0abs = np.asarray(abs(A0).sum(axis=1)).ravel()
+    Rabs = np.asarray(abs(R).sum(axis=1)).ravel()
+    normA = max(A0abs[nb:].max() + np.abs(kvals).max(),
+                (Rabs + (abs(zeta) + abs(nu)) * A0abs[:nb]).max())
+    bmax = max(np.abs(F).max(), np.abs(G).max() if G.size else 0.0)
+    return float(np.abs(res).max() / (normA * np.abs(U).max() + bmax))

@@ -1,0 +1,317 @@
+"""Host-side mirror of robinsolver's public API over the B200 C-ABI.
+
+Same type names, fields and calls as the reference:
+
+    T = robin_tree();  T.bndry_params = ...             (robin_tree_module.f90:55-77)
+    T.factor(L, op, opts)                               (robin_tree_factor, :96-185)
+    T.solve(rhs)                                        (robin_tree_solve, :198-233)
+    u = get_solution(T)                                 (robin_output_module.f90:48-75)
+
+Differences that follow from the host/device split:
+
+* callbacks (``elliptic_operator.k``, ``elliptic_rhs.f``, ``bndry_rhs.g_face``) are
+  vectorised: they receive an ``(npts, 3)`` float64 array of the points the reference would
+  pass one at a time, and return ``npts`` complex values (``scalar_callback`` adapts a
+  per-point function);
+* ``solve`` also accepts a list of ``elliptic_rhs``: every right-hand side is solved in one
+  batched sweep and ``get_solution(T, irhs)`` selects one;
+* errors raise ``RobinSolverError`` carrying the reference's ``stop`` message;
+* every solve applies its own boundary data (the reference applies boundary data only on the
+  first solve of a process).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import lib
+
+
+class RobinSolverError(RuntimeError):
+    """A failed call; ``code`` is the C-ABI status (RB_ERR_*)."""
+
+    def __init__(self, code, msg):
+        super().__init__(msg)
+        self.code = code
+
+
+def _check(code, handle=None):
+    if code != _lib.RB_OK:
+        raise RobinSolverError(code, _lib.last_error(handle))
+
+
+def scalar_callback(fn):
+    """Adapts a per-point function ``fn(x) -> complex`` (x of length 3) to the vectorised form."""
+    def vec(X):
+        return np.array([fn(x) for x in np.asarray(X)], dtype=np.complex128)
+    return vec
+
+
+@dataclass
+class debug_opts:
+    """derived_type_module.f90:285-290."""
+    txt_output: bool = False
+    no_delete: bool = False
+
+
+@dataclass
+class solve_opts:
+    """derived_type_module.f90:309-320.  ``h`` is overwritten by ``factor`` with the last leaf's
+    grid spacing, as get_h does on robin_tree%opts."""
+    h_tgt: float = 0.0
+    h: np.ndarray = field(default_factory=lambda: np.zeros(3))
+    ordering: int = 1
+    disc: str = "fd"
+    local_mode: str = "LU"
+    R_mode: str = "LU"
+    kb: float = 1.0
+    debug: debug_opts = field(default_factory=debug_opts)
+
+
+@dataclass
+class elliptic_operator:
+    """derived_type_module.f90:72-84.  ``coeff`` and ``robin_coeff`` are carried but, as in the
+    reference, never read on the factor/solve path."""
+    d: int = 2
+    domain: np.ndarray = field(default_factory=lambda: np.array([[0.0, 0.0, 0.0], [1.0, 1.0, 1.0]]))
+    coeff: object = None
+    k: object = None
+    robin_coeff: np.ndarray = field(default_factory=lambda: np.zeros((6, 2), dtype=np.complex128))
+
+
+@dataclass
+class bndry_rhs:
+    """derived_type_module.f90:92-96."""
+    g_face: object = None
+
+
+@dataclass
+class elliptic_rhs:
+    """derived_type_module.f90:109-115."""
+    d: int = 2
+    f: object = None
+    g: list = field(default_factory=lambda: [bndry_rhs() for _ in range(6)])
+
+
+@dataclass
+class leaf_solution:
+    """robin_output_module.f90:32-37."""
+    box: np.ndarray
+    u: np.ndarray
+
+
+PRECISIONS = {"fp64": _lib.RB_PREC_FP64, "mixed": _lib.RB_PREC_MIXED}
+
+
+class robin_tree:
+    """robin_tree (robin_tree_module.f90:55-77) backed by a device-resident factorization."""
+
+    def __init__(self, device_budget: int = 0, skip_root_rtr: bool = False):
+        self.bndry_params = None
+        self.nlvls = 0
+        self.ell_op = None
+        self.opts = None
+        self.factored = False
+        self.f_time = 0.0
+        self.s_time = 0.0
+        self._h = None
+        self._info = None
+        self._budget = int(device_budget)
+        self._skip_root = bool(skip_root_rtr)
+
+    # -- handle ----------------------------------------------------------------------------------
+    def close(self):
+        if self._h is not None:
+            lib.rb_tree_destroy(self._h)
+            self._h = None
+        self.factored = False
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def _create(self, L, ell_op, opts):
+        if self.bndry_params is None:
+            raise RobinSolverError(_lib.RB_ERR_BNDRY_PARAMS, "robin_tree%bndry_params is not set")
+        self.close()
+        g = _lib.rb_geom()
+        g.d = int(ell_op.d)
+        g.L = int(L)
+        dom = np.asarray(ell_op.domain, dtype=np.float64)
+        for j in range(3):
+            g.domain[2 * j] = dom[0, j]
+            g.domain[2 * j + 1] = dom[1, j]
+        g.h_tgt = float(opts.h_tgt)
+        g.kb = float(opts.kb)
+        bp = np.asarray(self.bndry_params, dtype=np.complex128)
+        for q, (i, j) in enumerate([(0, 0), (1, 0), (0, 1), (1, 1)]):
+            g.bndry_params[2 * q] = bp[i, j].real
+            g.bndry_params[2 * q + 1] = bp[i, j].imag
+        g.ordering = int(opts.ordering)
+        g.flags = (_lib.RB_FLAG_VERBOSE if opts.debug.txt_output else 0) | \
+                  (_lib.RB_FLAG_SKIP_ROOT_RTR if self._skip_root else 0)
+        g.device_budget = self._budget
+        h = _lib.C.c_void_p()
+        _check(lib.rb_tree_create(_lib.C.byref(g), _lib.C.byref(h)))
+        self._h = h
+        self._info = self.info()
+
+    def info(self) -> _lib.rb_info:
+        inf = _lib.rb_info()
+        _check(lib.rb_tree_info(self._h, _lib.C.byref(inf)), self._h)
+        return inf
+
+    def sample_points(self, which: int) -> np.ndarray:
+        inf = self._info
+        n = {
+            _lib.RB_POINTS_POTENTIAL: inf.n_interior,
+            _lib.RB_POINTS_SOURCE: inf.n_interior,
+            _lib.RB_POINTS_BOUNDARY: inf.root_nb,
+            _lib.RB_POINTS_SOLUTION: inf.nleaves * inf.leaf_n,
+        }[which]
+        X = np.zeros((n, 3), dtype=np.float64)
+        _check(lib.rb_tree_sample_points(self._h, which, _lib.dptr(X)), self._h)
+        return X
+
+    # -- factor / solve ----------------------------------------------------------------------------
+    def plan(self, L, ell_op, opts):
+        """Builds the tree without factoring (host only)."""
+        self.nlvls = int(L)
+        self.ell_op = ell_op
+        self.opts = opts
+        self._create(L, ell_op, opts)
+        return self._info
+
+    def factor(self, L, ell_op: elliptic_operator, opts: solve_opts, precision: str = "fp64"):
+        """robin_tree%factor(L, op, opts)."""
+        self.plan(L, ell_op, opts)
+        if ell_op.k is None:
+            raise RobinSolverError(_lib.RB_ERR_INVALID, "elliptic_operator%k is not associated")
+        X = self.sample_points(_lib.RB_POINTS_POTENTIAL)
+        kv = np.ascontiguousarray(np.asarray(ell_op.k(X), dtype=np.complex128))
+        self.factor_samples(kv, precision)
+
+    def factor_samples(self, kv: np.ndarray, precision: str = "fp64"):
+        """Factor with the potential already sampled at RB_POINTS_POTENTIAL."""
+        kv = np.ascontiguousarray(kv, dtype=np.complex128)
+        if kv.size != self._info.n_interior:
+            raise RobinSolverError(_lib.RB_ERR_INVALID, "potential sample count mismatch")
+        self.factored = False
+        _check(lib.rb_tree_factor(self._h, _lib.dptr(kv), PRECISIONS[precision]), self._h)
+        self.factored = True
+        self._info = self.info()
+        if self.opts is not None:
+            self.opts.h = np.array(self._info.h_last[:], dtype=np.float64)
+        self._update_times()
+
+    def _update_times(self):
+        f = _lib.C.c_double()
+        s = _lib.C.c_double()
+        _check(lib.rb_tree_times(self._h, _lib.C.byref(f), _lib.C.byref(s)), self._h)
+        self.f_time, self.s_time = f.value, s.value
+
+    def sample_rhs(self, rhs_list):
+        """(f, g) sample arrays for a list of elliptic_rhs, in the C-ABI layouts."""
+        inf = self._info
+        Xf = self.sample_points(_lib.RB_POINTS_SOURCE)
+        Xg = self.sample_points(_lib.RB_POINTS_BOUNDARY)
+        a, b = inf.root_a, inf.root_b
+        bounds = [0, b, 2 * b, 2 * b + a, 2 * b + 2 * a]
+        F = np.zeros((len(rhs_list), inf.n_interior), dtype=np.complex128)
+        G = np.zeros((len(rhs_list), inf.root_nb), dtype=np.complex128)
+        for r, rhs in enumerate(rhs_list):
+            if rhs.d != self.ell_op.d:
+                raise RobinSolverError(_lib.RB_ERR_DIM_MISMATCH, "Error: Dimensions of Robin Tree and RHS do not match.")
+            if rhs.f is not None:
+                F[r] = rhs.f(Xf)
+            for fc in range(4):
+                gf = rhs.g[fc].g_face if isinstance(rhs.g[fc], bndry_rhs) else rhs.g[fc]
+                if gf is not None:
+                    G[r, bounds[fc]:bounds[fc + 1]] = gf(Xg[bounds[fc]:bounds[fc + 1]])
+        return F, G
+
+    def solve(self, rhs):
+        """robin_tree%solve(rhs); ``rhs`` may be a list for a batched solve."""
+        if not self.factored:
+            raise RobinSolverError(_lib.RB_ERR_NOT_FACTORED, "Error: Robin Tree must be factored first.")
+        rhs_list = rhs if isinstance(rhs, (list, tuple)) else [rhs]
+        F, G = self.sample_rhs(rhs_list)
+        self.solve_samples(F, G)
+
+    def solve_samples(self, F: np.ndarray, G: np.ndarray):
+        F = np.ascontiguousarray(F, dtype=np.complex128)
+        G = np.ascontiguousarray(G, dtype=np.complex128)
+        nr = F.shape[0]
+        if F.size != nr * self._info.n_interior or G.size != nr * self._info.root_nb:
+            raise RobinSolverError(_lib.RB_ERR_INVALID, "right-hand side sample count mismatch")
+        _check(lib.rb_tree_solve(self._h, nr, _lib.dptr(F), _lib.dptr(G)), self._h)
+        self._info = self.info()
+        self._update_times()
+
+    def solution_array(self, irhs: int = 0) -> np.ndarray:
+        """Solution of one RHS as an (nleaves, leaf_n) array in get_solution order."""
+        inf = self._info
+        u = np.zeros((inf.nleaves, inf.leaf_n), dtype=np.complex128)
+        _check(lib.rb_get_solution(self._h, irhs, _lib.dptr(u), None), self._h)
+        return u
+
+    def get_rtr(self, level: int, node: int) -> np.ndarray:
+        """node%RtR of a node as one nb x nb matrix (faces x1 x2 y1 y2)."""
+        a, b = self._level_grid(level)
+        nb = 2 * (a + b)
+        out = np.zeros((nb, nb), dtype=np.complex128, order="F")
+        _check(lib.rb_tree_get_rtr(self._h, level, node, _lib.dptr(out)), self._h)
+        return out
+
+    def _level_grid(self, level: int):
+        """(a, b) grid of the nodes of a level."""
+        sh = (_lib.C.c_int32 * 3)()
+        _check(lib.rb_tree_level_shape(self._h, level, sh), self._h)
+        return sh[1], sh[2]
+
+    def stage_times(self, with_flops=False):
+        """Timed entries as (name, ms) or (name, ms, flops)."""
+        n = lib.rb_tree_stage_times(self._h, None, None, None, 0)
+        ms = (_lib.C.c_double * max(n, 1))()
+        fl = (_lib.C.c_double * max(n, 1))()
+        names = (_lib.C.c_char_p * max(n, 1))()
+        lib.rb_tree_stage_times(self._h, ms, fl, names, n)
+        if with_flops:
+            return [(names[i].decode(), ms[i], fl[i]) for i in range(n)]
+        return [(names[i].decode(), ms[i]) for i in range(n)]
+
+    def clear_stage_times(self):
+        _check(lib.rb_tree_clear_stage_times(self._h), self._h)
+
+    def set_timing(self, mode=1):
+        """0 off, 1 per stage, 2 per kernel launch (accumulating)."""
+        _check(lib.rb_tree_set_timing(self._h, int(mode)), self._h)
+
+    def launch_counts(self):
+        f = _lib.C.c_int64()
+        s = _lib.C.c_int64()
+        _check(lib.rb_tree_launch_counts(self._h, _lib.C.byref(f), _lib.C.byref(s)), self._h)
+        return f.value, s.value
+
+
+def get_solution(T: robin_tree, irhs: int = 0):
+    """get_solution(T, u) (robin_output_module.f90:48-75): leaf_solution per leaf, DFS order."""
+    if not T.factored:
+        raise RobinSolverError(_lib.RB_ERR_NOT_FACTORED, "Error in GET_SOLUTION: Robin Tree not factored.")
+    inf = T._info
+    u = np.zeros((inf.nleaves, inf.leaf_n), dtype=np.complex128)
+    boxes = np.zeros((inf.nleaves, 6), dtype=np.float64)
+    _check(lib.rb_get_solution(T.handle, irhs, _lib.dptr(u), _lib.dptr(boxes)), T.handle)
+    out = []
+    for i in range(inf.nleaves):
+        box = np.array([[boxes[i, 0], boxes[i, 2], boxes[i, 4]], [boxes[i, 1], boxes[i, 3], boxes[i, 5]]])
+        out.append(leaf_solution(box=box, u=u[i].copy()))
+    return out

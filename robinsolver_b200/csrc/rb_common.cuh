@@ -1,0 +1,101 @@
+// rb_common.cuh -- complex FP64 helpers and the strided/gathered matrix views shared by
+// every kernel of the B200 HPS factor/solve.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+#include <climits>
+#include <cstdint>
+
+namespace rb {
+
+using z = double2;  // interleaved complex128: x = re, y = im
+
+__host__ __device__ __forceinline__ z zmk(double re, double im) { return make_double2(re, im); }
+__host__ __device__ __forceinline__ z zadd(z a, z b) { return zmk(a.x + b.x, a.y + b.y); }
+__host__ __device__ __forceinline__ z zsub(z a, z b) { return zmk(a.x - b.x, a.y - b.y); }
+__host__ __device__ __forceinline__ z zneg(z a) { return zmk(-a.x, -a.y); }
+__host__ __device__ __forceinline__ z zmul(z a, z b) {
+    return zmk(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__host__ __device__ __forceinline__ z zscale(double s, z a) { return zmk(s * a.x, s * a.y); }
+// acc += a*b with four FMAs
+__device__ __forceinline__ void zfma(z& acc, z a, z b) {
+    acc.x = fma(a.x, b.x, acc.x);
+    acc.x = fma(-a.y, b.y, acc.x);
+    acc.y = fma(a.x, b.y, acc.y);
+    acc.y = fma(a.y, b.x, acc.y);
+}
+// acc -= a*b
+__device__ __forceinline__ void zfms(z& acc, z a, z b) {
+    acc.x = fma(-a.x, b.x, acc.x);
+    acc.x = fma(a.y, b.y, acc.x);
+    acc.y = fma(-a.x, b.y, acc.y);
+    acc.y = fma(-a.y, b.x, acc.y);
+}
+// 1/a from (re - i im) / (re^2 + im^2)
+__host__ __device__ __forceinline__ z zrcp(z a) {
+    double d = a.x * a.x + a.y * a.y;
+    return zmk(a.x / d, -a.y / d);
+}
+// |re| + |im|: the magnitude LAPACK's izamax ranks pivots by
+__host__ __device__ __forceinline__ double zabs1(z a) { return fabs(a.x) + fabs(a.y); }
+
+// A matrix view: logical element (i, j) lives at p[row(i) + col(j) * ld], where row(i) is
+// rmap[i] when a map is given, else i shifted past a skipped band [rs, rs + rl) (same for
+// columns).  Maps and bands express the face gathers of the merge (non-interface faces of
+// a child) without copies.
+struct ZView {
+    const z* p;
+    const int* rmap;
+    const int* cmap;
+    long long ld;
+    int rs, rl, cs, cl;
+};
+struct ZOut {
+    z* p;
+    const int* rmap;
+    const int* cmap;
+    long long ld;
+    int rs, rl, cs, cl;
+};
+
+__host__ __device__ __forceinline__ ZView zview(const z* p, long long ld) {
+    ZView v;
+    v.p = p; v.rmap = nullptr; v.cmap = nullptr; v.ld = ld;
+    v.rs = INT_MAX; v.rl = 0; v.cs = INT_MAX; v.cl = 0;
+    return v;
+}
+__host__ __device__ __forceinline__ ZOut zout(z* p, long long ld) {
+    ZOut v;
+    v.p = p; v.rmap = nullptr; v.cmap = nullptr; v.ld = ld;
+    v.rs = INT_MAX; v.rl = 0; v.cs = INT_MAX; v.cl = 0;
+    return v;
+}
+template <class V>
+__device__ __forceinline__ int vrow(const V& v, int i) {
+    return v.rmap ? __ldg(v.rmap + i) : (i + (i >= v.rs ? v.rl : 0));
+}
+template <class V>
+__device__ __forceinline__ int vcol(const V& v, int j) {
+    return v.cmap ? __ldg(v.cmap + j) : (j + (j >= v.cs ? v.cl : 0));
+}
+
+// One complex GEMM problem: D(i,j) = alpha * sum_k A(i,k) B(k,j) + beta * C(i,j)
+// (the beta term only when C.p != nullptr; C may alias D).
+struct GemmDesc {
+    ZView A, B, C;
+    ZOut D;
+    z alpha, beta;
+    int m, n, k;
+    int pad;
+};
+
+// A batch of GEMM problems resident in device memory, with the largest sizes for grid setup.
+struct GemmBatch {
+    GemmDesc* d_desc = nullptr;
+    int count = 0;
+    int max_m = 0, max_n = 0, max_k = 0;
+    double flops = 0.0;   // 8*m*n*k summed
+};
+
+}  // namespace rb

@@ -1,0 +1,51 @@
+// rb_gemm.cu -- descriptor-driven batched complex128 GEMM for sm_100a.
+//
+// One launch runs a whole batch of independent problems (all nodes of a tree level, all
+// leaves of a tree): blockIdx.y picks the problem descriptor, blockIdx.x a C tile.  Operands
+// are ZViews, so the merge's face gathers (non-interface rows/columns of a child's
+// Robin-to-Robin matrix) and the scatter into the parent's face order happen inside the loads
+// and the epilogue instead of in copy kernels.
+//
+// FP64 has no tcgen05 kind; the arithmetic is DFMA with register tiling (rb_gemm_tile.cuh).
+#include "rb_gemm_tile.cuh"
+#include "rb_kernels.h"
+
+namespace rb {
+
+template <int BM, int BN, int TM, int TN, int BK, int MINB>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN), MINB)
+zgemm_desc_kernel(const GemmDesc* __restrict__ descs) {
+    constexpr int NT = (BM / TM) * (BN / TN);
+    __shared__ GemmDesc sd;
+    {
+        const unsigned long long* src = reinterpret_cast<const unsigned long long*>(descs + blockIdx.y);
+        unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sd);
+        for (int w = threadIdx.x; w < (int)(sizeof(GemmDesc) / 8); w += NT) dst[w] = src[w];
+    }
+    __syncthreads();
+    zgemm_tile<BM, BN, TM, TN, BK>(sd, blockIdx.x);
+}
+
+template <int BM, int BN, int TM, int TN, int BK, int MINB>
+static cudaError_t launch_cfg(const GemmBatch& b, cudaStream_t s) {
+    constexpr int NT = (BM / TM) * (BN / TN);
+    const int tiles = ((b.max_m + BM - 1) / BM) * ((b.max_n + BN - 1) / BN);
+    for (int off = 0; off < b.count; off += 65535) {
+        const int cnt = (b.count - off) < 65535 ? (b.count - off) : 65535;
+        dim3 grid(tiles, cnt);
+        zgemm_desc_kernel<BM, BN, TM, TN, BK, MINB><<<grid, NT, 0, s>>>(b.d_desc + off);
+        note_launch();
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gemm_batch(const GemmBatch& b, cudaStream_t s) {
+    static_assert(sizeof(GemmDesc) % 8 == 0, "descriptor copy assumes 8-byte words");
+    if (b.count == 0 || b.max_m == 0 || b.max_n == 0) return cudaSuccess;
+    const int mm = b.max_m, nn = b.max_n;
+    if (mm <= 16 && nn <= 16) return launch_cfg<16, 16, 2, 2, 8, 8>(b, s);
+    if (mm <= 32 || nn <= 32) return launch_cfg<32, 32, 4, 2, 8, 4>(b, s);
+    return launch_cfg<64, 64, 4, 4, 8, 1>(b, s);
+}
+
+}  // namespace rb

@@ -1,0 +1,71 @@
+// rb_kernels.h -- internal launch interface of the CUDA kernels (not part of the C-ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include "rb_common.cuh"
+
+namespace rb {
+
+// ---- launch accounting --------------------------------------------------------------------------
+void note_launch();
+long long launch_count();
+
+// ---- batched GEMM ---------------------------------------------------------------------------------
+cudaError_t launch_gemm_batch(const GemmBatch& b, cudaStream_t s);
+
+// ---- batched Gauss-Jordan inversion (in place, partial pivoting by |re|+|im|) ----------------------
+struct GJDesc {
+    z* A;          // m x m, column-major
+    long long ld;
+    int* ipiv;     // m
+    z* Wm;         // m x nb workspace (blocked path)
+    z* Zb;         // nb x m workspace (blocked path)
+};
+constexpr int GJ_SMALL_MAX = 64;
+int gj_panel_width(int m);                         // nb of the blocked path (0 for the small path)
+long long gj_workspace_elems(int m);               // complex elements of Wm + Zb per matrix
+cudaError_t gj_invert_batch(const GJDesc* d_desc, int count, int m, int* d_status, cudaStream_t s);
+
+// ---- leaf stage ---------------------------------------------------------------------------------------
+struct LeafGeom {
+    int a, b;          // interior grid
+    int nb, n;         // boundary points, unknowns
+    double kb;         // solve_opts%kb
+};
+// Interior Schur complement S = A_ii - A_ib A_bb^-1 A_bi of every leaf's FD matrix, written
+// column-major (ld = a*b) at S + leaf * (a*b)^2.  k: nleaves*a*b potential samples.
+cudaError_t leaf_schur(const LeafGeom& g, int nleaves, const double* h /*2 per leaf*/, const z* k,
+                       z* S, cudaStream_t s);
+// Y = R A^-1 (nb x n, ld = nb) of every leaf from its inverted Schur complement.
+cudaError_t leaf_outgoing(const LeafGeom& g, int nleaves, const double* h, const z* Sinv, z* Y,
+                          cudaStream_t s);
+// t = f - A_ib A_bb^-1 g_b for every leaf and right-hand side: t is (a*b) x nrhs per leaf (ld a*b),
+// f is RHS-major [rhs][leaf][a*b], g is [leaf][rhs][nb].
+cudaError_t leaf_condense_rhs(const LeafGeom& g, int nleaves, int nrhs, const double* h, const z* f,
+                              const z* gb, z* t, cudaStream_t s);
+// u_b = A_bb^-1 (g_b - A_bi u_i) into the boundary rows of the solution [rhs][leaf][n].
+cudaError_t leaf_boundary_values(const LeafGeom& g, int nleaves, int nrhs, const double* h,
+                                 const z* gb, z* sol, cudaStream_t s);
+
+// ---- merge helpers -------------------------------------------------------------------------------------
+struct ChildStore {
+    const z* rtr;      // node 0's Robin-to-Robin matrix
+    long long stride;  // elements between consecutive nodes
+    long long ld;      // leading dimension
+};
+// D = zeta*I - T2_ii for every parent node (child2 = 2*node+1), into dst + node*m*m.
+cudaError_t merge_form_d(ChildStore c, int nnodes, int m, int o2, z zeta, z* dst, cudaStream_t s);
+// S = zeta*I - T1_ii - nu^2 * Dinv for every parent node (child1 = 2*node).
+cudaError_t merge_form_s(ChildStore c, int nnodes, int m, int o1, z zeta, z nu, const z* dinv, z* dst,
+                         cudaStream_t s);
+
+// ---- sweep helpers --------------------------------------------------------------------------------------
+// children's g on their non-interface faces from the parent's g (backward sweep):
+// g_child[phys(t)] = g_parent[pmap[t]] for both children, every node and RHS.
+cudaError_t sweep_scatter_down(int nnodes, int nrhs, int nbp, int nbc, int m, int o1, int o2, int n1,
+                               int n2, const int* pmap1, const int* pmap2, const z* gpar, z* gchild,
+                               cudaStream_t s);
+// g_i^(1) += y1, g_i^(2) += y2 (tmp holds per node [tg1 | tg2 | y2 | y1], each m x nrhs).
+cudaError_t sweep_add_interface(int nnodes, int nrhs, int nbc, int m, int o1, int o2, const z* tmp,
+                                z* gchild, cudaStream_t s);
+
+}  // namespace rb

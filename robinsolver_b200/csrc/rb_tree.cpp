@@ -1,0 +1,940 @@
+// rb_tree.cpp -- the C-ABI of the B200 HPS factor/solve (include/robin_b200.h).
+//
+// Host runtime: builds the tree plan (no device work), owns the device memory of a tree, builds
+// the GEMM / Gauss-Jordan descriptor batches once per tree (factor) and once per right-hand-side
+// count (solve), and launches the level-by-level stages on the handle's stream.
+//
+// Factor (robin_tree_factor -> compute_RTR, robin_tree_module.f90:96-185, 375-650):
+//   leaves:  S = A_ii - A_ib A_bb^-1 A_bi from the potential samples, S^-1 by Gauss-Jordan,
+//            Y = R A^-1 (RtR in its first nb columns)
+//   level l = L-1 .. 0, all nodes of the level in one launch per stage:
+//            inv(D), D = zeta I - T2_ii;  inv(S), S = zeta I - T1_ii - nu^2 inv(D)
+//            Y2R = inv(D) T2_iN;  Y1 = inv(S) [T1_iN, -nu Y2R];  Y2 = [0, Y2R] - nu inv(D) Y1
+//            parent RtR = T_NN + [T1_Ni Y1; T2_Ni Y2], scattered into the parent's face order
+//   (Y1 = [C11, -C12] and Y2 = [-C21, C22] in the reference's names, :482-615.)
+// Solve (forward_sub / backward_sub, robin_tree_module.f90:813-1146), all RHS at once:
+//   forward:  leaf h = Y(:, nb:) f;  per level (g1_i, g2_i) = M^-1 (h1_i, h2_i) and the parent's
+//             h = h_N + T_Ni g_i
+//   backward: root g = boundary data; per level children's g_N from the parent, Tg = T_iN g_N,
+//             g_i += M^-1 Tg;  leaf u = A^-1 [g; f] through the condensed Schur inverse.
+//   M^-1 (x1, x2): w = inv(D) x2; y1 = inv(S)(x1 - nu w); y2 = w - nu inv(D) y1 (apply_invm, :1252).
+#include <algorithm>
+#include <atomic>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "robin_b200.h"
+#include "rb_kernels.h"
+#include "rb_plan.hpp"
+
+namespace rb {
+static std::atomic<long long> g_launches{0};
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+}  // namespace rb
+
+using namespace rb;
+
+static thread_local std::string g_create_error;
+
+namespace {
+
+struct DevBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+struct GJBatch {
+    GJDesc* d_desc = nullptr;
+    int count = 0;
+    int m = 0;
+};
+
+struct StageTimer {
+    const char* name;
+    double flops;
+    int ev;          // index of the start event in the pool (end = ev + 1)
+};
+
+}  // namespace
+
+struct rb_tree {
+    rb_geom geom;
+    Plan P;
+    std::string err;
+    cudaStream_t stream = nullptr;
+    int device = 0;
+    bool factored = false;
+    double f_time = 0.0, s_time = 0.0;
+    z zeta, nu;
+    int64_t budget = 0;
+    std::vector<DevBuf> bufs;        // every allocation, for the budget and destroy
+    int64_t held = 0;
+    bool verbose = false;
+    bool skip_root = false;
+
+    // persistent factor storage
+    double* d_h = nullptr;
+    z* d_k = nullptr;
+    z* leaf_sinv = nullptr;
+    z* leaf_Y = nullptr;
+    std::vector<z*> rtr;             // per level < L
+    std::vector<z*> dinv, sinv;      // per level < L
+    std::vector<int*> d_pmap1, d_pmap2;
+    int* d_status = nullptr;
+    // factor workspace
+    z* Y1 = nullptr;
+    z* Y2 = nullptr;
+    z* gj_work = nullptr;
+    int* gj_ipiv = nullptr;
+    // factor launch batches
+    GJBatch gj_leaf;
+    std::vector<GJBatch> gj_d, gj_s;
+    std::vector<GemmBatch> fM1, fM2, fM3, fM4;
+    bool factor_ready = false;
+
+    // solve storage
+    int cap_rhs = 0;                 // capacity of the solve buffers
+    int built_rhs = 0;               // nrhs the solve batches were built for
+    int nrhs = 0;                    // RHS held from the last solve
+    z* d_f = nullptr;
+    std::vector<z*> hbuf, gbuf;      // per level 0..L
+    z* tmp = nullptr;
+    z* tleaf = nullptr;
+    z* sol = nullptr;
+    GemmBatch sL0, sL2;
+    std::vector<GemmBatch> sF12, sF3, sF4, sF5, sB1, sB23, sB4, sB5;
+    std::vector<DevBuf> solve_bufs;
+
+    // timing: 0 off, 1 per stage, 2 per launch
+    int timing = 0;
+    struct StageTime { std::string name; double ms; double flops; };
+    std::vector<StageTime> stage_ms;
+    std::vector<StageTimer> timers;
+    std::vector<cudaEvent_t> ev_pool;
+    int ev_used = 0;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    int64_t factor_launches = 0, solve_launches = 0;
+};
+
+// ---------------------------------------------------------------------------------------------------
+#define RB_CK(call)                                                                              \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess) {                                                                 \
+            t->err = std::string("CUDA error: ") + cudaGetErrorString(e_) + " at " #call;        \
+            return RB_ERR_CUDA;                                                                  \
+        }                                                                                        \
+    } while (0)
+
+static int fail(rb_tree* t, int code, const std::string& msg) {
+    t->err = msg;
+    return code;
+}
+
+static int dev_alloc(rb_tree* t, std::vector<DevBuf>& list, size_t bytes, void** out) {
+    *out = nullptr;
+    if (bytes == 0) return RB_OK;
+    bytes = (bytes + 255) & ~size_t(255);
+    if (t->budget > 0 && t->held + (int64_t)bytes > t->budget)
+        return fail(t, RB_ERR_OUT_OF_MEMORY, "device budget exceeded: need " + std::to_string(t->held + bytes) +
+                                                 " bytes, budget " + std::to_string(t->budget));
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(t, e == cudaErrorMemoryAllocation ? RB_ERR_OUT_OF_MEMORY : RB_ERR_CUDA,
+                    std::string("cudaMalloc of ") + std::to_string(bytes) + " bytes failed: " + cudaGetErrorString(e));
+    }
+    list.push_back({p, bytes});
+    t->held += (int64_t)bytes;
+    *out = p;
+    return RB_OK;
+}
+
+template <class T>
+static int alloc_n(rb_tree* t, std::vector<DevBuf>& list, size_t n, T** out) {
+    void* p = nullptr;
+    int rc = dev_alloc(t, list, n * sizeof(T), &p);
+    *out = static_cast<T*>(p);
+    return rc;
+}
+
+static void free_list(rb_tree* t, std::vector<DevBuf>& list) {
+    for (auto& b : list) {
+        cudaFree(b.p);
+        t->held -= (int64_t)b.bytes;
+    }
+    list.clear();
+}
+
+static int upload_gemm(rb_tree* t, std::vector<DevBuf>& list, const std::vector<GemmDesc>& h, GemmBatch& b) {
+    b = GemmBatch();
+    b.count = (int)h.size();
+    if (h.empty()) return RB_OK;
+    int rc = alloc_n(t, list, h.size(), &b.d_desc);
+    if (rc) return rc;
+    RB_CK(cudaMemcpy(b.d_desc, h.data(), h.size() * sizeof(GemmDesc), cudaMemcpyHostToDevice));
+    for (const auto& d : h) {
+        b.max_m = std::max(b.max_m, d.m);
+        b.max_n = std::max(b.max_n, d.n);
+        b.max_k = std::max(b.max_k, d.k);
+        b.flops += 8.0 * d.m * d.n * d.k;
+    }
+    return RB_OK;
+}
+
+static int upload_gj(rb_tree* t, std::vector<DevBuf>& list, const std::vector<GJDesc>& h, int m, GJBatch& b) {
+    b = GJBatch();
+    b.count = (int)h.size();
+    b.m = m;
+    if (h.empty()) return RB_OK;
+    int rc = alloc_n(t, list, h.size(), &b.d_desc);
+    if (rc) return rc;
+    RB_CK(cudaMemcpy(b.d_desc, h.data(), h.size() * sizeof(GJDesc), cudaMemcpyHostToDevice));
+    return RB_OK;
+}
+
+static ZView band_view(const z* p, long long ld, int rs, int rl, int cs, int cl) {
+    ZView v = zview(p, ld);
+    v.rs = rs; v.rl = rl; v.cs = cs; v.cl = cl;
+    return v;
+}
+
+static GemmDesc gdesc(int m, int n, int k, ZView A, ZView B, ZOut D, z alpha) {
+    GemmDesc g;
+    std::memset(&g, 0, sizeof(g));
+    g.A = A; g.B = B; g.C = zview(nullptr, 1); g.D = D;
+    g.alpha = alpha; g.beta = zmk(0.0, 0.0);
+    g.m = m; g.n = n; g.k = k;
+    return g;
+}
+
+static ChildStore child_store(const rb_tree* t, int l) {   // storage of level l+1's RtR
+    const Plan& P = t->P;
+    ChildStore c;
+    if (l + 1 == P.L) {
+        c.rtr = t->leaf_Y;
+        c.stride = (long long)P.leaf_nb() * P.leaf_n();
+        c.ld = P.leaf_nb();
+    } else {
+        const int nbc = P.lv[l + 1].nb;
+        c.rtr = t->rtr[l + 1];
+        c.stride = (long long)nbc * nbc;
+        c.ld = nbc;
+    }
+    return c;
+}
+
+// ---------------------------------------------------------------------------------------------------
+static int timer_open(rb_tree* t, const char* name, double flops) {
+    if (t->ev_used + 2 > (int)t->ev_pool.size()) {
+        for (int i = 0; i < 64; ++i) {
+            cudaEvent_t e;
+            RB_CK(cudaEventCreate(&e));
+            t->ev_pool.push_back(e);
+        }
+    }
+    StageTimer st{name, flops, t->ev_used};
+    t->ev_used += 2;
+    RB_CK(cudaEventRecord(t->ev_pool[st.ev], t->stream));
+    t->timers.push_back(st);
+    return RB_OK;
+}
+static int timer_close(rb_tree* t) {
+    RB_CK(cudaEventRecord(t->ev_pool[t->timers.back().ev + 1], t->stream));
+    return RB_OK;
+}
+// stage granularity (timing == 1)
+static int timer_begin(rb_tree* t, const char* name) { return t->timing == 1 ? timer_open(t, name, 0.0) : RB_OK; }
+static int timer_end(rb_tree* t) { return t->timing == 1 ? timer_close(t) : RB_OK; }
+// launch granularity (timing == 2): one entry per kernel launch (or per Gauss-Jordan batch)
+static int ltimer_begin(rb_tree* t, const char* name, double flops) {
+    return t->timing == 2 ? timer_open(t, name, flops) : RB_OK;
+}
+static int ltimer_end(rb_tree* t) { return t->timing == 2 ? timer_close(t) : RB_OK; }
+static void timers_collect(rb_tree* t) {
+    for (auto& st : t->timers) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, t->ev_pool[st.ev], t->ev_pool[st.ev + 1]) == cudaSuccess)
+            t->stage_ms.push_back({st.name, (double)ms, st.flops});
+    }
+    t->timers.clear();
+    t->ev_used = 0;
+}
+
+// ---------------------------------------------------------------------------------------------------
+static int ensure_factor_storage(rb_tree* t) {
+    if (t->factor_ready) return RB_OK;
+    const Plan& P = t->P;
+    const int L = P.L, nl = P.nleaves(), a = P.leaf_a(), b = P.leaf_b(), ab = a * b;
+    const int nb = P.leaf_nb(), n = P.leaf_n();
+    int rc;
+    RB_CK(cudaGetDevice(&t->device));
+    if (!t->stream) RB_CK(cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking));
+    if ((rc = alloc_n(t, t->bufs, 2 * (size_t)nl, &t->d_h))) return rc;
+    RB_CK(cudaMemcpy(t->d_h, P.leaf_h.data(), 2 * nl * sizeof(double), cudaMemcpyHostToDevice));
+    if ((rc = alloc_n(t, t->bufs, (size_t)nl * ab, &t->d_k))) return rc;
+    if ((rc = alloc_n(t, t->bufs, (size_t)nl * ab * ab, &t->leaf_sinv))) return rc;
+    if ((rc = alloc_n(t, t->bufs, (size_t)nl * nb * n, &t->leaf_Y))) return rc;
+    if ((rc = alloc_n(t, t->bufs, 1, &t->d_status))) return rc;
+    t->rtr.assign(L, nullptr);
+    t->dinv.assign(L, nullptr);
+    t->sinv.assign(L, nullptr);
+    t->d_pmap1.assign(L, nullptr);
+    t->d_pmap2.assign(L, nullptr);
+    size_t ymax = 0;
+    for (int l = 0; l < L; ++l) {
+        const PlanLevel& p = P.lv[l];
+        if (!(l == 0 && t->skip_root))
+            if ((rc = alloc_n(t, t->bufs, (size_t)p.nnodes * p.nb * p.nb, &t->rtr[l]))) return rc;
+        if ((rc = alloc_n(t, t->bufs, (size_t)p.nnodes * p.m * p.m, &t->dinv[l]))) return rc;
+        if ((rc = alloc_n(t, t->bufs, (size_t)p.nnodes * p.m * p.m, &t->sinv[l]))) return rc;
+        if ((rc = alloc_n(t, t->bufs, p.pmap1.size(), &t->d_pmap1[l]))) return rc;
+        if ((rc = alloc_n(t, t->bufs, p.pmap2.size(), &t->d_pmap2[l]))) return rc;
+        RB_CK(cudaMemcpy(t->d_pmap1[l], p.pmap1.data(), p.pmap1.size() * sizeof(int), cudaMemcpyHostToDevice));
+        RB_CK(cudaMemcpy(t->d_pmap2[l], p.pmap2.data(), p.pmap2.size() * sizeof(int), cudaMemcpyHostToDevice));
+        ymax = std::max(ymax, (size_t)p.nnodes * p.m * (p.n1 + p.n2));
+    }
+    if ((rc = alloc_n(t, t->bufs, ymax, &t->Y1))) return rc;
+    if ((rc = alloc_n(t, t->bufs, ymax, &t->Y2))) return rc;
+    // Gauss-Jordan workspace: the largest batch (leaves or one level's nodes)
+    size_t wmax = (size_t)nl * (size_t)gj_workspace_elems(ab), imax = (size_t)nl * ab;
+    for (int l = 0; l < L; ++l) {
+        const PlanLevel& p = P.lv[l];
+        wmax = std::max(wmax, (size_t)p.nnodes * (size_t)gj_workspace_elems(p.m));
+        imax = std::max(imax, (size_t)p.nnodes * p.m);
+    }
+    if ((rc = alloc_n(t, t->bufs, std::max<size_t>(wmax, 1), &t->gj_work))) return rc;
+    if ((rc = alloc_n(t, t->bufs, imax, &t->gj_ipiv))) return rc;
+
+    auto gj_descs = [&](z* base, long long stride, int ld, int count, int m) {
+        std::vector<GJDesc> v(count);
+        const long long ws = gj_workspace_elems(m);
+        const int nbw = gj_panel_width(m);
+        for (int i = 0; i < count; ++i) {
+            v[i].A = base + (long long)i * stride;
+            v[i].ld = ld;
+            v[i].ipiv = t->gj_ipiv + (long long)i * m;
+            v[i].Wm = t->gj_work + (long long)i * ws;
+            v[i].Zb = t->gj_work + (long long)i * ws + (long long)m * nbw;
+        }
+        return v;
+    };
+    if ((rc = upload_gj(t, t->bufs, gj_descs(t->leaf_sinv, (long long)ab * ab, ab, nl, ab), ab, t->gj_leaf))) return rc;
+    t->gj_d.resize(L);
+    t->gj_s.resize(L);
+    t->fM1.resize(L); t->fM2.resize(L); t->fM3.resize(L); t->fM4.resize(L);
+    const z one = zmk(1.0, 0.0);
+    const z mnu = zneg(t->nu);
+    for (int l = 0; l < L; ++l) {
+        const PlanLevel& p = P.lv[l];
+        const int m = p.m, n1 = p.n1, n2 = p.n2, o1 = p.o1, o2 = p.o2, nn = p.nnodes;
+        if ((rc = upload_gj(t, t->bufs, gj_descs(t->dinv[l], (long long)m * m, m, nn, m), m, t->gj_d[l]))) return rc;
+        if ((rc = upload_gj(t, t->bufs, gj_descs(t->sinv[l], (long long)m * m, m, nn, m), m, t->gj_s[l]))) return rc;
+        const ChildStore cs = child_store(t, l);
+        std::vector<GemmDesc> m1, m2, m3, m4;
+        for (int i = 0; i < nn; ++i) {
+            const z* r1 = cs.rtr + (2LL * i) * cs.stride;
+            const z* r2 = cs.rtr + (2LL * i + 1) * cs.stride;
+            const long long ld = cs.ld;
+            z* dv = t->dinv[l] + (long long)i * m * m;
+            z* sv = t->sinv[l] + (long long)i * m * m;
+            z* y1 = t->Y1 + (long long)i * m * (n1 + n2);
+            z* y2 = t->Y2 + (long long)i * m * (n1 + n2);
+            // Y2R = inv(D) T2_iN
+            m1.push_back(gdesc(m, n2, m, zview(dv, m), band_view(r2 + o2, ld, INT_MAX, 0, o2, m),
+                               zout(y2 + (long long)m * n1, m), one));
+            // Y1L = inv(S) T1_iN ; Y1R = -nu inv(S) Y2R
+            m2.push_back(gdesc(m, n1, m, zview(sv, m), band_view(r1 + o1, ld, INT_MAX, 0, o1, m), zout(y1, m), one));
+            m2.push_back(gdesc(m, n2, m, zview(sv, m), zview(y2 + (long long)m * n1, m),
+                               zout(y1 + (long long)m * n1, m), mnu));
+            // Y2L = -nu inv(D) Y1L ; Y2R = Y2R - nu inv(D) Y1R
+            m3.push_back(gdesc(m, n1, m, zview(dv, m), zview(y1, m), zout(y2, m), mnu));
+            {
+                GemmDesc g = gdesc(m, n2, m, zview(dv, m), zview(y1 + (long long)m * n1, m),
+                                   zout(y2 + (long long)m * n1, m), mnu);
+                g.C = zview(y2 + (long long)m * n1, m);
+                g.beta = one;
+                m3.push_back(g);
+            }
+            if (!(l == 0 && t->skip_root)) {
+                z* par = t->rtr[l] + (long long)i * p.nb * p.nb;
+                const ZView t1ni = band_view(r1 + (long long)o1 * ld, ld, o1, m, INT_MAX, 0);
+                const ZView t2ni = band_view(r2 + (long long)o2 * ld, ld, o2, m, INT_MAX, 0);
+                ZOut o11 = zout(par, p.nb), o12 = zout(par, p.nb), o21 = zout(par, p.nb), o22 = zout(par, p.nb);
+                o11.rmap = t->d_pmap1[l]; o11.cmap = t->d_pmap1[l];
+                o12.rmap = t->d_pmap1[l]; o12.cmap = t->d_pmap2[l];
+                o21.rmap = t->d_pmap2[l]; o21.cmap = t->d_pmap1[l];
+                o22.rmap = t->d_pmap2[l]; o22.cmap = t->d_pmap2[l];
+                GemmDesc g11 = gdesc(n1, n1, m, t1ni, zview(y1, m), o11, one);
+                g11.C = band_view(r1, ld, o1, m, o1, m);
+                g11.beta = one;
+                GemmDesc g12 = gdesc(n1, n2, m, t1ni, zview(y1 + (long long)m * n1, m), o12, one);
+                GemmDesc g21 = gdesc(n2, n1, m, t2ni, zview(y2, m), o21, one);
+                GemmDesc g22 = gdesc(n2, n2, m, t2ni, zview(y2 + (long long)m * n1, m), o22, one);
+                g22.C = band_view(r2, ld, o2, m, o2, m);
+                g22.beta = one;
+                m4.push_back(g11); m4.push_back(g12); m4.push_back(g21); m4.push_back(g22);
+            }
+        }
+        if ((rc = upload_gemm(t, t->bufs, m1, t->fM1[l]))) return rc;
+        if ((rc = upload_gemm(t, t->bufs, m2, t->fM2[l]))) return rc;
+        if ((rc = upload_gemm(t, t->bufs, m3, t->fM3[l]))) return rc;
+        if ((rc = upload_gemm(t, t->bufs, m4, t->fM4[l]))) return rc;
+    }
+    t->factor_ready = true;
+    return RB_OK;
+}
+
+#define RB_LAUNCH(call)                                                                          \
+    do {                                                                                         \
+        cudaError_t e_ = (call);                                                                 \
+        if (e_ != cudaSuccess) {                                                                 \
+            t->err = std::string("CUDA launch failed: ") + cudaGetErrorString(e_) + " in " #call; \
+            return RB_ERR_CUDA;                                                                  \
+        }                                                                                        \
+    } while (0)
+
+#define RB_TIMED(name, flops, call)                                                              \
+    do {                                                                                         \
+        int rc_ = ltimer_begin(t, name, flops);                                                  \
+        if (rc_) return rc_;                                                                     \
+        RB_LAUNCH(call);                                                                         \
+        if ((rc_ = ltimer_end(t))) return rc_;                                                   \
+    } while (0)
+
+static double gj_flops(int m, int count) { return 8.0 * (double)m * m * m * count; }
+
+static int run_factor(rb_tree* t, const z* dk) {
+    const Plan& P = t->P;
+    const int L = P.L, nl = P.nleaves();
+    LeafGeom lg{P.leaf_a(), P.leaf_b(), P.leaf_nb(), P.leaf_n(), P.kb};
+    cudaStream_t s = t->stream;
+    int rc;
+    RB_CK(cudaMemsetAsync(t->d_status, 0, sizeof(int), s));
+    if ((rc = timer_begin(t, "leaf_schur"))) return rc;
+    RB_TIMED("leaf_schur", 0.0, leaf_schur(lg, nl, t->d_h, dk, t->leaf_sinv, s));
+    if ((rc = timer_end(t))) return rc;
+    if ((rc = timer_begin(t, "leaf_invert"))) return rc;
+    RB_TIMED("gj_invert", gj_flops(lg.a * lg.b, nl), gj_invert_batch(t->gj_leaf.d_desc, nl, lg.a * lg.b, t->d_status, s));
+    if ((rc = timer_end(t))) return rc;
+    if ((rc = timer_begin(t, "leaf_outgoing"))) return rc;
+    RB_TIMED("leaf_outgoing", 0.0, leaf_outgoing(lg, nl, t->d_h, t->leaf_sinv, t->leaf_Y, s));
+    if ((rc = timer_end(t))) return rc;
+    static const char* lvl_names[] = {"merge_l0", "merge_l1", "merge_l2", "merge_l3", "merge_l4", "merge_l5",
+                                      "merge_l6", "merge_l7", "merge_l8", "merge_l9", "merge_l10", "merge_l11",
+                                      "merge_l12", "merge_l13", "merge_l14", "merge_l15", "merge_l16"};
+    for (int l = L - 1; l >= 0; --l) {
+        const PlanLevel& p = P.lv[l];
+        const ChildStore cs = child_store(t, l);
+        if ((rc = timer_begin(t, l < 17 ? lvl_names[l] : "merge_deep"))) return rc;
+        RB_TIMED("merge_form", 0.0, merge_form_d(cs, p.nnodes, p.m, p.o2, t->zeta, t->dinv[l], s));
+        RB_TIMED("gj_invert", gj_flops(p.m, p.nnodes), gj_invert_batch(t->gj_d[l].d_desc, p.nnodes, p.m, t->d_status, s));
+        RB_TIMED("merge_form", 0.0, merge_form_s(cs, p.nnodes, p.m, p.o1, t->zeta, t->nu, t->dinv[l], t->sinv[l], s));
+        RB_TIMED("gj_invert", gj_flops(p.m, p.nnodes), gj_invert_batch(t->gj_s[l].d_desc, p.nnodes, p.m, t->d_status, s));
+        RB_TIMED("zgemm", t->fM1[l].flops, launch_gemm_batch(t->fM1[l], s));
+        RB_TIMED("zgemm", t->fM2[l].flops, launch_gemm_batch(t->fM2[l], s));
+        RB_TIMED("zgemm", t->fM3[l].flops, launch_gemm_batch(t->fM3[l], s));
+        RB_TIMED("zgemm", t->fM4[l].flops, launch_gemm_batch(t->fM4[l], s));
+        if ((rc = timer_end(t))) return rc;
+    }
+    return RB_OK;
+}
+
+// ---------------------------------------------------------------------------------------------------
+static int ensure_solve_storage(rb_tree* t, int nrhs) {
+    const Plan& P = t->P;
+    const int L = P.L, nl = P.nleaves(), ab = P.leaf_a() * P.leaf_b(), nb = P.leaf_nb(), n = P.leaf_n();
+    int rc;
+    if (nrhs > t->cap_rhs) {
+        free_list(t, t->solve_bufs);
+        t->built_rhs = 0;
+        const int k = nrhs;
+        if ((rc = alloc_n(t, t->solve_bufs, (size_t)k * nl * ab, &t->d_f))) return rc;
+        t->hbuf.assign(L + 1, nullptr);
+        t->gbuf.assign(L + 1, nullptr);
+        size_t tmax = 0;
+        for (int l = 0; l <= L; ++l) {
+            const PlanLevel& p = P.lv[l];
+            if (l > 0)
+                if ((rc = alloc_n(t, t->solve_bufs, (size_t)p.nnodes * p.nb * k, &t->hbuf[l]))) return rc;
+            if ((rc = alloc_n(t, t->solve_bufs, (size_t)p.nnodes * p.nb * k, &t->gbuf[l]))) return rc;
+            if (l < L) tmax = std::max(tmax, (size_t)p.nnodes * 4 * p.m * k);
+        }
+        if ((rc = alloc_n(t, t->solve_bufs, tmax, &t->tmp))) return rc;
+        if ((rc = alloc_n(t, t->solve_bufs, (size_t)nl * k * ab, &t->tleaf))) return rc;
+        if ((rc = alloc_n(t, t->solve_bufs, (size_t)k * nl * n, &t->sol))) return rc;
+        t->cap_rhs = k;
+    }
+    if (t->built_rhs == nrhs) return RB_OK;
+    // descriptor batches for this RHS count (allocated in solve_bufs too)
+    const int k = nrhs;
+    const z one = zmk(1.0, 0.0), mnu = zneg(t->nu);
+    std::vector<GemmDesc> v;
+    for (int i = 0; i < nl; ++i)
+        v.push_back(gdesc(nb, k, ab, zview(t->leaf_Y + (long long)i * nb * n + (long long)nb * nb, nb),
+                          zview(t->d_f + (long long)i * ab, (long long)nl * ab),
+                          zout(t->hbuf[L] + (long long)i * nb * k, nb), one));
+    if ((rc = upload_gemm(t, t->solve_bufs, v, t->sL0))) return rc;
+    v.clear();
+    for (int i = 0; i < nl; ++i)
+        v.push_back(gdesc(ab, k, ab, zview(t->leaf_sinv + (long long)i * ab * ab, ab),
+                          zview(t->tleaf + (long long)i * ab * k, ab),
+                          zout(t->sol + (long long)i * n + nb, (long long)nl * n), one));
+    if ((rc = upload_gemm(t, t->solve_bufs, v, t->sL2))) return rc;
+    t->sF12.assign(L, GemmBatch()); t->sF3.assign(L, GemmBatch()); t->sF4.assign(L, GemmBatch());
+    t->sF5.assign(L, GemmBatch()); t->sB1.assign(L, GemmBatch()); t->sB23.assign(L, GemmBatch());
+    t->sB4.assign(L, GemmBatch()); t->sB5.assign(L, GemmBatch());
+    for (int l = 0; l < L; ++l) {
+        const PlanLevel& p = P.lv[l];
+        const int m = p.m, n1 = p.n1, n2 = p.n2, o1 = p.o1, o2 = p.o2, nbc = p.nbc, nbp = p.nb;
+        const ChildStore cs = child_store(t, l);
+        std::vector<GemmDesc> f12, f3, f4, f5, b1, b23, b4, b5;
+        for (int i = 0; i < p.nnodes; ++i) {
+            const z* r1 = cs.rtr + (2LL * i) * cs.stride;
+            const z* r2 = cs.rtr + (2LL * i + 1) * cs.stride;
+            const long long ld = cs.ld;
+            z* dv = t->dinv[l] + (long long)i * m * m;
+            z* sv = t->sinv[l] + (long long)i * m * m;
+            z* h1 = t->hbuf[l + 1] + (2LL * i) * nbc * k;
+            z* h2 = t->hbuf[l + 1] + (2LL * i + 1) * nbc * k;
+            z* g1 = t->gbuf[l + 1] + (2LL * i) * nbc * k;
+            z* g2 = t->gbuf[l + 1] + (2LL * i + 1) * nbc * k;
+            // forward: g2_i = inv(D) h2_i ; g1_i = inv(S) h1_i
+            f12.push_back(gdesc(m, k, m, zview(dv, m), zview(h2 + o2, nbc), zout(g2 + o2, nbc), one));
+            f12.push_back(gdesc(m, k, m, zview(sv, m), zview(h1 + o1, nbc), zout(g1 + o1, nbc), one));
+            {   // g1_i -= nu inv(S) g2_i
+                GemmDesc g = gdesc(m, k, m, zview(sv, m), zview(g2 + o2, nbc), zout(g1 + o1, nbc), mnu);
+                g.C = zview(g1 + o1, nbc); g.beta = one;
+                f3.push_back(g);
+            }
+            {   // g2_i -= nu inv(D) g1_i
+                GemmDesc g = gdesc(m, k, m, zview(dv, m), zview(g1 + o1, nbc), zout(g2 + o2, nbc), mnu);
+                g.C = zview(g2 + o2, nbc); g.beta = one;
+                f4.push_back(g);
+            }
+            if (l > 0) {   // parent h = h_N + T_Ni g_i
+                z* hp = t->hbuf[l] + (long long)i * nbp * k;
+                ZOut oa = zout(hp, nbp), ob = zout(hp, nbp);
+                oa.rmap = t->d_pmap1[l];
+                ob.rmap = t->d_pmap2[l];
+                GemmDesc ga = gdesc(n1, k, m, band_view(r1 + (long long)o1 * ld, ld, o1, m, INT_MAX, 0),
+                                    zview(g1 + o1, nbc), oa, one);
+                ga.C = band_view(h1, nbc, o1, m, INT_MAX, 0); ga.beta = one;
+                GemmDesc gb = gdesc(n2, k, m, band_view(r2 + (long long)o2 * ld, ld, o2, m, INT_MAX, 0),
+                                    zview(g2 + o2, nbc), ob, one);
+                gb.C = band_view(h2, nbc, o2, m, INT_MAX, 0); gb.beta = one;
+                f5.push_back(ga); f5.push_back(gb);
+            }
+            // backward: tmp = [tg1 | tg2 | y2 | y1]
+            z* tb = t->tmp + (long long)i * 4 * m * k;
+            z* tg1 = tb;
+            z* tg2 = tb + (long long)m * k;
+            z* w = tb + 2LL * m * k;
+            z* y1 = tb + 3LL * m * k;
+            b1.push_back(gdesc(m, k, n1, band_view(r1 + o1, ld, INT_MAX, 0, o1, m),
+                               band_view(g1, nbc, o1, m, INT_MAX, 0), zout(tg1, m), one));
+            b1.push_back(gdesc(m, k, n2, band_view(r2 + o2, ld, INT_MAX, 0, o2, m),
+                               band_view(g2, nbc, o2, m, INT_MAX, 0), zout(tg2, m), one));
+            b23.push_back(gdesc(m, k, m, zview(dv, m), zview(tg2, m), zout(w, m), one));
+            b23.push_back(gdesc(m, k, m, zview(sv, m), zview(tg1, m), zout(y1, m), one));
+            {
+                GemmDesc g = gdesc(m, k, m, zview(sv, m), zview(w, m), zout(y1, m), mnu);
+                g.C = zview(y1, m); g.beta = one;
+                b4.push_back(g);
+            }
+            {
+                GemmDesc g = gdesc(m, k, m, zview(dv, m), zview(y1, m), zout(w, m), mnu);
+                g.C = zview(w, m); g.beta = one;
+                b5.push_back(g);
+            }
+        }
+        if ((rc = upload_gemm(t, t->solve_bufs, f12, t->sF12[l]))) return rc;
+        if ((rc = upload_gemm(t, t->solve_bufs, f3, t->sF3[l]))) return rc;
+        if ((rc = upload_gemm(t, t->solve_bufs, f4, t->sF4[l]))) return rc;
+        if ((rc = upload_gemm(t, t->solve_bufs, f5, t->sF5[l]))) return rc;
+        if ((rc = upload_gemm(t, t->solve_bufs, b1, t->sB1[l]))) return rc;
+        if ((rc = upload_gemm(t, t->solve_bufs, b23, t->sB23[l]))) return rc;
+        if ((rc = upload_gemm(t, t->solve_bufs, b4, t->sB4[l]))) return rc;
+        if ((rc = upload_gemm(t, t->solve_bufs, b5, t->sB5[l]))) return rc;
+    }
+    t->built_rhs = nrhs;
+    return RB_OK;
+}
+
+static int run_solve(rb_tree* t, int k) {
+    const Plan& P = t->P;
+    const int L = P.L, nl = P.nleaves();
+    LeafGeom lg{P.leaf_a(), P.leaf_b(), P.leaf_nb(), P.leaf_n(), P.kb};
+    cudaStream_t s = t->stream;
+    int rc;
+    if ((rc = timer_begin(t, "forward"))) return rc;
+    RB_TIMED("zgemm", t->sL0.flops, launch_gemm_batch(t->sL0, s));
+    for (int l = L - 1; l >= 0; --l) {
+        RB_TIMED("zgemm", t->sF12[l].flops, launch_gemm_batch(t->sF12[l], s));
+        RB_TIMED("zgemm", t->sF3[l].flops, launch_gemm_batch(t->sF3[l], s));
+        RB_TIMED("zgemm", t->sF4[l].flops, launch_gemm_batch(t->sF4[l], s));
+        if (l > 0) RB_TIMED("zgemm", t->sF5[l].flops, launch_gemm_batch(t->sF5[l], s));
+    }
+    if ((rc = timer_end(t))) return rc;
+    if ((rc = timer_begin(t, "backward"))) return rc;
+    for (int l = 0; l < L; ++l) {
+        const PlanLevel& p = P.lv[l];
+        RB_TIMED("sweep_aux", 0.0, sweep_scatter_down(p.nnodes, k, p.nb, p.nbc, p.m, p.o1, p.o2, p.n1, p.n2, t->d_pmap1[l],
+                                     t->d_pmap2[l], t->gbuf[l], t->gbuf[l + 1], s));
+        RB_TIMED("zgemm", t->sB1[l].flops, launch_gemm_batch(t->sB1[l], s));
+        RB_TIMED("zgemm", t->sB23[l].flops, launch_gemm_batch(t->sB23[l], s));
+        RB_TIMED("zgemm", t->sB4[l].flops, launch_gemm_batch(t->sB4[l], s));
+        RB_TIMED("zgemm", t->sB5[l].flops, launch_gemm_batch(t->sB5[l], s));
+        RB_TIMED("sweep_aux", 0.0, sweep_add_interface(p.nnodes, k, p.nbc, p.m, p.o1, p.o2, t->tmp, t->gbuf[l + 1], s));
+    }
+    if ((rc = timer_end(t))) return rc;
+    if ((rc = timer_begin(t, "leaf_recover"))) return rc;
+    RB_TIMED("sweep_aux", 0.0, leaf_condense_rhs(lg, nl, k, t->d_h, t->d_f, t->gbuf[L], t->tleaf, s));
+    RB_TIMED("zgemm", t->sL2.flops, launch_gemm_batch(t->sL2, s));
+    RB_TIMED("sweep_aux", 0.0, leaf_boundary_values(lg, nl, k, t->d_h, t->gbuf[L], t->sol, s));
+    if ((rc = timer_end(t))) return rc;
+    return RB_OK;
+}
+
+// ---------------------------------------------------------------------------------------------------
+extern "C" {
+
+int rb_tree_create(const rb_geom* geom, rb_tree** out) {
+    if (!geom || !out) {
+        g_create_error = "rb_tree_create: null argument";
+        return RB_ERR_INVALID;
+    }
+    *out = nullptr;
+    Plan P;
+    std::string msg = build_plan(geom->d, geom->L, geom->domain, geom->h_tgt, geom->kb, P);
+    if (!msg.empty()) {
+        g_create_error = msg;
+        if (geom->d == 3 && msg.find("not implemented") != std::string::npos) return RB_ERR_UNSUPPORTED;
+        if (msg.find("Interface sizes") != std::string::npos) return RB_ERR_GEOMETRY;
+        if (msg.find("Dimension") != std::string::npos || msg.find("domain") != std::string::npos) return RB_ERR_DOMAIN;
+        return RB_ERR_INVALID;
+    }
+    if (geom->ordering != 1) {
+        g_create_error = "Invalid ordering parameter in igrid2lin";
+        return RB_ERR_INVALID;
+    }
+    // bndry_params(i,j) column-major, interleaved
+    const double* bp = geom->bndry_params;
+    const z b11 = zmk(bp[0], bp[1]), b21 = zmk(bp[2], bp[3]), b12 = zmk(bp[4], bp[5]), b22 = zmk(bp[6], bp[7]);
+    const z det = zsub(zmul(b11, b22), zmul(b12, b21));
+    if (std::hypot(det.x, det.y) < 1.0e-3) {
+        g_create_error = "Error: Boundary parameter matrix is nearly singular.";
+        return RB_ERR_BNDRY_PARAMS;
+    }
+    rb_tree* t = new rb_tree();
+    t->geom = *geom;
+    t->P = std::move(P);
+    // nu and zeta of compute_RTR (robin_tree_module.f90:425-431)
+    const z den = zmul(zmul(zmk(2.0, 0.0), b11), b12);
+    const z rden = zrcp(den);
+    t->nu = zmul(zadd(zneg(zmul(b11, b22)), zmul(b12, b21)), rden);
+    t->zeta = zmul(zadd(zmul(b11, b22), zmul(b12, b21)), rden);
+    t->budget = geom->device_budget;
+    t->verbose = (geom->flags & RB_FLAG_VERBOSE) != 0;
+    t->skip_root = (geom->flags & RB_FLAG_SKIP_ROOT_RTR) != 0;
+    // refuse up front a problem the budget cannot hold (persistent factor storage only)
+    if (t->budget > 0) {
+        const Plan& Q = t->P;
+        const double ab = (double)Q.leaf_a() * Q.leaf_b();
+        double need = (double)Q.nleaves() * (ab * ab + (double)Q.leaf_nb() * Q.leaf_n() + ab) * 16.0;
+        for (int l = 0; l < Q.L; ++l)
+            need += (double)Q.lv[l].nnodes * ((double)Q.lv[l].nb * Q.lv[l].nb + 2.0 * Q.lv[l].m * Q.lv[l].m) * 16.0;
+        if (need > (double)t->budget) {
+            g_create_error = "device budget exceeded: the factorization needs at least " +
+                             std::to_string((long long)need) + " bytes, budget " + std::to_string(t->budget);
+            delete t;
+            return RB_ERR_OUT_OF_MEMORY;
+        }
+    }
+    if (t->verbose) std::printf("Domain partition completed.\n");
+    *out = t;
+    return RB_OK;
+}
+
+int rb_tree_destroy(rb_tree* t) {
+    if (!t) return RB_OK;
+    if (t->stream) cudaStreamSynchronize(t->stream);
+    timers_collect(t);
+    free_list(t, t->solve_bufs);
+    free_list(t, t->bufs);
+    for (auto& e : t->ev)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : t->ev_pool) cudaEventDestroy(e);
+    if (t->stream) cudaStreamDestroy(t->stream);
+    delete t;
+    return RB_OK;
+}
+
+const char* rb_last_error(const rb_tree* t) { return t ? t->err.c_str() : g_create_error.c_str(); }
+
+int rb_tree_info(const rb_tree* t, rb_info* info) {
+    if (!t || !info) return RB_ERR_INVALID;
+    const Plan& P = t->P;
+    info->nleaves = P.nleaves();
+    info->leaf_a = P.leaf_a();
+    info->leaf_b = P.leaf_b();
+    info->leaf_n = P.leaf_n();
+    info->leaf_nb = P.leaf_nb();
+    info->root_nb = P.lv[0].nb;
+    info->root_a = P.lv[0].a;
+    info->root_b = P.lv[0].b;
+    for (int j = 0; j < 3; ++j) info->h_last[j] = P.h_last[j];
+    info->n_interior = (int64_t)P.nleaves() * P.leaf_a() * P.leaf_b();
+    info->device_bytes = t->held;
+    info->factored = t->factored ? 1 : 0;
+    info->nrhs = t->nrhs;
+    return RB_OK;
+}
+
+int rb_tree_sample_points(const rb_tree* t, int which, double* xyz) {
+    if (!t || !xyz) return RB_ERR_INVALID;
+    const Plan& P = t->P;
+    const PlanLevel& lf = P.lv[P.L];
+    const int a = lf.a, b = lf.b, nl = lf.nnodes;
+    // grid2real (fd_module.f90:669-700): lo + g*h - h/2, snapped to the face on the boundary
+    auto coord = [&](int leaf, int gi, int gj, const double* h, double* out) {
+        const double* lo = &lf.lo[3 * leaf];
+        const double* hi = &lf.hi[3 * leaf];
+        out[0] = (lo[0] + gi * h[0]) - h[0] / 2;
+        out[1] = (lo[1] + gj * h[1]) - h[1] / 2;
+        out[2] = (lo[2] + 1 * h[2]) - h[2] / 2;
+        if (gi == 0) out[0] = lo[0]; else if (gi == a + 1) out[0] = hi[0];
+        if (gj == 0) out[1] = lo[1]; else if (gj == b + 1) out[1] = hi[1];
+    };
+    size_t q = 0;
+    if (which == RB_POINTS_POTENTIAL || which == RB_POINTS_SOURCE) {
+        for (int i = 0; i < nl; ++i) {
+            double h[3] = {P.leaf_h[2 * i], P.leaf_h[2 * i + 1], 0.0};
+            const double* hp = which == RB_POINTS_POTENTIAL ? h : P.h_last;
+            for (int gj = 1; gj <= b; ++gj)
+                for (int gi = 1; gi <= a; ++gi, ++q) coord(i, gi, gj, hp, xyz + 3 * q);
+        }
+        return RB_OK;
+    }
+    if (which == RB_POINTS_BOUNDARY) {
+        for (int f = 0; f < 4; ++f)
+            for (int i = 0; i < nl; ++i) {
+                if (!lf.isb[4 * i + f]) continue;
+                const int cnt = f < 2 ? b : a;
+                for (int s = 1; s <= cnt; ++s, ++q) {
+                    double pt[3];
+                    if (f == 0) coord(i, 0, s, P.h_last, pt);
+                    else if (f == 1) coord(i, a + 1, s, P.h_last, pt);
+                    else if (f == 2) coord(i, s, 0, P.h_last, pt);
+                    else coord(i, s, b + 1, P.h_last, pt);
+                    // face-local coordinates as fd_make_bndry_vec leaves them (fd_module.f90:648-649)
+                    xyz[3 * q] = f < 2 ? pt[1] : pt[0];
+                    xyz[3 * q + 1] = 0.0;
+                    xyz[3 * q + 2] = 0.0;
+                }
+            }
+        return RB_OK;
+    }
+    if (which == RB_POINTS_SOLUTION) {
+        for (int i = 0; i < nl; ++i) {
+            for (int s = 1; s <= b; ++s, ++q) coord(i, 0, s, P.h_last, xyz + 3 * q);
+            for (int s = 1; s <= b; ++s, ++q) coord(i, a + 1, s, P.h_last, xyz + 3 * q);
+            for (int s = 1; s <= a; ++s, ++q) coord(i, s, 0, P.h_last, xyz + 3 * q);
+            for (int s = 1; s <= a; ++s, ++q) coord(i, s, b + 1, P.h_last, xyz + 3 * q);
+            for (int gj = 1; gj <= b; ++gj)
+                for (int gi = 1; gi <= a; ++gi, ++q) coord(i, gi, gj, P.h_last, xyz + 3 * q);
+        }
+        return RB_OK;
+    }
+    return RB_ERR_INVALID;
+}
+
+static int factor_common(rb_tree* t, const double* k, int precision, bool host, int sync) {
+    if (!t) return RB_ERR_INVALID;
+    if (!k) return fail(t, RB_ERR_INVALID, "rb_tree_factor: null potential samples");
+    if (precision != RB_PREC_FP64)
+        return fail(t, RB_ERR_UNSUPPORTED, "precision mode " + std::to_string(precision) + " is not implemented");
+    int rc = ensure_factor_storage(t);
+    if (rc) return rc;
+    const Plan& P = t->P;
+    const size_t nint = (size_t)P.nleaves() * P.leaf_a() * P.leaf_b();
+    t->factored = false;
+    t->nrhs = 0;
+    if (t->timing == 1) {
+        timers_collect(t);
+        t->stage_ms.clear();
+    }
+    const z* dk = reinterpret_cast<const z*>(k);
+    if (host) {
+        RB_CK(cudaMemcpyAsync(t->d_k, k, nint * sizeof(z), cudaMemcpyHostToDevice, t->stream));
+        dk = t->d_k;
+    }
+    for (auto& e : t->ev)
+        if (!e) RB_CK(cudaEventCreate(&e));
+    const long long l0 = launch_count();
+    RB_CK(cudaEventRecord(t->ev[0], t->stream));
+    if ((rc = run_factor(t, dk))) return rc;
+    RB_CK(cudaEventRecord(t->ev[1], t->stream));
+    t->factor_launches = launch_count() - l0;
+    if (host || sync) {
+        RB_CK(cudaStreamSynchronize(t->stream));
+        int st = 0;
+        RB_CK(cudaMemcpy(&st, t->d_status, sizeof(int), cudaMemcpyDeviceToHost));
+        if (st) return fail(t, RB_ERR_NUMERIC, "zero pivot met while inverting a leaf or interface matrix");
+        float ms = 0.f;
+        RB_CK(cudaEventElapsedTime(&ms, t->ev[0], t->ev[1]));
+        t->f_time = ms * 1e-3;
+        timers_collect(t);
+        if (t->verbose) std::printf("RTR computation completed.\nFactorization completed.\n");
+    }
+    t->factored = true;
+    return RB_OK;
+}
+
+int rb_tree_factor(rb_tree* t, const double* k, int precision) { return factor_common(t, k, precision, true, 1); }
+int rb_tree_factor_device(rb_tree* t, const double* dk, int precision, int sync) {
+    return factor_common(t, dk, precision, false, sync);
+}
+
+static int solve_common(rb_tree* t, int nrhs, const double* f, const double* g, bool host, int sync) {
+    if (!t) return RB_ERR_INVALID;
+    if (!t->factored) return fail(t, RB_ERR_NOT_FACTORED, "Error: Robin Tree must be factored first.");
+    if (nrhs <= 0) return fail(t, RB_ERR_INVALID, "rb_tree_solve: nrhs must be positive");
+    if (!f || !g) return fail(t, RB_ERR_INVALID, "rb_tree_solve: null right-hand side");
+    int rc = ensure_solve_storage(t, nrhs);
+    if (rc) return rc;
+    const Plan& P = t->P;
+    const size_t nint = (size_t)P.nleaves() * P.leaf_a() * P.leaf_b();
+    const size_t nroot = (size_t)P.lv[0].nb;
+    const cudaMemcpyKind kind = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
+    t->nrhs = 0;
+    RB_CK(cudaEventRecord(t->ev[2], t->stream));
+    RB_CK(cudaMemcpyAsync(t->d_f, f, nrhs * nint * sizeof(z), kind, t->stream));
+    RB_CK(cudaMemcpyAsync(t->gbuf[0], g, nrhs * nroot * sizeof(z), kind, t->stream));
+    const long long l0 = launch_count();
+    if ((rc = run_solve(t, nrhs))) return rc;
+    t->solve_launches = launch_count() - l0;
+    RB_CK(cudaEventRecord(t->ev[3], t->stream));
+    if (host || sync) {
+        RB_CK(cudaStreamSynchronize(t->stream));
+        float ms = 0.f;
+        RB_CK(cudaEventElapsedTime(&ms, t->ev[2], t->ev[3]));
+        t->s_time = ms * 1e-3;
+        timers_collect(t);
+        if (t->verbose) std::printf("Elliptic solve completed.\n");
+    }
+    t->nrhs = nrhs;
+    return RB_OK;
+}
+
+int rb_tree_solve(rb_tree* t, int nrhs, const double* f, const double* g) {
+    return solve_common(t, nrhs, f, g, true, 1);
+}
+int rb_tree_solve_device(rb_tree* t, int nrhs, const double* f, const double* g, int sync) {
+    return solve_common(t, nrhs, f, g, false, sync);
+}
+
+int rb_get_solution(const rb_tree* tc, int irhs, double* u, double* boxes) {
+    rb_tree* t = const_cast<rb_tree*>(tc);
+    if (!t || !u) return RB_ERR_INVALID;
+    if (!t->factored) return fail(t, RB_ERR_NOT_FACTORED, "Error in GET_SOLUTION: Robin Tree not factored.");
+    if (irhs < 0 || irhs >= t->nrhs) return fail(t, RB_ERR_NO_SOLUTION, "get_solution: no solution for this right-hand side");
+    const Plan& P = t->P;
+    const size_t per = (size_t)P.nleaves() * P.leaf_n();
+    RB_CK(cudaMemcpyAsync(u, t->sol + (size_t)irhs * per, per * sizeof(z), cudaMemcpyDeviceToHost, t->stream));
+    RB_CK(cudaStreamSynchronize(t->stream));
+    if (boxes) {
+        const PlanLevel& lf = P.lv[P.L];
+        for (int i = 0; i < lf.nnodes; ++i)
+            for (int j = 0; j < 3; ++j) {
+                boxes[6 * i + 2 * j] = lf.lo[3 * i + j];
+                boxes[6 * i + 2 * j + 1] = lf.hi[3 * i + j];
+            }
+    }
+    return RB_OK;
+}
+
+int rb_get_solution_device(const rb_tree* tc, double* du, int sync) {
+    rb_tree* t = const_cast<rb_tree*>(tc);
+    if (!t || !du) return RB_ERR_INVALID;
+    if (!t->factored) return fail(t, RB_ERR_NOT_FACTORED, "Error in GET_SOLUTION: Robin Tree not factored.");
+    if (t->nrhs <= 0) return fail(t, RB_ERR_NO_SOLUTION, "get_solution: no solve has run");
+    const Plan& P = t->P;
+    const size_t tot = (size_t)t->nrhs * P.nleaves() * P.leaf_n();
+    RB_CK(cudaMemcpyAsync(du, t->sol, tot * sizeof(z), cudaMemcpyDeviceToDevice, t->stream));
+    if (sync) RB_CK(cudaStreamSynchronize(t->stream));
+    return RB_OK;
+}
+
+int rb_tree_times(const rb_tree* t, double* f_time, double* s_time) {
+    if (!t) return RB_ERR_INVALID;
+    if (f_time) *f_time = t->f_time;
+    if (s_time) *s_time = t->s_time;
+    return RB_OK;
+}
+
+void* rb_tree_stream(const rb_tree* t) { return t ? (void*)t->stream : nullptr; }
+
+int rb_tree_set_timing(rb_tree* t, int mode) {
+    if (!t || mode < 0 || mode > 2) return RB_ERR_INVALID;
+    t->timing = mode;
+    return RB_OK;
+}
+
+int rb_tree_stage_times(const rb_tree* tc, double* ms, double* flops, const char** names, int n) {
+    rb_tree* t = const_cast<rb_tree*>(tc);
+    if (!t) return RB_ERR_INVALID;
+    const int cnt = (int)t->stage_ms.size();
+    for (int i = 0; i < std::min(n, cnt); ++i) {
+        if (ms) ms[i] = t->stage_ms[i].ms;
+        if (flops) flops[i] = t->stage_ms[i].flops;
+        if (names) names[i] = t->stage_ms[i].name.c_str();
+    }
+    return cnt;
+}
+
+int rb_tree_clear_stage_times(rb_tree* t) {
+    if (!t) return RB_ERR_INVALID;
+    if (t->stream) RB_CK(cudaStreamSynchronize(t->stream));
+    timers_collect(t);
+    t->stage_ms.clear();
+    return RB_OK;
+}
+
+int rb_tree_level_shape(const rb_tree* t, int level, int32_t* shape) {
+    if (!t || !shape || level < 0 || level > t->P.L) return RB_ERR_INVALID;
+    shape[0] = t->P.lv[level].nnodes;
+    shape[1] = t->P.lv[level].a;
+    shape[2] = t->P.lv[level].b;
+    return RB_OK;
+}
+
+int rb_tree_get_rtr(const rb_tree* tc, int level, int node, double* out) {
+    rb_tree* t = const_cast<rb_tree*>(tc);
+    if (!t || !out) return RB_ERR_INVALID;
+    if (!t->factored) return fail(t, RB_ERR_NOT_FACTORED, "Error: Robin Tree must be factored first.");
+    const Plan& P = t->P;
+    if (level < 0 || level > P.L || node < 0 || node >= P.lv[level].nnodes)
+        return fail(t, RB_ERR_INVALID, "rb_tree_get_rtr: level or node out of range");
+    const int nb = P.lv[level].nb;
+    const z* src = nullptr;
+    if (level == P.L) src = t->leaf_Y + (long long)node * nb * P.leaf_n();
+    else if (t->rtr[level]) src = t->rtr[level] + (long long)node * nb * nb;
+    if (!src) return fail(t, RB_ERR_INVALID, "rb_tree_get_rtr: the root RtR was not formed (RB_FLAG_SKIP_ROOT_RTR)");
+    RB_CK(cudaMemcpyAsync(out, src, (size_t)nb * nb * sizeof(z), cudaMemcpyDeviceToHost, t->stream));
+    RB_CK(cudaStreamSynchronize(t->stream));
+    return RB_OK;
+}
+
+int rb_tree_launch_counts(const rb_tree* t, int64_t* fl, int64_t* sl) {
+    if (!t) return RB_ERR_INVALID;
+    if (fl) *fl = t->factor_launches;
+    if (sl) *sl = t->solve_launches;
+    return RB_OK;
+}
+
+}  // extern "C"
