@@ -48,6 +48,7 @@ points and returns ``npts`` complex values (the reference calls a scalar
 from __future__ import annotations
 
 import math
+import time
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -353,9 +354,24 @@ def outgoing_rows(X, a, b, h, kb):
 # LAPACK wrappers with the reference's matrixdata semantics (factorization_module.f90)
 # ----------------------------------------------------------------------------------------------
 
+# When a list, every LAPACK/BLAS call adds its wall time to PROFILE[0] and 1 to PROFILE[1]:
+# the CPU cost of the reference is its LAPACK/BLAS call sequence (the Python index loops of
+# this restatement are compiled loops in the reference and are not counted).
+PROFILE = None
+
+
+def _timed(fn, *a, **kw):
+    if PROFILE is None:
+        return fn(*a, **kw)
+    t0 = time.perf_counter()
+    out = fn(*a, **kw)
+    PROFILE[0] += time.perf_counter() - t0
+    PROFILE[1] += 1
+    return out
+
 
 def _getrf(A):
-    lu, piv, info = lapack.zgetrf(A)
+    lu, piv, info = _timed(lapack.zgetrf, A)
     if info < 0:
         raise RuntimeError(f"zgetrf illegal argument {info}")
     return lu, piv
@@ -363,7 +379,7 @@ def _getrf(A):
 
 def _getrs(F, B):
     lu, piv = F
-    X, info = lapack.zgetrs(lu, piv, B)
+    X, info = _timed(lapack.zgetrs, lu, piv, B)
     if info != 0:
         raise RuntimeError(f"zgetrs info {info}")
     return X
@@ -373,12 +389,12 @@ def _getri(F):
     """mtrx_getinv with lwork = max(64, m) (factorization_module.f90:124-129)."""
     lu, piv = F
     m = lu.shape[0]
-    inv, info = lapack.zgetri(lu, piv, lwork=max(64, m))
+    inv, info = _timed(lapack.zgetri, lu, piv, lwork=max(64, m))
     return inv
 
 
 def _gemm(alpha, A, B):
-    return blas.zgemm(alpha, A, B)
+    return _timed(blas.zgemm, alpha, A, B)
 
 
 # ----------------------------------------------------------------------------------------------

@@ -81,12 +81,14 @@ __device__ __forceinline__ int vcol(const V& v, int j) {
 }
 
 // One complex GEMM problem: D(i,j) = alpha * sum_k A(i,k) B(k,j) + beta * C(i,j)
-// (the beta term only when C.p != nullptr; C may alias D).
+// (the beta term only when C.p != nullptr, and not for rows in [nobeta_r0, nobeta_r1);
+// C may alias D).
 struct GemmDesc {
     ZView A, B, C;
     ZOut D;
     z alpha, beta;
     int m, n, k;
+    int nobeta_r0, nobeta_r1;
     int pad;
 };
 

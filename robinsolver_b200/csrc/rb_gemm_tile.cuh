@@ -111,13 +111,14 @@ __device__ __forceinline__ void zgemm_tile(const GemmDesc& sd, int tile) {
         const int gi = m0 + tr + i * RG;
         if (gi >= m) continue;
         const long long drow = (long long)vrow(D, gi);
-        const long long crow = C.p ? (long long)vrow(C, gi) : 0;
+        const bool use_c = C.p && !(gi >= sd.nobeta_r0 && gi < sd.nobeta_r1);
+        const long long crow = use_c ? (long long)vrow(C, gi) : 0;
 #pragma unroll
         for (int j = 0; j < TN; ++j) {
             const int gj = n0 + tc + j * CG;
             if (gj >= n) continue;
             z v = zmul(alpha, acc[i][j]);
-            if (C.p) {
+            if (use_c) {
                 const z c = C.p[crow + (long long)vcol(C, gj) * C.ld];
                 zfma(v, beta, c);
             }

@@ -10,10 +10,14 @@
 // m  > 64: blocked Gauss-Jordan.  Per panel of nb columns:
 //   1. gj_panel: one CTA per matrix, one matrix row per thread in registers, runs the
 //      unblocked elimination on the panel (pivot search below the diagonal, row exchange,
-//      scaling, elimination of every other row) and writes W - E to a workspace;
+//      scaling, elimination of every other row), leaving the accumulated transform W in the
+//      panel columns;
 //   2. gj_swapcopy: applies the panel's row exchanges to every other column and copies the
 //      panel rows Z = A[P, rest];
-//   3. gj_update: A[:, rest] += (W - E) Z, a GEMM on the shared tile engine.
+//   3. gj_update: A[i, rest] += W[i,:] Z for rows outside the panel and A[P, rest] = W_P Z for
+//      the panel rows, one GEMM on the shared tile engine.  (Writing the panel rows as
+//      Z + (W_P - I) Z instead cancels catastrophically: W_P's diagonal holds the reciprocal
+//      pivots, ~h^2 for the FD matrices here.)
 // After the last panel the column exchanges are undone in reverse order (gj_unscramble).
 #include "rb_gemm_tile.cuh"
 #include "rb_kernels.h"
@@ -28,7 +32,7 @@ int gj_panel_width(int m) {
 
 long long gj_workspace_elems(int m) {
     const int nb = gj_panel_width(m);
-    return nb == 0 ? 0 : 2LL * m * nb;
+    return nb == 0 ? 0 : (long long)m * nb;
 }
 
 // warp argmax: larger value wins, equal values go to the smaller index
@@ -189,9 +193,6 @@ __global__ void __launch_bounds__(MAXT) gj_panel_kernel(const GJDesc* __restrict
         for (int kk = 0; kk < NB; ++kk) {
             if (kk >= nbk) break;
             g.A[r + (long long)(k0 + kk) * g.ld] = row[kk];
-            z w = row[kk];
-            if (r == k0 + kk) w.x -= 1.0;
-            g.Wm[r + (long long)kk * m] = w;
         }
     }
     if (bad) atomicOr(status, 1);
@@ -222,7 +223,7 @@ gj_update_kernel(const GJDesc* __restrict__ descs, int m, int k0, int nbk) {
     __shared__ GemmDesc sd;
     if (threadIdx.x == 0) {
         const GJDesc g = descs[blockIdx.y];
-        sd.A = zview(g.Wm, m);
+        sd.A = zview(g.A + (long long)k0 * g.ld, g.ld);   // the panel columns hold W
         sd.B = zview(g.Zb, nbk);
         sd.C = zview(g.A, g.ld);
         sd.C.cs = k0;
@@ -235,6 +236,8 @@ gj_update_kernel(const GJDesc* __restrict__ descs, int m, int k0, int nbk) {
         sd.m = m;
         sd.n = m - nbk;
         sd.k = nbk;
+        sd.nobeta_r0 = k0;          // panel rows are overwritten with W_P Z
+        sd.nobeta_r1 = k0 + nbk;
         sd.pad = 0;
     }
     __syncthreads();

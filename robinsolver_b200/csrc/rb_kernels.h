@@ -17,12 +17,11 @@ struct GJDesc {
     z* A;          // m x m, column-major
     long long ld;
     int* ipiv;     // m
-    z* Wm;         // m x nb workspace (blocked path)
     z* Zb;         // nb x m workspace (blocked path)
 };
 constexpr int GJ_SMALL_MAX = 64;
 int gj_panel_width(int m);                         // nb of the blocked path (0 for the small path)
-long long gj_workspace_elems(int m);               // complex elements of Wm + Zb per matrix
+long long gj_workspace_elems(int m);               // complex elements of Zb per matrix
 cudaError_t gj_invert_batch(const GJDesc* d_desc, int count, int m, int* d_status, cudaStream_t s);
 
 // ---- leaf stage ---------------------------------------------------------------------------------------
@@ -31,20 +30,16 @@ struct LeafGeom {
     int nb, n;         // boundary points, unknowns
     double kb;         // solve_opts%kb
 };
-// Interior Schur complement S = A_ii - A_ib A_bb^-1 A_bi of every leaf's FD matrix, written
-// column-major (ld = a*b) at S + leaf * (a*b)^2.  k: nleaves*a*b potential samples.
-cudaError_t leaf_schur(const LeafGeom& g, int nleaves, const double* h /*2 per leaf*/, const z* k,
-                       z* S, cudaStream_t s);
-// Y = R A^-1 (nb x n, ld = nb) of every leaf from its inverted Schur complement.
-cudaError_t leaf_outgoing(const LeafGeom& g, int nleaves, const double* h, const z* Sinv, z* Y,
-                          cudaStream_t s);
-// t = f - A_ib A_bb^-1 g_b for every leaf and right-hand side: t is (a*b) x nrhs per leaf (ld a*b),
-// f is RHS-major [rhs][leaf][a*b], g is [leaf][rhs][nb].
-cudaError_t leaf_condense_rhs(const LeafGeom& g, int nleaves, int nrhs, const double* h, const z* f,
-                              const z* gb, z* t, cudaStream_t s);
-// u_b = A_bb^-1 (g_b - A_bi u_i) into the boundary rows of the solution [rhs][leaf][n].
-cudaError_t leaf_boundary_values(const LeafGeom& g, int nleaves, int nrhs, const double* h,
-                                 const z* gb, z* sol, cudaStream_t s);
+// Structured leaf factor (rb_leaf.cu): per leaf the inverted diagonal blocks Sig_j^-1 of the
+// block-tridiagonal interior Schur complement (b blocks of a x a, at sinv + leaf*b*a*a) and
+// Y = R A^-1 (nb x n, ld nb, at Y + leaf*nb*n); k: nleaves*a*b potential samples.
+size_t leaf_block_factor_smem(const LeafGeom& g);
+cudaError_t leaf_block_factor(const LeafGeom& g, int nleaves, const double* h, const z* k, z* sinv, z* Y,
+                              int* status, cudaStream_t s);
+// Structured leaf solve: u = A^-1 [g; f] into sol [rhs][leaf][n]; f is [rhs][leaf][a*b] (may be
+// null for zero sources), gb is [leaf][rhs][nb].
+cudaError_t leaf_block_solve(const LeafGeom& g, int nleaves, int nrhs, const double* h, const z* f, const z* gb,
+                             const z* sinv, z* sol, cudaStream_t s);
 
 // ---- merge helpers -------------------------------------------------------------------------------------
 struct ChildStore {

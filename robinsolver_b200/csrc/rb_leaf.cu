@@ -1,0 +1,402 @@
+// rb_leaf.cu -- structured leaf factor and leaf solve for sm_100a (one CTA per leaf).
+//
+// Leaf algebra.  The reference's leaf matrix A (FD_matrix_row, fd_module.f90:104-224) has its rows/
+// columns in lin2fgrid order: the nb = 2(a+b) cornerless boundary points first (faces
+// x1 x2 y1 y2), then the a*b interior points x-fastest.  Every boundary row r reads only
+// itself and two interior points along the inward normal:
+//     A(r,r) = i*kb + (8/3)/h,  A(r,p1) = -3/h,  A(r,p2) = (1/3)/h        (fd_module.f90:207-215)
+// so A_bb is diagonal and the boundary unknowns condense exactly.  With
+// d_r = A(r,r), c1 = -3/h, c2 = 1/(3h) and w_c = (8/3)/h^2 (the interior row next to boundary
+// point c couples to it with that weight, fd_module.f90:150-153):
+//     S      = A_ii - A_ib A_bb^-1 A_bi                       (a*b x a*b)
+//     A^-1   = [[ (I - A_bi A^-1_ib) / d ,  -A_bi S^-1 / d ],
+//               [ -S^-1 A_ib / d          ,   S^-1          ]]
+// The reference's leaf Robin-to-Robin map is R X with X = A^-1 [I; 0] and R the outgoing rows
+// sigma*u + tau*(8/3 u - 3 u_p1 + 1/3 u_p2)/h, sigma = -i*kb, tau = 1
+// (RTR_update, robin_tree_module.f90:683-713).  Row r of Y = R A^-1 is
+//     Y(r,:) = (sigma'_r / d_r) e_r + (2 i kb / d_r) (c1 A^-1(p1,:) + c2 A^-1(p2,:)),
+// sigma'_r = sigma + (8/3)/h, because sigma'_r - d_r = -2 i kb.  Y(:, 0:nb) is the leaf RtR,
+// Y(:, nb:n) maps an interior source to the outgoing data of the particular solution
+// (fd_leaf_solve + fd_outgoing_bc, fd_module.f90:390-513).
+//
+// The condensed interior operator S inherits the 5-point stencil of FD_matrix_row
+// (fd_module.f90:140-181): with the interior points ordered x-fastest (igrid2lin, fd_module.f90:835-841) it is block tridiagonal,
+// b blocks of a x a,
+//     S = tridiag(Lo_j, D_j, Up_j),  D_j tridiagonal,  Lo_j = diag(lam_j),  Up_j = diag(mu_j).
+// Block elimination without exchanges between blocks (the blocks are diagonally dominant
+// Laplacian blocks shifted by the potential; each block inverse pivots by |re|+|im|):
+//     Sig_1 = D_1,  Sig_j = D_j - Lo_j Sig_{j-1}^-1 Up_{j-1},       S = L U,
+//     L = [I; Lo_j Sig_{j-1}^-1 below],  U = [Sig_j; Up_j above].
+// The leaf factor keeps Sig_j^-1 (b a^2 values instead of the reference's (ab+nb)^2 LU) and
+// forms the Robin-to-Robin data Y = R A^-1 from Q = C S^-1, where row r of C is
+// c1 e_p1(r) + c2 e_p2(r) (the interior part of the outgoing row of RTR_update,
+// robin_tree_module.f90:699-713): Q^T = S^-T C^T by one block forward and one block backward
+// sweep with nb right-hand sides.  Then, by the row formula above,
+//     Y(r, nb+s) = f_r Q(r,s),   Y(r,c) = (sigma'_r/d_r) delta_rc - f_r (w_c/d_c) Q(r, p1(c)),
+//     f_r = 2 i kb / d_r.
+// The leaf solve applies A^-1 [g; f] (fd_leaf_solve + fd_leaf_update, fd_module.f90:390-566)
+// through the same block factors: t = f - A_ib A_bb^-1 g, S u_i = t, u_b = (g - A_bi u_i)/d.
+#include "rb_kernels.h"
+
+namespace rb {
+
+__device__ __forceinline__ void leaf_bpoint2(int a, int b, int r, int& axis, int& p1, int& p2) {
+    if (r < b) { axis = 0; p1 = r * a; p2 = r * a + 1; }
+    else if (r < 2 * b) { const int j = r - b; axis = 0; p1 = j * a + (a - 1); p2 = j * a + (a - 2); }
+    else if (r < 2 * b + a) { const int i = r - 2 * b; axis = 1; p1 = i; p2 = a + i; }
+    else { const int i = r - 2 * b - a; axis = 1; p1 = (b - 1) * a + i; p2 = (b - 2) * a + i; }
+}
+
+__device__ __forceinline__ void stencil1(int i, int a, double& wm, double& w0, double& wp) {
+    if (i == 1) { wm = 8.0 / 3.0; w0 = -4.0; wp = 4.0 / 3.0; }
+    else if (i == a) { wm = 4.0 / 3.0; w0 = -4.0; wp = 8.0 / 3.0; }
+    else { wm = 1.0; w0 = -2.0; wp = 1.0; }
+}
+
+// constants of one leaf's condensed stencil
+struct LeafConst {
+    double hx, hy, hx2, hy2;
+    z rdx, rdy;                 // 1 / d for x-face and y-face boundary points
+    double c1x, c2x, c1y, c2y;  // -3/h, 1/(3h)
+    double wbx, wby;            // (8/3)/h^2
+};
+
+__device__ __forceinline__ LeafConst leaf_const(const double* hh, int leaf, double kb) {
+    LeafConst c;
+    c.hx = hh[2 * leaf];
+    c.hy = hh[2 * leaf + 1];
+    c.hx2 = c.hx * c.hx;
+    c.hy2 = c.hy * c.hy;
+    c.rdx = zrcp(zmk((8.0 / 3.0) / c.hx, kb));
+    c.rdy = zrcp(zmk((8.0 / 3.0) / c.hy, kb));
+    c.c1x = -3.0 / c.hx; c.c2x = (1.0 / 3.0) / c.hx;
+    c.c1y = -3.0 / c.hy; c.c2y = (1.0 / 3.0) / c.hy;
+    c.wbx = (8.0 / 3.0) / c.hx2;
+    c.wby = (8.0 / 3.0) / c.hy2;
+    return c;
+}
+
+// entry (r, c) of the diagonal block D_j (grid row jj = j+1) of S
+__device__ __forceinline__ z block_d(const LeafConst& L, int a, int b, int jj, int r, int c, z k) {
+    const int i = r + 1;
+    double wxm, wx0, wxp, wym, wy0, wyp;
+    stencil1(i, a, wxm, wx0, wxp);
+    stencil1(jj, b, wym, wy0, wyp);
+    z v = zmk(0.0, 0.0);
+    if (c == r) {
+        v = zmk((k.x + wx0 / L.hx2) + wy0 / L.hy2, k.y);
+        if (i == 1 || i == a) v = zsub(v, zscale(L.wbx * L.c1x, L.rdx));
+        if (jj == 1 || jj == b) v = zsub(v, zscale(L.wby * L.c1y, L.rdy));
+    } else if (c == r + 1 && i < a) {
+        v = zmk(wxp / L.hx2, 0.0);
+        if (i == 1) v = zsub(v, zscale(L.wbx * L.c2x, L.rdx));
+    } else if (c == r - 1 && i > 1) {
+        v = zmk(wxm / L.hx2, 0.0);
+        if (i == a) v = zsub(v, zscale(L.wbx * L.c2x, L.rdx));
+    }
+    return v;
+}
+// Lo_j(i,i) = S(e, e-a) for grid row jj >= 2 and Up_j(i,i) = S(e, e+a) for jj <= b-1
+__device__ __forceinline__ z block_lo(const LeafConst& L, int b, int jj) {
+    double wm, w0, wp;
+    stencil1(jj, b, wm, w0, wp);
+    z v = zmk(wm / L.hy2, 0.0);
+    if (jj == b) v = zsub(v, zscale(L.wby * L.c2y, L.rdy));
+    return v;
+}
+__device__ __forceinline__ z block_up(const LeafConst& L, int b, int jj) {
+    double wm, w0, wp;
+    stencil1(jj, b, wm, w0, wp);
+    z v = zmk(wp / L.hy2, 0.0);
+    if (jj == 1) v = zsub(v, zscale(L.wby * L.c2y, L.rdy));
+    return v;
+}
+
+// In-place Gauss-Jordan inverse of an m x m column-major matrix in shared memory by the whole
+// CTA (partial pivoting by |re|+|im|, first maximum).  Returns false on an exactly zero pivot.
+__device__ bool cta_gj_invert(z* S, int m, z* fcol, int* ipiv, int* sp) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    bool ok = true;
+    for (int k = 0; k < m; ++k) {
+        if (tid < 32) {
+            double best = -1.0;
+            int bi = m;
+            for (int r = k + tid; r < m; r += 32) {
+                const double v = zabs1(S[r + k * m]);
+                if (v > best) { best = v; bi = r; }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ov = __shfl_down_sync(0xffffffffu, best, o);
+                const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+                if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+            }
+            if (tid == 0) { *sp = bi; ipiv[k] = bi; }
+        }
+        __syncthreads();
+        const int p = *sp;
+        if (p != k)
+            for (int c = tid; c < m; c += nt) {
+                const z t = S[k + c * m];
+                S[k + c * m] = S[p + c * m];
+                S[p + c * m] = t;
+            }
+        __syncthreads();
+        const z piv = S[k + k * m];
+        if (piv.x == 0.0 && piv.y == 0.0) ok = false;
+        const z pinv = zrcp(piv);
+        for (int i = tid; i < m; i += nt) fcol[i] = S[i + k * m];
+        __syncthreads();
+        for (int c = tid; c < m; c += nt) S[k + c * m] = (c == k) ? pinv : zmul(S[k + c * m], pinv);
+        __syncthreads();
+        for (int e = tid; e < m * m; e += nt) {
+            const int i = e % m, c = e / m;
+            if (i == k) continue;
+            const z f = fcol[i];
+            if (c == k) S[e] = zneg(zmul(f, pinv));
+            else zfms(S[e], f, S[k + c * m]);
+        }
+        __syncthreads();
+    }
+    for (int r = tid; r < m; r += nt)
+        for (int k = m - 1; k >= 0; --k) {
+            const int p = ipiv[k];
+            if (p != k) {
+                const z t = S[r + k * m];
+                S[r + k * m] = S[r + p * m];
+                S[r + p * m] = t;
+            }
+        }
+    __syncthreads();
+    return ok;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Leaf factor: Sig_j^-1 for every block and Y = R A^-1 (nb x n, ld nb).  Shared memory:
+// sig (a^2), sigp (a^2), v0, v1 (a x nb each), fcol (a), ipiv (a), sp.
+__global__ void __launch_bounds__(256) leaf_block_factor_kernel(LeafGeom g, const double* __restrict__ hh,
+                                                                const z* __restrict__ kv, z* __restrict__ sinv,
+                                                                z* __restrict__ Y, int* status) {
+    extern __shared__ z sm[];
+    const int leaf = blockIdx.x;
+    const int a = g.a, b = g.b, nb = g.nb, n = g.n, ab = a * b, aa = a * a;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    z* sig = sm;
+    z* sigp = sig + aa;
+    z* v0 = sigp + aa;
+    z* v1 = v0 + (size_t)a * nb;
+    z* fcol = v1 + (size_t)a * nb;
+    int* ipiv = reinterpret_cast<int*>(fcol + a);
+    int* sp = ipiv + a;
+    const LeafConst L = leaf_const(hh, leaf, g.kb);
+    const z* kl = kv + (size_t)leaf * ab;
+    z* Sl = sinv + (size_t)leaf * b * aa;
+    z* Yl = Y + (size_t)leaf * nb * n;
+    bool ok = true;
+
+    // ---- block LU: Sig_j^-1, j = 0..b-1 ------------------------------------------------------
+    for (int j = 0; j < b; ++j) {
+        const int jj = j + 1;
+        const z lam = jj > 1 ? block_lo(L, b, jj) : zmk(0.0, 0.0);
+        const z mup = jj > 1 ? block_up(L, b, jj - 1) : zmk(0.0, 0.0);
+        for (int e = tid; e < aa; e += nt) {
+            const int r = e % a, c = e / a;
+            z v = block_d(L, a, b, jj, r, c, kl[j * a + r]);
+            if (jj > 1) zfms(v, zmul(lam, mup), sigp[e]);
+            sig[e] = v;
+        }
+        __syncthreads();
+        ok &= cta_gj_invert(sig, a, fcol, ipiv, sp);
+        for (int e = tid; e < aa; e += nt) {
+            Sl[(size_t)j * aa + e] = sig[e];
+            sigp[e] = sig[e];
+        }
+        __syncthreads();
+    }
+
+    // ---- forward sweep of S^T Z = C^T: v_j = Sig_j^-T (c_j - Up_{j-1} v_{j-1}) ---------------------
+    // v_j (a x nb, ld a) is kept in shared memory and stored transposed into Y(:, nb + j*a + i).
+    z* vp = v0;
+    z* vc = v1;
+    for (int j = 0; j < b; ++j) {
+        const int jj = j + 1;
+        for (int e = tid; e < aa; e += nt) sig[e] = Sl[(size_t)j * aa + e];
+        const z mup = jj > 1 ? block_up(L, b, jj - 1) : zmk(0.0, 0.0);
+        __syncthreads();
+        for (int e = tid; e < a * nb; e += nt) {
+            const int i = e % a, r = e / a;
+            int ax, p1, p2;
+            leaf_bpoint2(a, b, r, ax, p1, p2);
+            const double hr = ax == 0 ? L.hx : L.hy;
+            const double c1 = -3.0 / hr, c2 = (1.0 / 3.0) / hr;
+            z acc = zmk(0.0, 0.0);
+            for (int q = 0; q < a; ++q) {
+                const int eq = j * a + q;
+                z rhs = zmk((eq == p1 ? c1 : 0.0) + (eq == p2 ? c2 : 0.0), 0.0);
+                if (jj > 1) zfms(rhs, mup, vp[q + r * a]);
+                zfma(acc, sig[q + i * a], rhs);       // (Sig^-T)(i,q) = Sig^-1(q,i)
+            }
+            vc[e] = acc;
+            Yl[r + (size_t)(nb + j * a + i) * nb] = acc;
+        }
+        __syncthreads();
+        z* t = vp; vp = vc; vc = t;
+    }
+    // ---- backward sweep: z_{j-1} = v_{j-1} - Sig_{j-1}^-T Lo_j z_j; z_{b-1} = v_{b-1} (in vp) -------
+    for (int j = b - 1; j >= 1; --j) {
+        const int jj = j + 1;              // grid row of block j
+        const z lam = block_lo(L, b, jj);
+        for (int e = tid; e < aa; e += nt) sig[e] = Sl[(size_t)(j - 1) * aa + e];
+        __syncthreads();
+        for (int e = tid; e < a * nb; e += nt) {
+            const int i = e % a, r = e / a;
+            z acc = Yl[r + (size_t)(nb + (j - 1) * a + i) * nb];
+            for (int q = 0; q < a; ++q) zfms(acc, sig[q + i * a], zmul(lam, vp[q + r * a]));
+            vc[e] = acc;
+            Yl[r + (size_t)(nb + (j - 1) * a + i) * nb] = acc;
+        }
+        __syncthreads();
+        z* t = vp; vp = vc; vc = t;
+    }
+    __syncthreads();
+    // ---- Y = R A^-1 from Q(r, s) = Z(s, r) = Y(r, nb+s) -------------------------------------------
+    for (int e = tid; e < nb * nb; e += nt) {
+        const int r = e % nb, c = e / nb;
+        int ax, p1, p2, axc, p1c, p2c;
+        leaf_bpoint2(a, b, r, ax, p1, p2);
+        leaf_bpoint2(a, b, c, axc, p1c, p2c);
+        const z rd = ax == 0 ? L.rdx : L.rdy;
+        const z f = zmul(zmk(0.0, 2.0 * g.kb), rd);
+        const z wd = axc == 0 ? zscale(L.wbx, L.rdx) : zscale(L.wby, L.rdy);
+        z v = zneg(zmul(zmul(f, wd), Yl[r + (size_t)(nb + p1c) * nb]));
+        if (c == r) {
+            const double hr = ax == 0 ? L.hx : L.hy;
+            v = zadd(v, zmul(zmk((8.0 / 3.0) / hr, -g.kb), rd));
+        }
+        Yl[e] = v;
+    }
+    __syncthreads();
+    for (int e = tid; e < nb * ab; e += nt) {
+        const int r = e % nb;
+        int ax, p1, p2;
+        leaf_bpoint2(a, b, r, ax, p1, p2);
+        const z f = zmul(zmk(0.0, 2.0 * g.kb), ax == 0 ? L.rdx : L.rdy);
+        Yl[(size_t)nb * nb + e] = zmul(f, Yl[(size_t)nb * nb + e]);
+    }
+    if (!ok && tid == 0) atomicOr(status, 1);
+}
+
+size_t leaf_block_factor_smem(const LeafGeom& g) {
+    return (2 * (size_t)g.a * g.a + 2 * (size_t)g.a * g.nb + g.a) * sizeof(z) + (g.a + 1) * sizeof(int) + 16;
+}
+
+cudaError_t leaf_block_factor(const LeafGeom& g, int nleaves, const double* h, const z* k, z* sinv, z* Y,
+                              int* status, cudaStream_t s) {
+    const size_t sh = leaf_block_factor_smem(g);
+    if (sh > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(leaf_block_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+        if (e != cudaSuccess) return e;
+    }
+    leaf_block_factor_kernel<<<nleaves, 256, sh, s>>>(g, h, k, sinv, Y, status);
+    note_launch();
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Leaf solve: u = A^-1 [g; f] for every leaf and right-hand side into sol [rhs][leaf][n].
+// RHS are processed in chunks of KC columns; shared memory: sig (a^2), w0, w1 (a x KC each).
+constexpr int LEAF_KC = 32;
+
+__global__ void __launch_bounds__(256) leaf_block_solve_kernel(LeafGeom g, int nleaves, int nrhs,
+                                                               const double* __restrict__ hh,
+                                                               const z* __restrict__ f, const z* __restrict__ gb,
+                                                               const z* __restrict__ sinv, z* __restrict__ sol) {
+    extern __shared__ z sm[];
+    const int leaf = blockIdx.x;
+    const int a = g.a, b = g.b, nb = g.nb, n = g.n, ab = a * b, aa = a * a;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    z* sig = sm;
+    z* w0 = sig + aa;
+    z* w1 = w0 + (size_t)a * LEAF_KC;
+    const LeafConst L = leaf_const(hh, leaf, g.kb);
+    const z* Sl = sinv + (size_t)leaf * b * aa;
+    const z wdx = zscale(L.wbx, L.rdx), wdy = zscale(L.wby, L.rdy);
+    for (int r0 = 0; r0 < nrhs; r0 += LEAF_KC) {
+        const int kc = min(LEAF_KC, nrhs - r0);
+        z* wp = w0;
+        z* wc = w1;
+        // forward: w_j = Sig_j^-1 (t_j - Lo_j w_{j-1}),  t = f - A_ib A_bb^-1 g
+        for (int j = 0; j < b; ++j) {
+            const int jj = j + 1;
+            for (int e = tid; e < aa; e += nt) sig[e] = Sl[(size_t)j * aa + e];
+            const z lam = jj > 1 ? block_lo(L, b, jj) : zmk(0.0, 0.0);
+            __syncthreads();
+            // right-hand side of block j into wc (t_j - Lo_j w_{j-1})
+            for (int e = tid; e < a * kc; e += nt) {
+                const int q = e % a, rc = e / a, rh = r0 + rc;
+                const int i = q + 1;
+                const z* gl = gb + ((size_t)leaf * nrhs + rh) * nb;
+                z t = f ? f[((size_t)rh * nleaves + leaf) * ab + j * a + q] : zmk(0.0, 0.0);
+                if (i == 1) zfms(t, wdx, gl[j]);
+                if (i == a) zfms(t, wdx, gl[b + j]);
+                if (jj == 1) zfms(t, wdy, gl[2 * b + q]);
+                if (jj == b) zfms(t, wdy, gl[2 * b + a + q]);
+                if (jj > 1) zfms(t, lam, wp[q + rc * a]);
+                wc[e] = t;
+            }
+            __syncthreads();
+            for (int e = tid; e < a * kc; e += nt) {
+                const int i = e % a, rc = e / a;
+                z acc = zmk(0.0, 0.0);
+                for (int q = 0; q < a; ++q) zfma(acc, sig[i + q * a], wc[q + rc * a]);
+                sol[((size_t)(r0 + rc) * nleaves + leaf) * n + nb + j * a + i] = acc;
+                wp[e] = acc;    // w_j becomes the previous block for j+1
+            }
+            __syncthreads();
+        }
+        // backward: x_{b-1} = w_{b-1} (in wp); x_j = w_j - Sig_j^-1 Up_j x_{j+1}
+        for (int j = b - 2; j >= 0; --j) {
+            const int jj = j + 1;
+            const z mu = block_up(L, b, jj);
+            for (int e = tid; e < aa; e += nt) sig[e] = Sl[(size_t)j * aa + e];
+            __syncthreads();
+            for (int e = tid; e < a * kc; e += nt) {
+                const int i = e % a, rc = e / a;
+                z* up = sol + ((size_t)(r0 + rc) * nleaves + leaf) * n + nb + j * a;
+                z acc = up[i];
+                for (int q = 0; q < a; ++q) zfms(acc, sig[i + q * a], zmul(mu, wp[q + rc * a]));
+                wc[e] = acc;
+                up[i] = acc;
+            }
+            __syncthreads();
+            z* t = wp; wp = wc; wc = t;
+        }
+        __syncthreads();
+        // boundary values u_b = (g - c1 u(p1) - c2 u(p2)) / d
+        for (int e = tid; e < nb * kc; e += nt) {
+            const int r = e % nb, rc = e / nb, rh = r0 + rc;
+            int ax, p1, p2;
+            leaf_bpoint2(a, b, r, ax, p1, p2);
+            const double h = ax == 0 ? L.hx : L.hy;
+            z* u = sol + ((size_t)rh * nleaves + leaf) * n;
+            z v = gb[((size_t)leaf * nrhs + rh) * nb + r];
+            v = zsub(v, zadd(zscale(-3.0 / h, u[nb + p1]), zscale((1.0 / 3.0) / h, u[nb + p2])));
+            u[r] = zmul(v, ax == 0 ? L.rdx : L.rdy);
+        }
+        __syncthreads();
+    }
+}
+
+cudaError_t leaf_block_solve(const LeafGeom& g, int nleaves, int nrhs, const double* h, const z* f, const z* gb,
+                             const z* sinv, z* sol, cudaStream_t s) {
+    const size_t sh = ((size_t)g.a * g.a + 2 * (size_t)g.a * LEAF_KC) * sizeof(z);
+    if (sh > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(leaf_block_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+        if (e != cudaSuccess) return e;
+    }
+    leaf_block_solve_kernel<<<nleaves, 256, sh, s>>>(g, nleaves, nrhs, h, f, gb, sinv, sol);
+    note_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace rb

@@ -5,8 +5,8 @@
 // count (solve), and launches the level-by-level stages on the handle's stream.
 //
 // Factor (robin_tree_factor -> compute_RTR, robin_tree_module.f90:96-185, 375-650):
-//   leaves:  S = A_ii - A_ib A_bb^-1 A_bi from the potential samples, S^-1 by Gauss-Jordan,
-//            Y = R A^-1 (RtR in its first nb columns)
+//   leaves:  block-tridiagonal factor of S = A_ii - A_ib A_bb^-1 A_bi from the potential
+//            samples and Y = R A^-1 (RtR in its first nb columns), one CTA per leaf (rb_leaf.cu)
 //   level l = L-1 .. 0, all nodes of the level in one launch per stage:
 //            inv(D), D = zeta I - T2_ii;  inv(S), S = zeta I - T1_ii - nu^2 inv(D)
 //            Y2R = inv(D) T2_iN;  Y1 = inv(S) [T1_iN, -nu Y2R];  Y2 = [0, Y2R] - nu inv(D) Y1
@@ -16,7 +16,7 @@
 //   forward:  leaf h = Y(:, nb:) f;  per level (g1_i, g2_i) = M^-1 (h1_i, h2_i) and the parent's
 //             h = h_N + T_Ni g_i
 //   backward: root g = boundary data; per level children's g_N from the parent, Tg = T_iN g_N,
-//             g_i += M^-1 Tg;  leaf u = A^-1 [g; f] through the condensed Schur inverse.
+//             g_i += M^-1 Tg;  leaf u = A^-1 [g; f] through the leaf's block factors.
 //   M^-1 (x1, x2): w = inv(D) x2; y1 = inv(S)(x1 - nu w); y2 = w - nu inv(D) y1 (apply_invm, :1252).
 #include <algorithm>
 #include <atomic>
@@ -90,7 +90,6 @@ struct rb_tree {
     z* gj_work = nullptr;
     int* gj_ipiv = nullptr;
     // factor launch batches
-    GJBatch gj_leaf;
     std::vector<GJBatch> gj_d, gj_s;
     std::vector<GemmBatch> fM1, fM2, fM3, fM4;
     bool factor_ready = false;
@@ -102,9 +101,8 @@ struct rb_tree {
     z* d_f = nullptr;
     std::vector<z*> hbuf, gbuf;      // per level 0..L
     z* tmp = nullptr;
-    z* tleaf = nullptr;
     z* sol = nullptr;
-    GemmBatch sL0, sL2;
+    GemmBatch sL0;
     std::vector<GemmBatch> sF12, sF3, sF4, sF5, sB1, sB23, sB4, sB5;
     std::vector<DevBuf> solve_bufs;
 
@@ -277,7 +275,7 @@ static int ensure_factor_storage(rb_tree* t) {
     if ((rc = alloc_n(t, t->bufs, 2 * (size_t)nl, &t->d_h))) return rc;
     RB_CK(cudaMemcpy(t->d_h, P.leaf_h.data(), 2 * nl * sizeof(double), cudaMemcpyHostToDevice));
     if ((rc = alloc_n(t, t->bufs, (size_t)nl * ab, &t->d_k))) return rc;
-    if ((rc = alloc_n(t, t->bufs, (size_t)nl * ab * ab, &t->leaf_sinv))) return rc;
+    if ((rc = alloc_n(t, t->bufs, (size_t)nl * b * a * a, &t->leaf_sinv))) return rc;
     if ((rc = alloc_n(t, t->bufs, (size_t)nl * nb * n, &t->leaf_Y))) return rc;
     if ((rc = alloc_n(t, t->bufs, 1, &t->d_status))) return rc;
     t->rtr.assign(L, nullptr);
@@ -300,8 +298,8 @@ static int ensure_factor_storage(rb_tree* t) {
     }
     if ((rc = alloc_n(t, t->bufs, ymax, &t->Y1))) return rc;
     if ((rc = alloc_n(t, t->bufs, ymax, &t->Y2))) return rc;
-    // Gauss-Jordan workspace: the largest batch (leaves or one level's nodes)
-    size_t wmax = (size_t)nl * (size_t)gj_workspace_elems(ab), imax = (size_t)nl * ab;
+    // Gauss-Jordan workspace: the largest batch of one level's nodes
+    size_t wmax = 1, imax = 1;
     for (int l = 0; l < L; ++l) {
         const PlanLevel& p = P.lv[l];
         wmax = std::max(wmax, (size_t)p.nnodes * (size_t)gj_workspace_elems(p.m));
@@ -313,17 +311,14 @@ static int ensure_factor_storage(rb_tree* t) {
     auto gj_descs = [&](z* base, long long stride, int ld, int count, int m) {
         std::vector<GJDesc> v(count);
         const long long ws = gj_workspace_elems(m);
-        const int nbw = gj_panel_width(m);
         for (int i = 0; i < count; ++i) {
             v[i].A = base + (long long)i * stride;
             v[i].ld = ld;
             v[i].ipiv = t->gj_ipiv + (long long)i * m;
-            v[i].Wm = t->gj_work + (long long)i * ws;
-            v[i].Zb = t->gj_work + (long long)i * ws + (long long)m * nbw;
+            v[i].Zb = t->gj_work + (long long)i * ws;
         }
         return v;
     };
-    if ((rc = upload_gj(t, t->bufs, gj_descs(t->leaf_sinv, (long long)ab * ab, ab, nl, ab), ab, t->gj_leaf))) return rc;
     t->gj_d.resize(L);
     t->gj_s.resize(L);
     t->fM1.resize(L); t->fM2.resize(L); t->fM3.resize(L); t->fM4.resize(L);
@@ -407,6 +402,11 @@ static int ensure_factor_storage(rb_tree* t) {
     } while (0)
 
 static double gj_flops(int m, int count) { return 8.0 * (double)m * m * m * count; }
+// arithmetic of one structured leaf factor: b block inverses (8 a^3 each) and two block sweeps
+// of S^T Z = C^T with nb right-hand sides (8 a^2 nb per block and sweep)
+static double leaf_flops(const LeafGeom& g) {
+    return 8.0 * g.a * g.a * g.a * g.b + 16.0 * g.a * g.a * (double)g.nb * g.b;
+}
 
 static int run_factor(rb_tree* t, const z* dk) {
     const Plan& P = t->P;
@@ -415,14 +415,9 @@ static int run_factor(rb_tree* t, const z* dk) {
     cudaStream_t s = t->stream;
     int rc;
     RB_CK(cudaMemsetAsync(t->d_status, 0, sizeof(int), s));
-    if ((rc = timer_begin(t, "leaf_schur"))) return rc;
-    RB_TIMED("leaf_schur", 0.0, leaf_schur(lg, nl, t->d_h, dk, t->leaf_sinv, s));
-    if ((rc = timer_end(t))) return rc;
-    if ((rc = timer_begin(t, "leaf_invert"))) return rc;
-    RB_TIMED("gj_invert", gj_flops(lg.a * lg.b, nl), gj_invert_batch(t->gj_leaf.d_desc, nl, lg.a * lg.b, t->d_status, s));
-    if ((rc = timer_end(t))) return rc;
-    if ((rc = timer_begin(t, "leaf_outgoing"))) return rc;
-    RB_TIMED("leaf_outgoing", 0.0, leaf_outgoing(lg, nl, t->d_h, t->leaf_sinv, t->leaf_Y, s));
+    if ((rc = timer_begin(t, "leaf_factor"))) return rc;
+    RB_TIMED("leaf_factor", leaf_flops(lg) * nl, leaf_block_factor(lg, nl, t->d_h, dk, t->leaf_sinv, t->leaf_Y,
+                                                                    t->d_status, s));
     if ((rc = timer_end(t))) return rc;
     static const char* lvl_names[] = {"merge_l0", "merge_l1", "merge_l2", "merge_l3", "merge_l4", "merge_l5",
                                       "merge_l6", "merge_l7", "merge_l8", "merge_l9", "merge_l10", "merge_l11",
@@ -465,7 +460,6 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
             if (l < L) tmax = std::max(tmax, (size_t)p.nnodes * 4 * p.m * k);
         }
         if ((rc = alloc_n(t, t->solve_bufs, tmax, &t->tmp))) return rc;
-        if ((rc = alloc_n(t, t->solve_bufs, (size_t)nl * k * ab, &t->tleaf))) return rc;
         if ((rc = alloc_n(t, t->solve_bufs, (size_t)k * nl * n, &t->sol))) return rc;
         t->cap_rhs = k;
     }
@@ -479,12 +473,6 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
                           zview(t->d_f + (long long)i * ab, (long long)nl * ab),
                           zout(t->hbuf[L] + (long long)i * nb * k, nb), one));
     if ((rc = upload_gemm(t, t->solve_bufs, v, t->sL0))) return rc;
-    v.clear();
-    for (int i = 0; i < nl; ++i)
-        v.push_back(gdesc(ab, k, ab, zview(t->leaf_sinv + (long long)i * ab * ab, ab),
-                          zview(t->tleaf + (long long)i * ab * k, ab),
-                          zout(t->sol + (long long)i * n + nb, (long long)nl * n), one));
-    if ((rc = upload_gemm(t, t->solve_bufs, v, t->sL2))) return rc;
     t->sF12.assign(L, GemmBatch()); t->sF3.assign(L, GemmBatch()); t->sF4.assign(L, GemmBatch());
     t->sF5.assign(L, GemmBatch()); t->sB1.assign(L, GemmBatch()); t->sB23.assign(L, GemmBatch());
     t->sB4.assign(L, GemmBatch()); t->sB5.assign(L, GemmBatch());
@@ -593,9 +581,7 @@ static int run_solve(rb_tree* t, int k) {
     }
     if ((rc = timer_end(t))) return rc;
     if ((rc = timer_begin(t, "leaf_recover"))) return rc;
-    RB_TIMED("sweep_aux", 0.0, leaf_condense_rhs(lg, nl, k, t->d_h, t->d_f, t->gbuf[L], t->tleaf, s));
-    RB_TIMED("zgemm", t->sL2.flops, launch_gemm_batch(t->sL2, s));
-    RB_TIMED("sweep_aux", 0.0, leaf_boundary_values(lg, nl, k, t->d_h, t->gbuf[L], t->sol, s));
+    RB_TIMED("leaf_solve", 0.0, leaf_block_solve(lg, nl, k, t->d_h, t->d_f, t->gbuf[L], t->leaf_sinv, t->sol, s));
     if ((rc = timer_end(t))) return rc;
     return RB_OK;
 }
@@ -645,7 +631,7 @@ int rb_tree_create(const rb_geom* geom, rb_tree** out) {
     if (t->budget > 0) {
         const Plan& Q = t->P;
         const double ab = (double)Q.leaf_a() * Q.leaf_b();
-        double need = (double)Q.nleaves() * (ab * ab + (double)Q.leaf_nb() * Q.leaf_n() + ab) * 16.0;
+        double need = (double)Q.nleaves() * (ab * Q.leaf_a() + (double)Q.leaf_nb() * Q.leaf_n() + ab) * 16.0;
         for (int l = 0; l < Q.L; ++l)
             need += (double)Q.lv[l].nnodes * ((double)Q.lv[l].nb * Q.lv[l].nb + 2.0 * Q.lv[l].m * Q.lv[l].m) * 16.0;
         if (need > (double)t->budget) {
@@ -888,6 +874,10 @@ int rb_tree_set_timing(rb_tree* t, int mode) {
 int rb_tree_stage_times(const rb_tree* tc, double* ms, double* flops, const char** names, int n) {
     rb_tree* t = const_cast<rb_tree*>(tc);
     if (!t) return RB_ERR_INVALID;
+    if (!t->timers.empty()) {      // entries of asynchronous calls: wait for them
+        if (t->stream) RB_CK(cudaStreamSynchronize(t->stream));
+        timers_collect(t);
+    }
     const int cnt = (int)t->stage_ms.size();
     for (int i = 0; i < std::min(n, cnt); ++i) {
         if (ms) ms[i] = t->stage_ms[i].ms;
