@@ -13,7 +13,8 @@
  *
  * Status codes: 0 on success, a negative RB_ERR_* value on failure; the message of
  * the last failure on a handle is returned by rb_last_error(handle), and
- * rb_last_error(NULL) reports the last failure of rb_tree_create on this thread.
+ * rb_last_error(NULL) reports the last failure of rb_tree_create (or of
+ * rb_leaf_rtr_noalloc) on this thread.
  * The reference stops the process instead ("stop '<message>'"); the messages below
  * carry the reference's wording where one exists.
  *
@@ -102,7 +103,8 @@ int rb_tree_create(const rb_geom* geom, rb_tree** out);
 /* Releases the handle and all its device memory. */
 int rb_tree_destroy(rb_tree* tree);
 
-/* Message of the last failure on `tree` (or of rb_tree_create on this thread when NULL). */
+/* Message of the last failure on `tree`; with NULL, of the last failed rb_tree_create or
+ * rb_leaf_rtr_noalloc on this thread. */
 const char* rb_last_error(const rb_tree* tree);
 
 int rb_tree_info(const rb_tree* tree, rb_info* info);
@@ -184,6 +186,35 @@ int rb_tree_get_rtr(const rb_tree* tree, int level, int node, double* out);
 
 /* Number of this library's kernels launched by the last factor and the last solve. */
 int rb_tree_launch_counts(const rb_tree* tree, int64_t* factor_launches, int64_t* solve_launches);
+
+/* Leaf Robin-to-Robin maps for callers that cannot allocate device memory.  No counterpart in
+ * the reference (whose leaf RtR is node%RtR after RTR_solve, robin_tree_module.f90:728-799; the
+ * maps this writes are those of rb_tree_factor's leaves, see rb_tree_get_rtr).
+ *
+ * Meant for callers that must not call cudaMalloc: a framework that owns the device's memory
+ * through its own pool (or has reserved it up front) and forbids allocations by libraries, or
+ * a latency-critical loop where cudaMalloc's implicit device synchronisation is unacceptable.
+ * This entry point allocates nothing and calls no allocating routine; its working memory is a
+ * file-scope device array of 32 MiB that every GPU holds from the library's load until exit.
+ *
+ *  a, b      leaf grid (ptbox) in x and y, each >= 3
+ *  kb        solve_opts%kb
+ *  d_h       device, 2*nleaves doubles: each leaf's (hx, hy)
+ *  d_k       device, nleaves*a*b complex: each leaf's potential at its interior cell centres
+ *            (x fastest), as rb_tree_factor's samples for one leaf
+ *  d_rtr     device, nleaves*nb*nb complex (nb = 2(a+b)) output: each leaf's RtR, column-major,
+ *            faces x1 x2 y1 y2 -- what rb_tree_get_rtr(tree, L, i) returns for a factored tree
+ *  stream    cudaStream_t to run on (NULL = the default stream); the call returns after the
+ *            stream's work is done
+ * Limit: nleaves * (b*a^2 + nb*(nb + a*b)) * 16 + 256 bytes of scratch must fit 32 MiB (102 leaves
+ * of 16x16); larger batches are refused with RB_ERR_INVALID and a message giving the limit.
+ * The first call on a device looks up the array's address (cudaGetSymbolAddress) with that device
+ * current; make that first call before starting any stream capture.  All calls share the array
+ * and it keeps the previous call's contents: calls whose GPU work overlaps (several streams or
+ * host threads on one device) race on it.  Errors: RB_ERR_INVALID, RB_ERR_CUDA, RB_ERR_NUMERIC
+ * (zero pivot); the message is rb_last_error(NULL). */
+int rb_leaf_rtr_noalloc(int a, int b, double kb, const double* d_h, const double* d_k, int nleaves,
+                        double* d_rtr, void* stream);
 
 #ifdef __cplusplus
 }

@@ -41,6 +41,7 @@ EXPORTS = [
     "rb_tree_factor", "rb_tree_factor_device", "rb_tree_solve", "rb_tree_solve_device",
     "rb_get_solution", "rb_get_solution_device", "rb_tree_times", "rb_tree_stream",
     "rb_tree_set_timing", "rb_tree_stage_times", "rb_tree_clear_stage_times", "rb_tree_level_shape", "rb_tree_get_rtr", "rb_tree_launch_counts",
+    "rb_leaf_rtr_noalloc",
 ]
 
 
@@ -102,6 +103,7 @@ def _load():
         "rb_tree_level_shape": (C.c_int, [P, C.c_int, C.POINTER(C.c_int32)]),
         "rb_tree_get_rtr": (C.c_int, [P, C.c_int, C.c_int, D]),
         "rb_tree_launch_counts": (C.c_int, [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
+        "rb_leaf_rtr_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_double, P, P, C.c_int, P, P]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

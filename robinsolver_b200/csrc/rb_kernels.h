@@ -8,6 +8,8 @@ namespace rb {
 // ---- launch accounting --------------------------------------------------------------------------
 void note_launch();
 long long launch_count();
+// message returned by rb_last_error(NULL) on this thread
+void set_thread_error(const char* msg);
 
 // ---- batched GEMM ---------------------------------------------------------------------------------
 cudaError_t launch_gemm_batch(const GemmBatch& b, cudaStream_t s);

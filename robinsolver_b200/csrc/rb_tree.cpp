@@ -35,9 +35,13 @@ void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 }  // namespace rb
 
-using namespace rb;
-
 static thread_local std::string g_create_error;
+
+namespace rb {
+void set_thread_error(const char* msg) { g_create_error = msg ? msg : ""; }
+}  // namespace rb
+
+using namespace rb;
 
 namespace {
 
