@@ -42,7 +42,6 @@ ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "Factor time + solves/s on 1024² 2D Helmholtz, mixed vs FP64 GPU @1e-10; p99 ms"
-CONFIG_ID = 4
 
 
 def parse():
@@ -51,19 +50,30 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--nrhs", type=int, default=32)
+    ap.add_argument("--nrhs", type=int, default=None, help="right-hand sides per step (default: the config's)")
+    ap.add_argument("--config", type=int, default=4, choices=[1, 2, 4],
+                    help="workload: 4 = 1024^2 L=12 (the headline), 2 = 512^2 L=10, 1 = 64^2 L=4 (profiling/tests)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
 
 
-def config_dict(nrhs):
+WORKLOAD_TEXT = {
+    4: "2D Helmholtz 1024^2, L=12 (4096 leaves of 16x16), kb=200, 100-bump potential, 0.002i*kb damping",
+    2: "2D Helmholtz 512^2, L=10 (1024 leaves of 16x16), kb=100, 40-bump potential, 0.005i*kb damping",
+    1: "2D Helmholtz 64^2, L=4 (16 leaves of 16x16), kb=20, 5-bump potential, 0.01i*kb damping",
+}
+
+
+def config_dict(cfg, nrhs):
+    from robinsolver_b200 import workloads as W
+    c = W.CONFIGS[cfg]
     return {
-        "workload": f"2D Helmholtz 1024^2, L=12 (4096 leaves of 16x16), kb=200, 100-bump potential, "
-                    f"0.002i*kb damping, impedance boundary; per step: factor + {nrhs} plane-wave RHS "
-                    f"batched solve + get_solution",
-        "grid": 1024, "L": 12, "leaf": "16x16", "nrhs": nrhs, "precision": "fp64",
-        "l2": "no flush: per-step working set ~13 GB and inputs 0.55 GB, both larger than L2 (126 MB)",
+        "workload": f"{WORKLOAD_TEXT[cfg]}, impedance boundary; per step: factor + {nrhs} "
+                    f"{'plane-wave' if cfg == 4 else 'point-source/plane-wave'} RHS batched solve + get_solution",
+        "grid": c["N"], "L": c["L"], "leaf": "16x16", "nrhs": nrhs, "precision": "fp64",
+        "l2": "no flush: per-step working set and inputs larger than L2 (126 MB)" if cfg != 1
+              else "small case: fits in L2",
     }
 
 
@@ -163,25 +173,26 @@ def reference_arm(args):
     if rank != 0:
         return 0
     from robinsolver_b200 import workloads as W
-    wl = W.make_workload(CONFIG_ID, nrhs=args.nrhs)
+    nrhs = args.nrhs or W.CONFIGS[args.config]["nrhs"]
+    wl = W.make_workload(args.config, nrhs=nrhs)
     threads = os.cpu_count() or 1
     for _ in range(args.warmup):
-        cpu_reference_step_seconds(wl, args.nrhs, threads)
+        cpu_reference_step_seconds(wl, nrhs, threads)
     steps = []
     t_wall = 0.0
     for _ in range(args.steps):
         t0 = time.perf_counter()
-        step, fac, sol = cpu_reference_step_seconds(wl, args.nrhs, threads)
+        step, fac, sol = cpu_reference_step_seconds(wl, nrhs, threads)
         t_wall += time.perf_counter() - t0
         steps.append((step, fac, sol))
     tot = sum(s[0] for s in steps)
-    value = args.nrhs * len(steps) / tot
+    value = nrhs * len(steps) / tot
     ms = 1e3 * tot / len(steps)
     out = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "RHS/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "complex128", "data": "synthetic (seeded)",
-        "config": config_dict(args.nrhs),
+        "config": config_dict(args.config, nrhs),
         "factor_ms": 1e3 * np.mean([s[1] for s in steps]),
         "solve_ms_per_rhs": 1e3 * np.mean([s[2] for s in steps]),
         "cpu_baseline": {"value": value, "unit": "RHS/s", "cores": threads, "kind": "port",
@@ -298,8 +309,8 @@ def our_arm(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
-    nrhs = args.nrhs
-    wl = W.make_workload(CONFIG_ID, nrhs=nrhs)
+    nrhs = args.nrhs or W.CONFIGS[args.config]["nrhs"]
+    wl = W.make_workload(args.config, nrhs=nrhs)
     T = rb.robin_tree()
     T.bndry_params = wl.bndry_params
     op = rb.elliptic_operator(d=2, domain=wl.domain, k=wl.potential)
@@ -437,7 +448,7 @@ def our_arm(args):
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
             "data": "synthetic (seeded potential and plane waves, no dataset)",
-            "config": config_dict(nrhs),
+            "config": config_dict(args.config, nrhs),
             "factor_ms": factor_ms, "solve_ms": solve_ms,
             "solves_per_s_resident": nrhs / (solve_ms * 1e-3),
             "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),

@@ -58,6 +58,7 @@ extern "C" {
 /* ---- flags in rb_geom.flags ----------------------------------------------------------------- */
 #define RB_FLAG_SKIP_ROOT_RTR 1   /* do not form the root's own RtR (the solve never reads it)         */
 #define RB_FLAG_VERBOSE       2   /* print the reference's progress lines to stdout                   */
+#define RB_FLAG_NO_GRAPHS     4   /* launch every kernel directly instead of replaying CUDA graphs     */
 
 typedef struct rb_tree rb_tree;
 
@@ -128,7 +129,10 @@ int rb_tree_sample_points(const rb_tree* tree, int which, double* xyz);
 
 /* robin_tree%factor(L, op, opts) (robin_tree_module.f90:96-185) with the potential already
  * sampled: `k_centres` = nleaves*a*b complex values at RB_POINTS_POTENTIAL (host memory).
- * Blocks until the factorization is done; robin_tree%f_time is set from device events. */
+ * Blocks until the factorization is done; robin_tree%f_time is set from device events.
+ * The first factorization of a handle launches its kernels directly; the second captures the
+ * (fixed) launch sequence into a CUDA graph that later calls replay (RB_FLAG_NO_GRAPHS turns
+ * this off; timing modes 1 and 2 launch directly).  The same holds for the solve, per RHS count. */
 int rb_tree_factor(rb_tree* tree, const double* k_centres, int precision);
 
 /* As rb_tree_factor, with `d_k_centres` already in device memory.  Asynchronous on the

@@ -34,6 +34,7 @@ RB_POINTS_SOLUTION = 3
 
 RB_FLAG_SKIP_ROOT_RTR = 1
 RB_FLAG_VERBOSE = 2
+RB_FLAG_NO_GRAPHS = 4
 
 # every entry point include/robin_b200.h declares
 EXPORTS = [

@@ -98,6 +98,9 @@ struct GemmBatch {
     int count = 0;
     int max_m = 0, max_n = 0, max_k = 0;
     double flops = 0.0;   // 8*m*n*k summed
+    // DFMA kernels only: every DFMA tile shape accumulates an element's k-sum in the same order,
+    // so results do not depend on the batch's sizes (used for the solve, whose n = RHS count)
+    bool fixed_order = false;
 };
 
 }  // namespace rb

@@ -7,6 +7,10 @@
 // and the epilogue instead of in copy kernels.
 //
 // FP64 has no tcgen05 kind; the arithmetic is DFMA with register tiling (rb_gemm_tile.cuh).
+#include <cstdlib>
+#include <cstring>
+
+#include "rb_gemm_dmma.cuh"
 #include "rb_gemm_tile.cuh"
 #include "rb_kernels.h"
 
@@ -24,6 +28,50 @@ zgemm_desc_kernel(const GemmDesc* __restrict__ descs) {
     }
     __syncthreads();
     zgemm_tile<BM, BN, TM, TN, BK>(sd, blockIdx.x);
+}
+
+template <int BM, int BN, int WM, int WN>
+__global__ void __launch_bounds__(32 * WM * WN, 1) zgemm_dmma_kernel(const GemmDesc* __restrict__ descs) {
+    extern __shared__ z dmma_smem[];
+    __shared__ GemmDesc sd;
+    {
+        const unsigned long long* src = reinterpret_cast<const unsigned long long*>(descs + blockIdx.y);
+        unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sd);
+        for (int w = threadIdx.x; w < (int)(sizeof(GemmDesc) / 8); w += 32 * WM * WN) dst[w] = src[w];
+    }
+    __syncthreads();
+    zgemm_tile_dmma<BM, BN, WM, WN>(sd, blockIdx.x, dmma_smem);
+}
+
+template <int BM, int BN, int WM, int WN>
+static cudaError_t launch_dmma(const GemmBatch& b, cudaStream_t s) {
+    using Cfg = DmmaCfg<BM, BN, WM, WN>;
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(zgemm_dmma_kernel<BM, BN, WM, WN>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    const int tiles = ((b.max_m + BM - 1) / BM) * ((b.max_n + BN - 1) / BN);
+    for (int off = 0; off < b.count; off += 65535) {
+        const int cnt = (b.count - off) < 65535 ? (b.count - off) : 65535;
+        dim3 grid(tiles, cnt);
+        zgemm_dmma_kernel<BM, BN, WM, WN><<<grid, Cfg::NT, Cfg::SMEM_BYTES, s>>>(b.d_desc + off);
+        note_launch();
+    }
+    return cudaGetLastError();
+}
+
+// GEMM engine for the large problems: FP64 tensor-core MMA (default) or DFMA register tiles
+// (RB_GEMM_ENGINE=dfma, read once; a tuning knob for comparisons)
+static bool use_dmma() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = std::getenv("RB_GEMM_ENGINE");
+        v = (e && std::strcmp(e, "dfma") == 0) ? 0 : 1;
+    }
+    return v == 1;
 }
 
 template <int BM, int BN, int TM, int TN, int BK, int MINB>
@@ -45,6 +93,13 @@ cudaError_t launch_gemm_batch(const GemmBatch& b, cudaStream_t s) {
     const int mm = b.max_m, nn = b.max_n;
     if (mm <= 16 && nn <= 16) return launch_cfg<16, 16, 2, 2, 8, 8>(b, s);
     if (mm <= 32 || nn <= 32) return launch_cfg<32, 32, 4, 2, 8, 4>(b, s);
+    const bool big = mm >= 256 && nn >= 128 && (long long)b.count * ((mm + 127) / 128) * ((nn + 63) / 64) >= 148;
+    if (use_dmma() && !b.fixed_order) {
+        if (big) return launch_dmma<128, 64, 4, 2>(b, s);
+        return launch_dmma<64, 64, 2, 4>(b, s);
+    }
+    // large problems: 8x4 complex register tile per thread (1.5 B of shared memory per DFMA)
+    if (big) return launch_cfg<128, 64, 8, 4, 4, 1>(b, s);
     return launch_cfg<64, 64, 4, 4, 8, 1>(b, s);
 }
 

@@ -12,12 +12,11 @@
 //      unblocked elimination on the panel (pivot search below the diagonal, row exchange,
 //      scaling, elimination of every other row), leaving the accumulated transform W in the
 //      panel columns;
-//   2. gj_swapcopy: applies the panel's row exchanges to every other column and copies the
-//      panel rows Z = A[P, rest];
-//   3. gj_update: A[i, rest] += W[i,:] Z for rows outside the panel and A[P, rest] = W_P Z for
-//      the panel rows, one GEMM on the shared tile engine.  (Writing the panel rows as
-//      Z + (W_P - I) Z instead cancels catastrophically: W_P's diagonal holds the reciprocal
-//      pivots, ~h^2 for the FD matrices here.)
+//   2. gj_apply: for every other column, applies the panel's row exchanges and then
+//      A[i, rest] += W[i,:] Z for rows outside the panel and A[P, rest] = W_P Z for the panel
+//      rows, Z = A[P, rest] after the exchanges.  (Writing the panel rows as Z + (W_P - I) Z
+//      instead cancels catastrophically: W_P's diagonal holds the reciprocal pivots, ~h^2 for
+//      the FD matrices here.)
 // After the last panel the column exchanges are undone in reverse order (gj_unscramble).
 #include "rb_gemm_tile.cuh"
 #include "rb_kernels.h"
@@ -26,14 +25,11 @@ namespace rb {
 
 int gj_panel_width(int m) {
     if (m <= GJ_SMALL_MAX) return 0;
-    if (m <= 256) return 16;
+    if (m <= 512) return 16;
     return 8;
 }
 
-long long gj_workspace_elems(int m) {
-    const int nb = gj_panel_width(m);
-    return nb == 0 ? 0 : (long long)m * nb;
-}
+long long gj_workspace_elems(int m) { return 0; }
 
 // warp argmax: larger value wins, equal values go to the smaller index
 __device__ __forceinline__ void argmax_warp(double& v, int& i) {
@@ -122,10 +118,14 @@ __global__ void __launch_bounds__(256) gj_small_kernel(const GJDesc* __restrict_
 template <int NB, int MAXT>
 __global__ void __launch_bounds__(MAXT) gj_panel_kernel(const GJDesc* __restrict__ descs, int m,
                                                         int k0, int nbk, int* status) {
-    __shared__ z xa[NB], xb[NB], prow[NB];
-    __shared__ double wv[32];
-    __shared__ int wi[32];
-    __shared__ int s_p;
+    // two block barriers per column: (1) per-warp pivot candidates, (2) the scaled pivot row and
+    // the displaced row.  Every warp reduces the 32 candidates itself, so the pivot index needs no
+    // extra barrier; the holder of the pivot row publishes it already scaled, the holder of row c
+    // publishes its row, and after barrier (2) row c takes the pivot row while the pivot's old
+    // row takes row c's values and is eliminated like any other row.
+    __shared__ z xb[2][NB], prow[2][NB];
+    __shared__ double wv[2][32];
+    __shared__ int wi[2][32];
     const GJDesc g = descs[blockIdx.x];
     const int r = threadIdx.x;
     const bool own = r < m;
@@ -139,53 +139,42 @@ __global__ void __launch_bounds__(MAXT) gj_panel_kernel(const GJDesc* __restrict
     for (int kk = 0; kk < NB; ++kk) {
         if (kk >= nbk) break;
         const int c = k0 + kk;
+        const int sb = kk & 1;           // alternate buffers so that barrier (1) of the next column
+                                         // also orders this column's reads of prow/xb
         double v = (own && r >= c) ? zabs1(row[kk]) : -1.0;
         int idx = own ? r : 0x7fffffff;
         argmax_warp(v, idx);
-        if (lane == 0) { wv[warp] = v; wi[warp] = idx; }
-        __syncthreads();
-        if (warp == 0) {
-            v = lane < nwarps ? wv[lane] : -1.0;
-            idx = lane < nwarps ? wi[lane] : 0x7fffffff;
-            argmax_warp(v, idx);
-            if (lane == 0) s_p = idx;
-        }
-        __syncthreads();
-        const int p = s_p;
-        if (p != c) {
-            if (r == p)
-#pragma unroll
-                for (int j = 0; j < NB; ++j) xa[j] = row[j];
-            if (r == c)
-#pragma unroll
-                for (int j = 0; j < NB; ++j) xb[j] = row[j];
-        }
-        __syncthreads();
-        if (p != c) {
-            if (r == c)
-#pragma unroll
-                for (int j = 0; j < NB; ++j) row[j] = xa[j];
-            if (r == p)
-#pragma unroll
-                for (int j = 0; j < NB; ++j) row[j] = xb[j];
-        }
-        if (r == c) {
+        if (lane == 0) { wv[sb][warp] = v; wi[sb][warp] = idx; }
+        __syncthreads();                                   // (1)
+        v = lane < nwarps ? wv[sb][lane] : -1.0;
+        idx = lane < nwarps ? wi[sb][lane] : 0x7fffffff;
+        argmax_warp(v, idx);
+        const int p = __shfl_sync(0xffffffffu, idx, 0);
+        if (r == p) {
             if (zis0(row[kk])) bad = true;
             const z pinv = zrcp(row[kk]);
 #pragma unroll
-            for (int j = 0; j < NB; ++j) {
-                row[j] = (j == kk) ? pinv : zmul(row[j], pinv);
-                prow[j] = row[j];
-            }
+            for (int j = 0; j < NB; ++j) prow[sb][j] = (j == kk) ? pinv : zmul(row[j], pinv);
             g.ipiv[c] = p;
         }
-        __syncthreads();
-        if (own && r != c) {
+        if (r == c && p != c) {
+#pragma unroll
+            for (int j = 0; j < NB; ++j) xb[sb][j] = row[j];
+        }
+        __syncthreads();                                   // (2)
+        if (r == c) {
+#pragma unroll
+            for (int j = 0; j < NB; ++j) row[j] = prow[sb][j];
+        } else if (own) {
+            if (r == p) {
+#pragma unroll
+                for (int j = 0; j < NB; ++j) row[j] = xb[sb][j];
+            }
             const z f = row[kk];
 #pragma unroll
             for (int j = 0; j < NB; ++j)
-                if (j != kk) zfms(row[j], f, prow[j]);
-            row[kk] = zneg(zmul(f, prow[kk]));
+                if (j != kk) zfms(row[j], f, prow[sb][j]);
+            row[kk] = zneg(zmul(f, prow[sb][kk]));
         }
     }
     if (own) {
@@ -198,50 +187,53 @@ __global__ void __launch_bounds__(MAXT) gj_panel_kernel(const GJDesc* __restrict
     if (bad) atomicOr(status, 1);
 }
 
-// exchange rows of every non-panel column and copy the panel rows into Z (nbk x (m - nbk))
-__global__ void gj_swapcopy_kernel(const GJDesc* __restrict__ descs, int m, int k0, int nbk) {
+// Applies one panel to the other columns: CW whole columns per CTA are staged in shared memory,
+// the panel's row exchanges are applied there, and the CTA writes
+//     A[i, j] + W[i,:] Z[:, j]   for rows i outside the panel,   W[i,:] Z[:, j]   for panel rows,
+// with Z = the (exchanged) panel rows of its own columns and W = the panel columns of A.  A CTA
+// owns whole columns, so no other CTA reads what it overwrites.
+template <int CW, int NBMAX>
+__global__ void __launch_bounds__(256) gj_apply_kernel(const GJDesc* __restrict__ descs, int m, int k0, int nbk) {
+    extern __shared__ z cols[];                 // m x CW, column-major (ld m)
     const GJDesc g = descs[blockIdx.y];
-    const int jl = blockIdx.x * blockDim.x + threadIdx.x;
-    if (jl >= m - nbk) return;
-    const int col = jl < k0 ? jl : jl + nbk;
-    z* a = g.A + (long long)col * g.ld;
-    for (int kk = 0; kk < nbk; ++kk) {
-        const int c = k0 + kk;
-        const int p = g.ipiv[c];
-        if (p != c) {
-            const z t = a[c];
-            a[c] = a[p];
-            a[p] = t;
-        }
-    }
-    for (int kk = 0; kk < nbk; ++kk) g.Zb[kk + (long long)jl * nbk] = a[k0 + kk];
-}
-
-template <int BM, int BN, int TM, int TN, int BK>
-__global__ void __launch_bounds__((BM / TM) * (BN / TN), 1)
-gj_update_kernel(const GJDesc* __restrict__ descs, int m, int k0, int nbk) {
-    __shared__ GemmDesc sd;
-    if (threadIdx.x == 0) {
-        const GJDesc g = descs[blockIdx.y];
-        sd.A = zview(g.A + (long long)k0 * g.ld, g.ld);   // the panel columns hold W
-        sd.B = zview(g.Zb, nbk);
-        sd.C = zview(g.A, g.ld);
-        sd.C.cs = k0;
-        sd.C.cl = nbk;
-        sd.D = zout(g.A, g.ld);
-        sd.D.cs = k0;
-        sd.D.cl = nbk;
-        sd.alpha = zmk(1.0, 0.0);
-        sd.beta = zmk(1.0, 0.0);
-        sd.m = m;
-        sd.n = m - nbk;
-        sd.k = nbk;
-        sd.nobeta_r0 = k0;          // panel rows are overwritten with W_P Z
-        sd.nobeta_r1 = k0 + nbk;
-        sd.pad = 0;
+    const int rest = m - nbk;
+    const int j0 = blockIdx.x * CW;
+    const int ncol = min(CW, rest - j0);
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int e = tid; e < m * ncol; e += nt) {
+        const int r = e % m, q = e / m;
+        const int jl = j0 + q;
+        const int col = jl < k0 ? jl : jl + nbk;
+        cols[r + q * m] = g.A[r + (long long)col * g.ld];
     }
     __syncthreads();
-    zgemm_tile<BM, BN, TM, TN, BK>(sd, blockIdx.x);
+    // the panel's exchanges, in order (each thread owns columns)
+    if (tid < ncol)
+        for (int kk = 0; kk < nbk; ++kk) {
+            const int c = k0 + kk, p = g.ipiv[c];
+            if (p != c) {
+                const z t = cols[c + tid * m];
+                cols[c + tid * m] = cols[p + tid * m];
+                cols[p + tid * m] = t;
+            }
+        }
+    __syncthreads();
+    for (int r = tid; r < m; r += nt) {
+        z w[NBMAX];
+#pragma unroll
+        for (int kk = 0; kk < NBMAX; ++kk)
+            w[kk] = kk < nbk ? g.A[r + (long long)(k0 + kk) * g.ld] : zmk(0.0, 0.0);
+        const bool in_panel = r >= k0 && r < k0 + nbk;
+        for (int q = 0; q < ncol; ++q) {
+            z v = in_panel ? zmk(0.0, 0.0) : cols[r + q * m];
+#pragma unroll
+            for (int kk = 0; kk < NBMAX; ++kk)
+                if (kk < nbk) zfma(v, w[kk], cols[k0 + kk + q * m]);
+            const int jl = j0 + q;
+            const int col = jl < k0 ? jl : jl + nbk;
+            g.A[r + (long long)col * g.ld] = v;
+        }
+    }
 }
 
 __global__ void gj_unscramble_kernel(const GJDesc* __restrict__ descs, int m) {
@@ -262,18 +254,22 @@ template <int NB, int MAXT>
 static cudaError_t gj_blocked(const GJDesc* d, int count, int m, int* st, cudaStream_t s) {
     const int threads = ((m + 31) / 32) * 32;
     if (threads > MAXT) return cudaErrorInvalidValue;
+    constexpr int CW = 8;
+    const size_t sh = (size_t)m * CW * sizeof(z);
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(gj_apply_kernel<CW, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)(1024 * CW * sizeof(z)));
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
     for (int k0 = 0; k0 < m; k0 += NB) {
         const int nbk = (m - k0) < NB ? (m - k0) : NB;
         gj_panel_kernel<NB, MAXT><<<count, threads, 0, s>>>(d, m, k0, nbk, st);
         note_launch();
         const int rest = m - nbk;
         if (rest > 0) {
-            gj_swapcopy_kernel<<<dim3((rest + 127) / 128, count), 128, 0, s>>>(d, m, k0, nbk);
-            note_launch();
-            constexpr int BM = 64, BN = 64, TM = 4, TN = 4, BK = 8;
-            const int tiles = ((m + BM - 1) / BM) * ((rest + BN - 1) / BN);
-            gj_update_kernel<BM, BN, TM, TN, BK><<<dim3(tiles, count), (BM / TM) * (BN / TN), 0, s>>>(
-                d, m, k0, nbk);
+            gj_apply_kernel<CW, NB><<<dim3((rest + CW - 1) / CW, count), 256, sh, s>>>(d, m, k0, nbk);
             note_launch();
         }
     }
@@ -298,7 +294,7 @@ cudaError_t gj_invert_batch(const GJDesc* d_desc, int count, int m, int* d_statu
         return cudaGetLastError();
     }
     if (m <= 256) return gj_blocked<16, 256>(d_desc, count, m, d_status, s);
-    if (m <= 512) return gj_blocked<8, 512>(d_desc, count, m, d_status, s);
+    if (m <= 512) return gj_blocked<16, 512>(d_desc, count, m, d_status, s);
     if (m <= 1024) return gj_blocked<8, 1024>(d_desc, count, m, d_status, s);
     return cudaErrorInvalidValue;
 }

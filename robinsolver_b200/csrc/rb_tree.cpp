@@ -33,6 +33,7 @@ namespace rb {
 static std::atomic<long long> g_launches{0};
 void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
+static void g_launches_add(long long d) { g_launches.fetch_add(d, std::memory_order_relaxed); }
 }  // namespace rb
 
 static thread_local std::string g_create_error;
@@ -119,6 +120,17 @@ struct rb_tree {
     int ev_used = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     int64_t factor_launches = 0, solve_launches = 0;
+
+    // CUDA graphs: the factor and solve launch sequences are fixed per tree (and per RHS count),
+    // so after one direct run each is captured once and replayed
+    bool graphs = true;
+    int factor_runs = 0;
+    cudaGraphExec_t gx_factor = nullptr;
+    long long gx_factor_launches = 0;
+    int solve_runs = 0;
+    cudaGraphExec_t gx_solve = nullptr;
+    int gx_solve_rhs = 0;
+    long long gx_solve_launches = 0;
 };
 
 // ---------------------------------------------------------------------------------------------------
@@ -265,6 +277,48 @@ static void timers_collect(rb_tree* t) {
     }
     t->timers.clear();
     t->ev_used = 0;
+}
+
+static void drop_graph(cudaGraphExec_t& g) {
+    if (g) cudaGraphExecDestroy(g);
+    g = nullptr;
+}
+
+// runs `body` directly, or captures it once into `gx` and replays it; `launches` receives the
+// number of kernels the sequence launches
+template <class F>
+static int run_graphed(rb_tree* t, cudaGraphExec_t& gx, long long& gx_launches, int& runs, F body) {
+    if (!t->graphs || t->timing != 0 || runs == 0) {
+        ++runs;
+        return body();
+    }
+    if (!gx) {
+        const long long l0 = launch_count();
+        RB_CK(cudaStreamBeginCapture(t->stream, cudaStreamCaptureModeThreadLocal));
+        const int rc = body();
+        cudaGraph_t g = nullptr;
+        const cudaError_t e = cudaStreamEndCapture(t->stream, &g);
+        if (rc || e != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();
+            if (rc) return rc;
+            t->err = std::string("CUDA graph capture failed: ") + cudaGetErrorString(e);
+            return RB_ERR_CUDA;
+        }
+        const cudaError_t ei = cudaGraphInstantiate(&gx, g, 0);
+        cudaGraphDestroy(g);
+        if (ei != cudaSuccess) {
+            gx = nullptr;
+            t->err = std::string("CUDA graph instantiation failed: ") + cudaGetErrorString(ei);
+            return RB_ERR_CUDA;
+        }
+        gx_launches = launch_count() - l0;
+        g_launches_add(-gx_launches);      // captured, not yet launched
+    }
+    RB_CK(cudaGraphLaunch(gx, t->stream));
+    g_launches_add(gx_launches);
+    ++runs;
+    return RB_OK;
 }
 
 // ---------------------------------------------------------------------------------------------------
@@ -449,6 +503,8 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
     const int L = P.L, nl = P.nleaves(), ab = P.leaf_a() * P.leaf_b(), nb = P.leaf_nb(), n = P.leaf_n();
     int rc;
     if (nrhs > t->cap_rhs) {
+        drop_graph(t->gx_solve);
+        t->gx_solve_rhs = 0;
         free_list(t, t->solve_bufs);
         t->built_rhs = 0;
         const int k = nrhs;
@@ -468,6 +524,8 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
         t->cap_rhs = k;
     }
     if (t->built_rhs == nrhs) return RB_OK;
+    drop_graph(t->gx_solve);
+    t->gx_solve_rhs = 0;
     // descriptor batches for this RHS count (allocated in solve_bufs too)
     const int k = nrhs;
     const z one = zmk(1.0, 0.0), mnu = zneg(t->nu);
@@ -553,6 +611,11 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
         if ((rc = upload_gemm(t, t->solve_bufs, b4, t->sB4[l]))) return rc;
         if ((rc = upload_gemm(t, t->solve_bufs, b5, t->sB5[l]))) return rc;
     }
+    t->sL0.fixed_order = true;
+    for (int l = 0; l < L; ++l)
+        for (GemmBatch* gb : {&t->sF12[l], &t->sF3[l], &t->sF4[l], &t->sF5[l], &t->sB1[l], &t->sB23[l], &t->sB4[l],
+                              &t->sB5[l]})
+            gb->fixed_order = true;
     t->built_rhs = nrhs;
     return RB_OK;
 }
@@ -631,6 +694,7 @@ int rb_tree_create(const rb_geom* geom, rb_tree** out) {
     t->budget = geom->device_budget;
     t->verbose = (geom->flags & RB_FLAG_VERBOSE) != 0;
     t->skip_root = (geom->flags & RB_FLAG_SKIP_ROOT_RTR) != 0;
+    t->graphs = (geom->flags & RB_FLAG_NO_GRAPHS) == 0;
     // refuse up front a problem the budget cannot hold (persistent factor storage only)
     if (t->budget > 0) {
         const Plan& Q = t->P;
@@ -654,6 +718,8 @@ int rb_tree_destroy(rb_tree* t) {
     if (!t) return RB_OK;
     if (t->stream) cudaStreamSynchronize(t->stream);
     timers_collect(t);
+    drop_graph(t->gx_factor);
+    drop_graph(t->gx_solve);
     free_list(t, t->solve_bufs);
     free_list(t, t->bufs);
     for (auto& e : t->ev)
@@ -758,16 +824,16 @@ static int factor_common(rb_tree* t, const double* k, int precision, bool host, 
         timers_collect(t);
         t->stage_ms.clear();
     }
-    const z* dk = reinterpret_cast<const z*>(k);
-    if (host) {
-        RB_CK(cudaMemcpyAsync(t->d_k, k, nint * sizeof(z), cudaMemcpyHostToDevice, t->stream));
-        dk = t->d_k;
-    }
+    // the factor always reads the handle's own copy, so one captured graph serves every call
+    RB_CK(cudaMemcpyAsync(t->d_k, k, nint * sizeof(z), host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
+                          t->stream));
     for (auto& e : t->ev)
         if (!e) RB_CK(cudaEventCreate(&e));
     const long long l0 = launch_count();
     RB_CK(cudaEventRecord(t->ev[0], t->stream));
-    if ((rc = run_factor(t, dk))) return rc;
+    if ((rc = run_graphed(t, t->gx_factor, t->gx_factor_launches, t->factor_runs,
+                          [&] { return run_factor(t, t->d_k); })))
+        return rc;
     RB_CK(cudaEventRecord(t->ev[1], t->stream));
     t->factor_launches = launch_count() - l0;
     if (host || sync) {
@@ -806,7 +872,13 @@ static int solve_common(rb_tree* t, int nrhs, const double* f, const double* g, 
     RB_CK(cudaMemcpyAsync(t->d_f, f, nrhs * nint * sizeof(z), kind, t->stream));
     RB_CK(cudaMemcpyAsync(t->gbuf[0], g, nrhs * nroot * sizeof(z), kind, t->stream));
     const long long l0 = launch_count();
-    if ((rc = run_solve(t, nrhs))) return rc;
+    if (t->gx_solve_rhs != nrhs) {     // the solve sequence depends on the RHS count
+        drop_graph(t->gx_solve);
+        t->gx_solve_rhs = nrhs;
+        t->solve_runs = 0;
+    }
+    if ((rc = run_graphed(t, t->gx_solve, t->gx_solve_launches, t->solve_runs, [&] { return run_solve(t, nrhs); })))
+        return rc;
     t->solve_launches = launch_count() - l0;
     RB_CK(cudaEventRecord(t->ev[3], t->stream));
     if (host || sync) {
