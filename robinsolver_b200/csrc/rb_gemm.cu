@@ -16,10 +16,11 @@
 
 namespace rb {
 
-template <int BM, int BN, int TM, int TN, int BK, int MINB>
+template <int BM, int BN, int TM, int TN, int BK, int STAGES, int MINB>
 __global__ void __launch_bounds__((BM / TM) * (BN / TN), MINB)
 zgemm_desc_kernel(const GemmDesc* __restrict__ descs) {
     constexpr int NT = (BM / TM) * (BN / TN);
+    extern __shared__ z dfma_smem[];
     __shared__ GemmDesc sd;
     {
         const unsigned long long* src = reinterpret_cast<const unsigned long long*>(descs + blockIdx.y);
@@ -27,7 +28,7 @@ zgemm_desc_kernel(const GemmDesc* __restrict__ descs) {
         for (int w = threadIdx.x; w < (int)(sizeof(GemmDesc) / 8); w += NT) dst[w] = src[w];
     }
     __syncthreads();
-    zgemm_tile<BM, BN, TM, TN, BK>(sd, blockIdx.x);
+    zgemm_tile<BM, BN, TM, TN, BK, STAGES>(sd, blockIdx.x, dfma_smem);
 }
 
 template <int BM, int BN, int WM, int WN>
@@ -74,14 +75,22 @@ static bool use_dmma() {
     return v == 1;
 }
 
-template <int BM, int BN, int TM, int TN, int BK, int MINB>
+template <int BM, int BN, int TM, int TN, int BK, int STAGES, int MINB>
 static cudaError_t launch_cfg(const GemmBatch& b, cudaStream_t s) {
     constexpr int NT = (BM / TM) * (BN / TN);
+    constexpr size_t SMEM = DfmaCfg<BM, BN, BK, STAGES>::SMEM_BYTES;
+    static bool attr = false;
+    if (!attr && SMEM > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(zgemm_desc_kernel<BM, BN, TM, TN, BK, STAGES, MINB>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+        if (e != cudaSuccess) return e;
+    }
+    attr = true;
     const int tiles = ((b.max_m + BM - 1) / BM) * ((b.max_n + BN - 1) / BN);
     for (int off = 0; off < b.count; off += 65535) {
         const int cnt = (b.count - off) < 65535 ? (b.count - off) : 65535;
         dim3 grid(tiles, cnt);
-        zgemm_desc_kernel<BM, BN, TM, TN, BK, MINB><<<grid, NT, 0, s>>>(b.d_desc + off);
+        zgemm_desc_kernel<BM, BN, TM, TN, BK, STAGES, MINB><<<grid, NT, SMEM, s>>>(b.d_desc + off);
         note_launch();
     }
     return cudaGetLastError();
@@ -91,16 +100,21 @@ cudaError_t launch_gemm_batch(const GemmBatch& b, cudaStream_t s) {
     static_assert(sizeof(GemmDesc) % 8 == 0, "descriptor copy assumes 8-byte words");
     if (b.count == 0 || b.max_m == 0 || b.max_n == 0) return cudaSuccess;
     const int mm = b.max_m, nn = b.max_n;
-    if (mm <= 16 && nn <= 16) return launch_cfg<16, 16, 2, 2, 8, 8>(b, s);
-    if (mm <= 32 || nn <= 32) return launch_cfg<32, 32, 4, 2, 8, 4>(b, s);
+    if (mm <= 16 && nn <= 16) return launch_cfg<16, 16, 2, 2, 8, 6, 8>(b, s);
+    // every DFMA shape sums an element's products in the same order, so the shape can follow the
+    // available parallelism: small-n batches (the solve) that would leave SMs idle with 32x32
+    // tiles take 16x16 tiles
+    if (nn <= 32 && (long long)b.count * ((mm + 31) / 32) * ((nn + 31) / 32) < 2 * 148)
+        return launch_cfg<16, 16, 2, 2, 8, 6, 8>(b, s);
+    if (mm <= 32 || nn <= 32) return launch_cfg<32, 32, 4, 2, 8, 4, 4>(b, s);
     const bool big = mm >= 256 && nn >= 128 && (long long)b.count * ((mm + 127) / 128) * ((nn + 63) / 64) >= 148;
     if (use_dmma() && !b.fixed_order) {
         if (big) return launch_dmma<128, 64, 4, 2>(b, s);
         return launch_dmma<64, 64, 2, 4>(b, s);
     }
     // large problems: 8x4 complex register tile per thread (1.5 B of shared memory per DFMA)
-    if (big) return launch_cfg<128, 64, 8, 4, 4, 1>(b, s);
-    return launch_cfg<64, 64, 4, 4, 8, 1>(b, s);
+    if (big) return launch_cfg<128, 64, 8, 4, 4, 4, 1>(b, s);
+    return launch_cfg<64, 64, 4, 4, 8, 4, 1>(b, s);
 }
 
 }  // namespace rb

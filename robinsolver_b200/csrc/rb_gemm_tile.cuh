@@ -1,18 +1,27 @@
-// rb_gemm_tile.cuh -- one C tile of a complex128 GEMM problem described by a GemmDesc that
-// already sits in shared memory.  Used by the descriptor-batched GEMM (rb_gemm.cu) and by the
-// blocked Gauss-Jordan update (rb_gj.cu), which builds its descriptor inside the kernel.
+// rb_gemm_tile.cuh -- one C tile of a complex128 GEMM problem on DFMA register tiles, for the small
+// merge GEMMs and every solve GEMM (rb_gemm.cu).
 //
 // Thread (tr, tc) owns rows tr + i*RG and columns tc + j*CG of the BM x BN tile (strided so
-// that a warp's epilogue stores and shared-memory operand reads are contiguous).  Operand
-// tiles go global -> registers -> shared memory with one tile of look-ahead; the inner loop is
-// 4 DFMA per complex multiply-add.
+// that a warp's epilogue stores and shared-memory operand reads are contiguous).  Operand tiles
+// stream global -> shared memory with cp.async in a STAGES-deep ring, so that STAGES-1 k-tiles
+// are in flight while one is multiplied (the skinny solve GEMMs, k ~ 1000 and n ~ 32, are
+// load-latency bound otherwise).  The inner loop is 4 DFMA per complex multiply-add, and every
+// element sums its products in k order: results do not depend on the tile shape.
 #pragma once
 #include "rb_common.cuh"
+#include "rb_gemm_dmma.cuh"    // cp.async helpers
 
 namespace rb {
 
-template <int BM, int BN, int TM, int TN, int BK>
-__device__ __forceinline__ void zgemm_tile(const GemmDesc& sd, int tile) {
+template <int BM, int BN, int BK, int STAGES>
+struct DfmaCfg {
+    static constexpr int STAGE_Z = BK * BM + BK * BN;
+    static constexpr size_t SMEM_BYTES = (size_t)STAGES * STAGE_Z * sizeof(z);
+};
+
+template <int BM, int BN, int TM, int TN, int BK, int STAGES>
+__device__ __forceinline__ void zgemm_tile(const GemmDesc& sd, int tile, z* smem) {
+    using Cfg = DfmaCfg<BM, BN, BK, STAGES>;
     constexpr int NT = (BM / TM) * (BN / TN);
     constexpr int RG = BM / TM;
     constexpr int CG = BN / TN;
@@ -20,9 +29,6 @@ __device__ __forceinline__ void zgemm_tile(const GemmDesc& sd, int tile) {
     constexpr int B_PER = BK * BN / NT;
     static_assert(NT % BM == 0 && NT % BK == 0, "tile/thread mismatch");
     static_assert(A_PER * NT == BM * BK && B_PER * NT == BK * BN, "tile/thread mismatch");
-
-    __shared__ z As[2][BK][BM];
-    __shared__ z Bs[2][BK][BN];
 
     const int tid = threadIdx.x;
     const int m = sd.m, n = sd.n, K = sd.k;
@@ -49,26 +55,28 @@ __device__ __forceinline__ void zgemm_tile(const GemmDesc& sd, int tile) {
         bcol_ok[e] = j < n;
         bcol[e] = bcol_ok[e] ? (long long)vcol(B, j) * B.ld : 0;
     }
-
-    z ra[A_PER], rbv[B_PER];
-    auto gload = [&](int k0) {
+    const int ktiles = (K + BK - 1) / BK;
+    auto issue = [&](int kt) {
+        z* As = smem + (kt % STAGES) * Cfg::STAGE_Z;
+        z* Bs = As + BK * BM;
+        const int k0 = kt * BK;
 #pragma unroll
         for (int e = 0; e < A_PER; ++e) {
-            const int gk = k0 + akk0 + e * (NT / BM);
-            ra[e] = (arow_ok && gk < K) ? A.p[arow + (long long)vcol(A, gk) * A.ld] : zmk(0.0, 0.0);
+            const int kk = akk0 + e * (NT / BM);
+            const int gk = k0 + kk;
+            const bool ok = arow_ok && gk < K;
+            const z* src = ok ? A.p + arow + (long long)vcol(A, gk) * A.ld : A.p;
+            cp_async16(As + kk * BM + ai, src, ok ? 16 : 0);
         }
         const int gk = k0 + bkk;
         const bool kok = gk < K;
         const long long brow = kok ? (long long)vrow(B, gk) : 0;
 #pragma unroll
-        for (int e = 0; e < B_PER; ++e)
-            rbv[e] = (kok && bcol_ok[e]) ? B.p[brow + bcol[e]] : zmk(0.0, 0.0);
-    };
-    auto sstore = [&](int buf) {
-#pragma unroll
-        for (int e = 0; e < A_PER; ++e) As[buf][akk0 + e * (NT / BM)][ai] = ra[e];
-#pragma unroll
-        for (int e = 0; e < B_PER; ++e) Bs[buf][bkk][bj0 + e * (NT / BK)] = rbv[e];
+        for (int e = 0; e < B_PER; ++e) {
+            const bool ok = kok && bcol_ok[e];
+            const z* src = ok ? B.p + brow + bcol[e] : B.p;
+            cp_async16(Bs + bkk * BN + bj0 + e * (NT / BK), src, ok ? 16 : 0);
+        }
     };
 
     const int tr = tid % RG;
@@ -79,29 +87,32 @@ __device__ __forceinline__ void zgemm_tile(const GemmDesc& sd, int tile) {
 #pragma unroll
         for (int j = 0; j < TN; ++j) acc[i][j] = zmk(0.0, 0.0);
 
-    gload(0);
-    sstore(0);
-    __syncthreads();
-    int buf = 0;
-    for (int k0 = 0; k0 < K; k0 += BK) {
-        const bool more = (k0 + BK) < K;
-        if (more) gload(k0 + BK);
+#pragma unroll
+    for (int s = 0; s < STAGES - 1; ++s) {
+        if (s < ktiles) issue(s);
+        cp_async_commit();
+    }
+    for (int kt = 0; kt < ktiles; ++kt) {
+        cp_async_wait<STAGES - 2>();
+        __syncthreads();                 // tile kt visible; everyone is done with tile kt-1's stage
+        if (kt + STAGES - 1 < ktiles) issue(kt + STAGES - 1);
+        cp_async_commit();
+        const z* As = smem + (kt % STAGES) * Cfg::STAGE_Z;
+        const z* Bs = As + BK * BM;
 #pragma unroll
         for (int kk = 0; kk < BK; ++kk) {
             z a[TM], b[TN];
 #pragma unroll
-            for (int i = 0; i < TM; ++i) a[i] = As[buf][kk][tr + i * RG];
+            for (int i = 0; i < TM; ++i) a[i] = As[kk * BM + tr + i * RG];
 #pragma unroll
-            for (int j = 0; j < TN; ++j) b[j] = Bs[buf][kk][tc + j * CG];
+            for (int j = 0; j < TN; ++j) b[j] = Bs[kk * BN + tc + j * CG];
 #pragma unroll
             for (int i = 0; i < TM; ++i)
 #pragma unroll
                 for (int j = 0; j < TN; ++j) zfma(acc[i][j], a[i], b[j]);
         }
-        if (more) sstore(buf ^ 1);
-        __syncthreads();
-        buf ^= 1;
     }
+    cp_async_wait<0>();
 
     const z alpha = sd.alpha, beta = sd.beta;
     const ZView C = sd.C;
@@ -126,9 +137,5 @@ __device__ __forceinline__ void zgemm_tile(const GemmDesc& sd, int tile) {
         }
     }
 }
-
-// thread-block sizes of the tile configurations
-template <int BM, int BN, int TM, int TN>
-struct TileThreads { static constexpr int value = (BM / TM) * (BN / TN); };
 
 }  // namespace rb

@@ -286,12 +286,200 @@ __global__ void __launch_bounds__(256) leaf_block_factor_kernel(LeafGeom g, cons
     if (!ok && tid == 0) atomicOr(status, 1);
 }
 
+// ---------------------------------------------------------------------------------------------------
+// Warp-per-leaf factor for a = 16 (every leaf of a 16x16 grid): the same algebra as
+// leaf_block_factor_kernel with no block barriers.  A 16x16 block lives in registers, lane l
+// holding row l%16, columns 8*(l/16)..+7; Gauss-Jordan pivots by shuffles (|re|+|im|, first
+// maximum) and the column exchanges are undone through the warp's shared memory.  In the
+// S^T Z = C^T sweeps each lane carries one right-hand side (a 16-vector per block) at a time.
+__global__ void __launch_bounds__(128) leaf_warp_factor_kernel(LeafGeom g, int nleaves, const double* __restrict__ hh,
+                                                               const z* __restrict__ kv, z* __restrict__ sinv,
+                                                               z* __restrict__ Y, int* status) {
+    constexpr int A = 16, AA = 256;
+    __shared__ z wsm[4][AA];
+    __shared__ int wpiv[4][2 * A];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int leaf = blockIdx.x * 4 + wib;
+    if (leaf >= nleaves) return;
+    z* sm = wsm[wib];
+    int* piv = wpiv[wib];
+    const int b = g.b, nb = g.nb, n = g.n, ab = A * b;
+    const LeafConst L = leaf_const(hh, leaf, g.kb);
+    const z* kl = kv + (size_t)leaf * ab;
+    z* Sl = sinv + (size_t)leaf * b * AA;
+    z* Yl = Y + (size_t)leaf * nb * n;
+    const int r = lane & 15, hf = lane >> 4;          // row, column half
+    z a[8], prev[8];
+    bool ok = true;
+
+    // ---- block LU ---------------------------------------------------------------------------------
+    for (int j = 0; j < b; ++j) {
+        const int jj = j + 1;
+        const z lm = jj > 1 ? zmul(block_lo(L, b, jj), block_up(L, b, jj - 1)) : zmk(0.0, 0.0);
+        const z kr = kl[j * A + r];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            z v = block_d(L, A, b, jj, r, hf * 8 + e, kr);
+            if (jj > 1) zfms(v, lm, prev[e]);
+            a[e] = v;
+        }
+#pragma unroll
+        for (int k = 0; k < A; ++k) {
+            const int hk = k >> 3, ek = k & 7;
+            double mag = (hf == hk && r >= k) ? zabs1(a[ek]) : -1.0;
+            int idx = r;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double om = __shfl_xor_sync(0xffffffffu, mag, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+                if (om > mag || (om == mag && oi < idx)) { mag = om; idx = oi; }
+            }
+            const int p = idx;
+            if (lane == 0) piv[k] = p;
+            if (p != k) {                           // exchange rows k and p
+                const int src = (r == k ? p : (r == p ? k : r)) + 16 * hf;
+#pragma unroll
+                for (int e = 0; e < 8; ++e) {
+                    const double x = __shfl_sync(0xffffffffu, a[e].x, src);
+                    const double y = __shfl_sync(0xffffffffu, a[e].y, src);
+                    a[e] = zmk(x, y);
+                }
+            }
+            const z pv = zmk(__shfl_sync(0xffffffffu, a[ek].x, k + 16 * hk),
+                             __shfl_sync(0xffffffffu, a[ek].y, k + 16 * hk));
+            if (pv.x == 0.0 && pv.y == 0.0) ok = false;
+            const z pinv = zrcp(pv);
+            const z f = zmk(__shfl_sync(0xffffffffu, a[ek].x, r + 16 * hk),
+                            __shfl_sync(0xffffffffu, a[ek].y, r + 16 * hk));
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const z pr = zmul(zmk(__shfl_sync(0xffffffffu, a[e].x, k + 16 * hf),
+                                      __shfl_sync(0xffffffffu, a[e].y, k + 16 * hf)), pinv);
+                const bool colk = (hf == hk) && (e == ek);
+                if (r == k) a[e] = colk ? pinv : pr;
+                else if (colk) a[e] = zneg(zmul(f, pinv));
+                else zfms(a[e], f, pr);
+            }
+        }
+        // undo the column exchanges: X = X_pre P, column c of X is column sig(c) of X_pre;
+        // piv[A + c'] receives the destination column of pre-column c'
+        __syncwarp();
+        if (lane == 0) {
+            int sg[A];
+            for (int c = 0; c < A; ++c) sg[c] = c;
+            for (int k = A - 1; k >= 0; --k) {
+                const int p = piv[k];
+                const int t = sg[k];
+                sg[k] = sg[p];
+                sg[p] = t;
+            }
+            for (int c = 0; c < A; ++c) piv[A + sg[c]] = c;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int e = 0; e < 8; ++e) sm[r + piv[A + hf * 8 + e] * A] = a[e];
+        __syncwarp();
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            prev[e] = sm[r + (hf * 8 + e) * A];
+            Sl[(size_t)j * AA + r + (hf * 8 + e) * A] = prev[e];
+        }
+        __syncwarp();
+    }
+    if (!ok && lane == 0) atomicOr(status, 1);
+
+    // ---- S^T Z = C^T, one right-hand side per lane at a time ---------------------------------------
+    for (int c = lane; c - lane < nb; c += 32) {
+        const bool live = c < nb;
+        int ax = 0, q1 = -1, q2 = -1;
+        if (live) leaf_bpoint2(A, b, c, ax, q1, q2);
+        const double hr = ax == 0 ? L.hx : L.hy;
+        const double c1 = -3.0 / hr, c2 = (1.0 / 3.0) / hr;
+        z v[A];
+#pragma unroll
+        for (int i = 0; i < A; ++i) v[i] = zmk(0.0, 0.0);
+        // forward: v_j = Sig_j^-T (c_j - Up_{j-1} v_{j-1})
+        for (int j = 0; j < b; ++j) {
+            const int jj = j + 1;
+            const z mup = jj > 1 ? block_up(L, b, jj - 1) : zmk(0.0, 0.0);
+            __syncwarp();
+#pragma unroll
+            for (int e = 0; e < 8; ++e) sm[r + (hf * 8 + e) * A] = Sl[(size_t)j * AA + r + (hf * 8 + e) * A];
+            __syncwarp();
+            z rhs[A];
+#pragma unroll
+            for (int q = 0; q < A; ++q) {
+                const int eq = j * A + q;
+                rhs[q] = zmk((eq == q1 ? c1 : 0.0) + (eq == q2 ? c2 : 0.0), 0.0);
+                if (jj > 1) zfms(rhs[q], mup, v[q]);
+            }
+#pragma unroll
+            for (int i = 0; i < A; ++i) {
+                z acc = zmk(0.0, 0.0);
+#pragma unroll
+                for (int q = 0; q < A; ++q) zfma(acc, sm[q + i * A], rhs[q]);
+                v[i] = acc;
+                if (live) Yl[c + (size_t)(nb + j * A + i) * nb] = acc;
+            }
+        }
+        // backward: z_{j-1} = v_{j-1} - Sig_{j-1}^-T Lo_j z_j, z_{b-1} = v_{b-1}
+        for (int j = b - 1; j >= 1; --j) {
+            const z lam = block_lo(L, b, j + 1);
+            __syncwarp();
+#pragma unroll
+            for (int e = 0; e < 8; ++e) sm[r + (hf * 8 + e) * A] = Sl[(size_t)(j - 1) * AA + r + (hf * 8 + e) * A];
+            __syncwarp();
+            z lz[A];
+#pragma unroll
+            for (int q = 0; q < A; ++q) lz[q] = zmul(lam, v[q]);
+#pragma unroll
+            for (int i = 0; i < A; ++i) {
+                z acc = live ? Yl[c + (size_t)(nb + (j - 1) * A + i) * nb] : zmk(0.0, 0.0);
+#pragma unroll
+                for (int q = 0; q < A; ++q) zfms(acc, sm[q + i * A], lz[q]);
+                v[i] = acc;
+                if (live) Yl[c + (size_t)(nb + (j - 1) * A + i) * nb] = acc;
+            }
+        }
+    }
+    __syncwarp();
+    // ---- Y = R A^-1 from Q(r, s) = Z(s, r) = Y(r, nb+s) -------------------------------------------
+    for (int e = lane; e < nb * nb; e += 32) {
+        const int rr = e % nb, c = e / nb;
+        int ax, p1, p2, axc, q1, q2;
+        leaf_bpoint2(A, b, rr, ax, p1, p2);
+        leaf_bpoint2(A, b, c, axc, q1, q2);
+        const z rd = ax == 0 ? L.rdx : L.rdy;
+        const z f = zmul(zmk(0.0, 2.0 * g.kb), rd);
+        const z wd = axc == 0 ? zscale(L.wbx, L.rdx) : zscale(L.wby, L.rdy);
+        z val = zneg(zmul(zmul(f, wd), Yl[rr + (size_t)(nb + q1) * nb]));
+        if (c == rr) {
+            const double hr2 = ax == 0 ? L.hx : L.hy;
+            val = zadd(val, zmul(zmk((8.0 / 3.0) / hr2, -g.kb), rd));
+        }
+        Yl[e] = val;
+    }
+    __syncwarp();
+    for (int e = lane; e < nb * ab; e += 32) {
+        const int rr = e % nb;
+        int ax, p1, p2;
+        leaf_bpoint2(A, b, rr, ax, p1, p2);
+        const z f = zmul(zmk(0.0, 2.0 * g.kb), ax == 0 ? L.rdx : L.rdy);
+        Yl[(size_t)nb * nb + e] = zmul(f, Yl[(size_t)nb * nb + e]);
+    }
+}
+
 size_t leaf_block_factor_smem(const LeafGeom& g) {
     return (2 * (size_t)g.a * g.a + 2 * (size_t)g.a * g.nb + g.a) * sizeof(z) + (g.a + 1) * sizeof(int) + 16;
 }
 
 cudaError_t leaf_block_factor(const LeafGeom& g, int nleaves, const double* h, const z* k, z* sinv, z* Y,
                               int* status, cudaStream_t s) {
+    if (g.a == 16) {                        // one warp per leaf
+        leaf_warp_factor_kernel<<<(nleaves + 3) / 4, 128, 0, s>>>(g, nleaves, h, k, sinv, Y, status);
+        note_launch();
+        return cudaGetLastError();
+    }
     const size_t sh = leaf_block_factor_smem(g);
     if (sh > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(leaf_block_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);

@@ -70,6 +70,8 @@ struct rb_tree {
     Plan P;
     std::string err;
     cudaStream_t stream = nullptr;
+    cudaStream_t stream2 = nullptr;      // runs Y2R = inv(D) T2_iN beside the inversion of S
+    std::vector<cudaEvent_t> ev_fork, ev_join;
     int device = 0;
     bool factored = false;
     double f_time = 0.0, s_time = 0.0;
@@ -330,6 +332,13 @@ static int ensure_factor_storage(rb_tree* t) {
     int rc;
     RB_CK(cudaGetDevice(&t->device));
     if (!t->stream) RB_CK(cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking));
+    if (!t->stream2) RB_CK(cudaStreamCreateWithFlags(&t->stream2, cudaStreamNonBlocking));
+    t->ev_fork.assign(L, nullptr);
+    t->ev_join.assign(L, nullptr);
+    for (int l = 0; l < L; ++l) {
+        RB_CK(cudaEventCreateWithFlags(&t->ev_fork[l], cudaEventDisableTiming));
+        RB_CK(cudaEventCreateWithFlags(&t->ev_join[l], cudaEventDisableTiming));
+    }
     if ((rc = alloc_n(t, t->bufs, 2 * (size_t)nl, &t->d_h))) return rc;
     RB_CK(cudaMemcpy(t->d_h, P.leaf_h.data(), 2 * nl * sizeof(double), cudaMemcpyHostToDevice));
     if ((rc = alloc_n(t, t->bufs, (size_t)nl * ab, &t->d_k))) return rc;
@@ -486,9 +495,18 @@ static int run_factor(rb_tree* t, const z* dk) {
         if ((rc = timer_begin(t, l < 17 ? lvl_names[l] : "merge_deep"))) return rc;
         RB_TIMED("merge_form", 0.0, merge_form_d(cs, p.nnodes, p.m, p.o2, t->zeta, t->dinv[l], s));
         RB_TIMED("gj_invert", gj_flops(p.m, p.nnodes), gj_invert_batch(t->gj_d[l].d_desc, p.nnodes, p.m, t->d_status, s));
+        // Y2R = inv(D) T2_iN needs only inv(D): on the second stream it overlaps the S inversion
+        const bool fork = t->timing == 0;
+        if (fork) {
+            RB_CK(cudaEventRecord(t->ev_fork[l], s));
+            RB_CK(cudaStreamWaitEvent(t->stream2, t->ev_fork[l], 0));
+            RB_LAUNCH(launch_gemm_batch(t->fM1[l], t->stream2));
+            RB_CK(cudaEventRecord(t->ev_join[l], t->stream2));
+        }
         RB_TIMED("merge_form", 0.0, merge_form_s(cs, p.nnodes, p.m, p.o1, t->zeta, t->nu, t->dinv[l], t->sinv[l], s));
         RB_TIMED("gj_invert", gj_flops(p.m, p.nnodes), gj_invert_batch(t->gj_s[l].d_desc, p.nnodes, p.m, t->d_status, s));
-        RB_TIMED("zgemm", t->fM1[l].flops, launch_gemm_batch(t->fM1[l], s));
+        if (fork) RB_CK(cudaStreamWaitEvent(s, t->ev_join[l], 0));
+        else RB_TIMED("zgemm", t->fM1[l].flops, launch_gemm_batch(t->fM1[l], s));
         RB_TIMED("zgemm", t->fM2[l].flops, launch_gemm_batch(t->fM2[l], s));
         RB_TIMED("zgemm", t->fM3[l].flops, launch_gemm_batch(t->fM3[l], s));
         RB_TIMED("zgemm", t->fM4[l].flops, launch_gemm_batch(t->fM4[l], s));
@@ -725,6 +743,9 @@ int rb_tree_destroy(rb_tree* t) {
     for (auto& e : t->ev)
         if (e) cudaEventDestroy(e);
     for (auto& e : t->ev_pool) cudaEventDestroy(e);
+    for (auto& e : t->ev_fork) if (e) cudaEventDestroy(e);
+    for (auto& e : t->ev_join) if (e) cudaEventDestroy(e);
+    if (t->stream2) cudaStreamDestroy(t->stream2);
     if (t->stream) cudaStreamDestroy(t->stream);
     delete t;
     return RB_OK;
