@@ -18,6 +18,7 @@
 //      instead cancels catastrophically: W_P's diagonal holds the reciprocal pivots, ~h^2 for
 //      the FD matrices here.)
 // After the last panel the column exchanges are undone in reverse order (gj_unscramble).
+#include <cstdlib>
 #include "rb_gemm_tile.cuh"
 #include "rb_kernels.h"
 
@@ -25,11 +26,11 @@ namespace rb {
 
 int gj_panel_width(int m) {
     if (m <= GJ_SMALL_MAX) return 0;
-    if (m <= 512) return 16;
     return 8;
 }
 
-long long gj_workspace_elems(int m) { return 0; }
+// one complex element per matrix: the resident path's two flag words
+long long gj_workspace_elems(int m) { return m <= GJ_SMALL_MAX ? 0 : 1; }
 
 // warp argmax: larger value wins, equal values go to the smaller index
 __device__ __forceinline__ void argmax_warp(double& v, int& i) {
@@ -236,6 +237,326 @@ __global__ void __launch_bounds__(256) gj_apply_kernel(const GJDesc* __restrict_
     }
 }
 
+// ---------------------------------------------------------------------------------------------------
+// Resident Gauss-Jordan: the whole batch in one launch.  Matrix i is split over P CTAs by whole
+// panels of NB columns; CTA j keeps its ppc panels (m x cw complex, cw <= ppc*NB) in shared
+// memory for the whole inversion.  The owner of panel p eliminates it (one row per thread in
+// registers, as gj_panel_kernel), writes the accumulated transform W_p to the matrix's own
+// global storage at panel p's columns (unused while the columns live in shared memory) and its
+// pivots to ipiv, and publishes p+1 in the matrix's flag word.  Every CTA then applies step p
+// (the exchanges, then A += W_p Z outside the panel rows and W_p Z on them) to its resident
+// columns.  The owner of panel p+1 applies step p to that panel first, eliminates and publishes
+// it, and only then updates its other columns, so the dependent chain per step is one flag
+// hand-off, one panel update and one panel elimination.  After the last step a per-matrix
+// counter holds every CTA until all have stopped reading W slots; then the columns go back.
+//
+// The launch is cooperative (all CTAs co-resident), and every wait is bounded in time: a CTA
+// that waits longer than GJ_WAIT_NS sets bit 2 of the status word and returns.
+constexpr unsigned long long GJ_WAIT_NS = 1000000000ull;
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+__device__ __forceinline__ int ld_acquire_gpu(const int* p) {
+    int v;
+    asm volatile("ld.acquire.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_gpu(int* p, int v) {
+    asm volatile("st.release.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
+// thread 0 waits until *flag >= target; the outcome is returned to every thread of the CTA
+__device__ bool cta_wait_geq(const int* flag, int target, int* status, int* s_ok) {
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        if (ld_acquire_gpu(flag) < target) {
+            const unsigned long long t0 = global_ns();
+            int spins = 0;
+            while (ld_acquire_gpu(flag) < target) {
+                if (++spins > 32) __nanosleep(40);
+                if (global_ns() - t0 > GJ_WAIT_NS) {
+                    ok = 0;
+                    atomicOr(status, 2);
+                    break;
+                }
+            }
+        }
+        *s_ok = ok;
+    }
+    __syncthreads();
+    const bool ok = *s_ok != 0;
+    __syncthreads();                     // s_ok may be rewritten by the next wait
+    return ok;
+}
+
+template <int NB>
+struct ResShared {
+    z xb[NB], prow[NB];
+    unsigned kh[32], kl[32];
+    int ki[32];
+    int ok;
+};
+
+// warp argmax over (hi, lo) = the bit pattern of a non-negative double (which orders like the
+// value), ties to the smaller row: three warp reductions instead of a shuffle tree
+__device__ __forceinline__ void warp_key_max(unsigned& hi, unsigned& lo, int& id) {
+    const unsigned mh = __reduce_max_sync(0xffffffffu, hi);
+    const unsigned ml = __reduce_max_sync(0xffffffffu, hi == mh ? lo : 0u);
+    id = __reduce_min_sync(0xffffffffu, (hi == mh && lo == ml) ? id : 0x7fffffff);
+    hi = mh;
+    lo = ml;
+}
+
+// CTA-wide argmax of v over the valid rows (largest first, then smallest row): one block
+// barrier; every thread gets the row
+template <int NB>
+__device__ __forceinline__ int block_argmax(double v, bool valid, int r, ResShared<NB>& sh) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = (blockDim.x + 31) >> 5;
+    unsigned hi = valid ? (unsigned)__double2hiint(v) : 0u;
+    unsigned lo = valid ? (unsigned)__double2loint(v) : 0u;
+    int id = valid ? r : 0x7fffffff;
+    warp_key_max(hi, lo, id);
+    if (lane == 0) {
+        sh.kh[warp] = hi;
+        sh.kl[warp] = lo;
+        sh.ki[warp] = id;
+    }
+    __syncthreads();
+    hi = lane < nwarps ? sh.kh[lane] : 0u;
+    lo = lane < nwarps ? sh.kl[lane] : 0u;
+    id = lane < nwarps ? sh.ki[lane] : 0x7fffffff;
+    warp_key_max(hi, lo, id);
+    return id;
+}
+
+// Eliminates the panel held at local columns [q0, q0+nbk) (matrix columns k0..): RPT rows per
+// thread (rows tid + i*blockDim.x) in registers, two block barriers per column (pivot
+// candidates; scaled pivot row and displaced row).  W is left in the local columns and copied
+// to Wg (ld wld); pivots go to ipiv.
+template <int NB, int RPT>
+__device__ __noinline__ void res_eliminate(z* cols, int m, int q0, int k0, int nbk, z* Wg, long long wld, int* ipiv,
+                                           int* status, ResShared<NB>& sh) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    z row[RPT][NB];
+#pragma unroll
+    for (int i = 0; i < RPT; ++i) {
+        const int r = tid + i * nt;
+#pragma unroll
+        for (int kk = 0; kk < NB; ++kk) row[i][kk] = (r < m && kk < nbk) ? cols[r + (q0 + kk) * m] : zmk(0.0, 0.0);
+    }
+    bool bad = false;
+#pragma unroll
+    for (int kk = 0; kk < NB; ++kk) {
+        if (kk >= nbk) break;
+        const int c = k0 + kk;
+        // this thread's candidate: its largest entry on or below row c, first on ties
+        double v = 0.0;
+        int vr = -1;
+#pragma unroll
+        for (int i = 0; i < RPT; ++i) {
+            const int r = tid + i * nt;
+            const double a = zabs1(row[i][kk]);
+            if (r < m && r >= c && (vr < 0 || a > v)) { v = a; vr = r; }
+        }
+        const int p = block_argmax<NB>(v, vr >= 0, vr, sh);
+#pragma unroll
+        for (int i = 0; i < RPT; ++i) {
+            const int r = tid + i * nt;
+            if (r == p) {
+                if (zis0(row[i][kk])) bad = true;
+                const z pinv = zrcp(row[i][kk]);
+#pragma unroll
+                for (int j = 0; j < NB; ++j) sh.prow[j] = (j == kk) ? pinv : zmul(row[i][j], pinv);
+                ipiv[c] = p;
+            }
+            if (r == c && p != c) {
+#pragma unroll
+                for (int j = 0; j < NB; ++j) sh.xb[j] = row[i][j];
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < RPT; ++i) {
+            const int r = tid + i * nt;
+            if (r == c) {
+#pragma unroll
+                for (int j = 0; j < NB; ++j) row[i][j] = sh.prow[j];
+            } else if (r < m) {
+                if (r == p) {
+#pragma unroll
+                    for (int j = 0; j < NB; ++j) row[i][j] = sh.xb[j];
+                }
+                const z f = row[i][kk];
+#pragma unroll
+                for (int j = 0; j < NB; ++j)
+                    if (j != kk) zfms(row[i][j], f, sh.prow[j]);
+                row[i][kk] = zneg(zmul(f, sh.prow[kk]));
+            }
+        }
+        __syncthreads();                 // prow / xb / candidate slots are rewritten next column
+    }
+#pragma unroll
+    for (int i = 0; i < RPT; ++i) {
+        const int r = tid + i * nt;
+        if (r >= m) continue;
+#pragma unroll
+        for (int kk = 0; kk < NB; ++kk) {
+            if (kk >= nbk) break;
+            cols[r + (q0 + kk) * m] = row[i][kk];
+            Wg[r + (long long)kk * wld] = row[i][kk];
+        }
+    }
+    if (bad) atomicOr(status, 1);
+    __syncthreads();
+}
+
+// Applies step (panel at matrix columns k0.., nbk wide, pivots at piv, W at W with ld wld, read
+// through L2 when w_global) to the local columns [qa, qb) except [xa, xb).  The panel's row
+// exchanges move only the panel rows and the pivot rows below the panel; their exchanged values
+// (row a takes stored row src(a), src = the transpositions traced backwards) are gathered in
+// parallel into zs (2*NB slots per column: slot t < NB panel row k0+t, slot NB+t pivot row t
+// unless it repeats), the displaced pivot rows are written back, and then every thread updates
+// its rows: A + W Z outside the panel rows, W_P Z on them, Z = the gathered panel rows.  Same
+// operations, in the same order, as exchanging row by row and then updating.
+template <int NB, int RPT>
+__device__ __noinline__ void res_apply(z* cols, z* zs, int m, int k0, int nbk, const z* W, long long wld,
+                                       bool w_global, const int* piv, int qa, int qb, int xa, int xb) {
+    if (qb <= qa) return;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int nq = qb - qa;
+    {
+        int pv[NB];
+#pragma unroll
+        for (int kk = 0; kk < NB; ++kk) pv[kk] = kk < nbk ? __ldcg(piv + kk) : -1;
+        for (int e = tid; e < 2 * NB * nq; e += nt) {
+            const int t = e % (2 * NB), q = qa + e / (2 * NB);
+            if (q >= xa && q < xb) continue;
+            int a = -1;
+            if (t < nbk) {
+                a = k0 + t;
+            } else if (t >= NB && t - NB < nbk) {
+                int pt = -1;
+#pragma unroll
+                for (int u = 0; u < NB; ++u)
+                    if (u == t - NB) pt = pv[u];
+                bool dup = pt < k0 + nbk;
+#pragma unroll
+                for (int u = 0; u < NB; ++u)
+                    if (u < t - NB && pv[u] == pt) dup = true;
+                if (!dup) a = pt;
+            }
+            if (a < 0) continue;
+            int jr = a;
+#pragma unroll
+            for (int kk = NB - 1; kk >= 0; --kk) {
+                const int c = k0 + kk;
+                if (kk < nbk) jr = (jr == c) ? pv[kk] : (jr == pv[kk] ? c : jr);
+            }
+            zs[t + (q - qa) * 2 * NB] = cols[jr + q * m];
+        }
+        __syncthreads();
+        for (int e = tid; e < NB * nq; e += nt) {
+            const int t = e % NB, q = qa + e / NB;
+            if ((q >= xa && q < xb) || t >= nbk) continue;
+            int pt = -1;
+#pragma unroll
+            for (int u = 0; u < NB; ++u)
+                if (u == t) pt = pv[u];
+            bool dup = pt < k0 + nbk;
+#pragma unroll
+            for (int u = 0; u < NB; ++u)
+                if (u < t && pv[u] == pt) dup = true;
+            if (!dup) cols[pt + q * m] = zs[NB + t + (q - qa) * 2 * NB];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < RPT; ++i) {
+        const int r = tid + i * nt;
+        if (r >= m) continue;
+        z w[NB];
+#pragma unroll
+        for (int kk = 0; kk < NB; ++kk)
+            w[kk] = kk < nbk ? (w_global ? __ldcg(W + r + kk * wld) : W[r + kk * wld]) : zmk(0.0, 0.0);
+        const bool in_panel = r >= k0 && r < k0 + nbk;
+        for (int q = qa; q < qb; ++q) {
+            if (q >= xa && q < xb) continue;
+            z v = in_panel ? zmk(0.0, 0.0) : cols[r + q * m];
+            const z* zq = zs + (q - qa) * 2 * NB;
+#pragma unroll
+            for (int kk = 0; kk < NB; ++kk)
+                if (kk < nbk) zfma(v, w[kk], zq[kk]);
+            cols[r + q * m] = v;
+        }
+    }
+    __syncthreads();
+}
+
+template <int NB, int MAXT, int RPT>
+__global__ void __launch_bounds__(MAXT, MAXT <= 256 ? 512 / MAXT : 1) gj_resident_kernel(
+    const GJDesc* __restrict__ descs, int m, int npanels, int ppc, int P, int* status) {
+    extern __shared__ z sm[];
+    __shared__ ResShared<NB> sh;
+    const int mat = blockIdx.x / P, j = blockIdx.x % P;
+    const GJDesc g = descs[mat];
+    const int pa = j * ppc, pb = min(npanels, pa + ppc);
+    const int c0 = pa * NB, cw = min(m, pb * NB) - c0;
+    z* cols = sm;                                   // m x cw, column-major (ld m)
+    z* zs = sm + (size_t)m * ppc * NB;              // 2NB x cw: exchanged panel and pivot rows
+    int* pub = reinterpret_cast<int*>(g.Zb);        // panels published
+    int* done = pub + 1;                            // CTAs past their last step
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int e = tid; e < m * cw; e += nt) {
+        const int r = e % m, q = e / m;
+        cols[r + q * m] = __ldcg(g.A + r + (long long)(c0 + q) * g.ld);
+    }
+    __syncthreads();
+    auto publish = [&](int p) {          // res_eliminate ended with a block barrier
+        if (tid == 0) {
+            __threadfence();
+            st_release_gpu(pub, p + 1);
+        }
+    };
+    if (pa == 0) {
+        res_eliminate<NB, RPT>(cols, m, 0, 0, min(NB, m), g.A, g.ld, g.ipiv, status, sh);
+        publish(0);
+    }
+    for (int p = 0; p < npanels; ++p) {
+        const int k0 = p * NB, nbk = min(NB, m - k0);
+        const bool own = p >= pa && p < pb;
+        if (!own && !cta_wait_geq(pub, p + 1, status, &sh.ok)) return;
+        const z* W = own ? cols + (size_t)(k0 - c0) * m : g.A + (long long)k0 * g.ld;
+        const long long wld = own ? m : g.ld;
+        const int* piv = g.ipiv + k0;
+        const int xa = own ? k0 - c0 : 0, xb = own ? k0 - c0 + nbk : 0;
+        const int nx = p + 1;
+        if (nx < npanels && nx >= pa && nx < pb) {
+            const int qn = nx * NB - c0, nbn = min(NB, m - nx * NB);
+            res_apply<NB, RPT>(cols, zs, m, k0, nbk, W, wld, !own, piv, qn, qn + nbn, xa, xb);
+            res_eliminate<NB, RPT>(cols, m, qn, nx * NB, nbn, g.A + (long long)nx * NB * g.ld, g.ld, g.ipiv, status,
+                                   sh);
+            publish(nx);
+            res_apply<NB, RPT>(cols, zs, m, k0, nbk, W, wld, !own, piv, 0, qn, xa, xb);
+            res_apply<NB, RPT>(cols, zs, m, k0, nbk, W, wld, !own, piv, qn + nbn, cw, xa, xb);
+        } else {
+            res_apply<NB, RPT>(cols, zs, m, k0, nbk, W, wld, !own, piv, 0, cw, xa, xb);
+        }
+    }
+    // no CTA of this matrix reads a W slot any more once all have arrived here
+    if (tid == 0) {
+        __threadfence();
+        atomicAdd(done, 1);
+    }
+    if (!cta_wait_geq(done, P, status, &sh.ok)) return;
+    for (int e = tid; e < m * cw; e += nt) {
+        const int r = e % m, q = e / m;
+        g.A[r + (long long)(c0 + q) * g.ld] = cols[r + q * m];
+    }
+}
+
 __global__ void gj_unscramble_kernel(const GJDesc* __restrict__ descs, int m) {
     const GJDesc g = descs[blockIdx.y];
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
@@ -278,7 +599,65 @@ static cudaError_t gj_blocked(const GJDesc* d, int count, int m, int* st, cudaSt
     return cudaGetLastError();
 }
 
-cudaError_t gj_invert_batch(const GJDesc* d_desc, int count, int m, int* d_status, cudaStream_t s) {
+// Resident path: the smallest number of panels per CTA whose grid is co-resident; false when
+// even one CTA per panel group cannot hold the batch (the caller then runs the blocked path).
+template <int NB, int MAXT, int RPT>
+static cudaError_t gj_resident(const GJDesc* d, int count, int m, void* flags, int* st, cudaStream_t s, bool* done) {
+    *done = false;
+    const int threads = ((m + RPT - 1) / RPT + 31) / 32 * 32;
+    if (threads > MAXT) return cudaSuccess;
+    const int npanels = (m + NB - 1) / NB;
+    int dev = 0, nsm = 0, coop = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev)) != cudaSuccess) return e;
+    if (!coop) return cudaSuccess;
+    constexpr int SMEM_MAX = 227 * 1024;
+    static bool attr = false;
+    if (!attr) {
+        e = cudaFuncSetAttribute(gj_resident_kernel<NB, MAXT, RPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 SMEM_MAX - (int)sizeof(ResShared<NB>));
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    for (int ppc = 1; ppc <= npanels; ++ppc) {
+        const int P = (npanels + ppc - 1) / ppc;
+        const size_t sh = ((size_t)m + 2 * NB) * ppc * NB * sizeof(z);
+        if (sh + sizeof(ResShared<NB>) > (size_t)SMEM_MAX) break;
+        int per_sm = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, gj_resident_kernel<NB, MAXT, RPT>, threads, sh);
+        if (e != cudaSuccess) return e;
+        if ((long long)count * P > (long long)per_sm * nsm) continue;
+        if ((e = cudaMemsetAsync(flags, 0, (size_t)count * sizeof(z), s)) != cudaSuccess) return e;
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)(count * P));
+        cfg.blockDim = dim3((unsigned)threads);
+        cfg.dynamicSmemBytes = sh;
+        cfg.stream = s;
+        cudaLaunchAttribute la[1];
+        la[0].id = cudaLaunchAttributeCooperative;
+        la[0].val.cooperative = 1;
+        cfg.attrs = la;
+        cfg.numAttrs = 1;
+        e = cudaLaunchKernelEx(&cfg, gj_resident_kernel<NB, MAXT, RPT>, d, m, npanels, ppc, P, st);
+        if (e != cudaSuccess) return e;
+        note_launch();
+        gj_unscramble_kernel<<<dim3((m + 127) / 128, count), 128, 0, s>>>(d, m);
+        note_launch();
+        *done = true;
+        return cudaGetLastError();
+    }
+    return cudaSuccess;
+}
+
+// RB_GJ_RESIDENT=0 selects the blocked path (read at every launch, so that a process can compare)
+static bool resident_enabled() {
+    const char* v = std::getenv("RB_GJ_RESIDENT");
+    return !(v && v[0] == '0');
+}
+
+cudaError_t gj_invert_batch(const GJDesc* d_desc, int count, int m, void* work, int* d_status, cudaStream_t s) {
     if (count <= 0 || m <= 0) return cudaSuccess;
     if (m <= GJ_SMALL_MAX) {
         const size_t sh = (size_t)m * m * sizeof(z);
@@ -293,8 +672,17 @@ cudaError_t gj_invert_batch(const GJDesc* d_desc, int count, int m, int* d_statu
         note_launch();
         return cudaGetLastError();
     }
-    if (m <= 256) return gj_blocked<16, 256>(d_desc, count, m, d_status, s);
-    if (m <= 512) return gj_blocked<16, 512>(d_desc, count, m, d_status, s);
+    if (resident_enabled() && work) {
+        bool done = false;
+        cudaError_t e = cudaSuccess;
+        if (m <= 128) e = gj_resident<8, 128, 1>(d_desc, count, m, work, d_status, s, &done);
+        else if (m <= 256) e = gj_resident<8, 256, 1>(d_desc, count, m, work, d_status, s, &done);
+        else if (m <= 512) e = gj_resident<8, 512, 1>(d_desc, count, m, work, d_status, s, &done);
+        else if (m <= 1024) e = gj_resident<8, 512, 2>(d_desc, count, m, work, d_status, s, &done);
+        if (e != cudaSuccess || done) return e;
+    }
+    if (m <= 256) return gj_blocked<8, 256>(d_desc, count, m, d_status, s);
+    if (m <= 512) return gj_blocked<8, 512>(d_desc, count, m, d_status, s);
     if (m <= 1024) return gj_blocked<8, 1024>(d_desc, count, m, d_status, s);
     return cudaErrorInvalidValue;
 }

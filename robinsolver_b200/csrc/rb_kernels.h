@@ -19,12 +19,13 @@ struct GJDesc {
     z* A;          // m x m, column-major
     long long ld;
     int* ipiv;     // m
-    z* Zb;         // nb x m workspace (blocked path)
+    z* Zb;         // workspace: the resident path's flag words (gj_workspace_elems)
 };
 constexpr int GJ_SMALL_MAX = 64;
 int gj_panel_width(int m);                         // nb of the blocked path (0 for the small path)
 long long gj_workspace_elems(int m);               // complex elements of Zb per matrix
-cudaError_t gj_invert_batch(const GJDesc* d_desc, int count, int m, int* d_status, cudaStream_t s);
+// work: the count descriptors' Zb areas, contiguous (count * gj_workspace_elems(m) elements)
+cudaError_t gj_invert_batch(const GJDesc* d_desc, int count, int m, void* work, int* d_status, cudaStream_t s);
 
 // ---- leaf stage ---------------------------------------------------------------------------------------
 struct LeafGeom {

@@ -494,7 +494,7 @@ static int run_factor(rb_tree* t, const z* dk) {
         const ChildStore cs = child_store(t, l);
         if ((rc = timer_begin(t, l < 17 ? lvl_names[l] : "merge_deep"))) return rc;
         RB_TIMED("merge_form", 0.0, merge_form_d(cs, p.nnodes, p.m, p.o2, t->zeta, t->dinv[l], s));
-        RB_TIMED("gj_invert", gj_flops(p.m, p.nnodes), gj_invert_batch(t->gj_d[l].d_desc, p.nnodes, p.m, t->d_status, s));
+        RB_TIMED("gj_invert", gj_flops(p.m, p.nnodes), gj_invert_batch(t->gj_d[l].d_desc, p.nnodes, p.m, t->gj_work, t->d_status, s));
         // Y2R = inv(D) T2_iN needs only inv(D): on the second stream it overlaps the S inversion
         const bool fork = t->timing == 0;
         if (fork) {
@@ -504,7 +504,7 @@ static int run_factor(rb_tree* t, const z* dk) {
             RB_CK(cudaEventRecord(t->ev_join[l], t->stream2));
         }
         RB_TIMED("merge_form", 0.0, merge_form_s(cs, p.nnodes, p.m, p.o1, t->zeta, t->nu, t->dinv[l], t->sinv[l], s));
-        RB_TIMED("gj_invert", gj_flops(p.m, p.nnodes), gj_invert_batch(t->gj_s[l].d_desc, p.nnodes, p.m, t->d_status, s));
+        RB_TIMED("gj_invert", gj_flops(p.m, p.nnodes), gj_invert_batch(t->gj_s[l].d_desc, p.nnodes, p.m, t->gj_work, t->d_status, s));
         if (fork) RB_CK(cudaStreamWaitEvent(s, t->ev_join[l], 0));
         else RB_TIMED("zgemm", t->fM1[l].flops, launch_gemm_batch(t->fM1[l], s));
         RB_TIMED("zgemm", t->fM2[l].flops, launch_gemm_batch(t->fM2[l], s));

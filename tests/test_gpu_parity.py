@@ -106,6 +106,20 @@ def test_skip_root_rtr_gives_the_same_solution():
     Ts.close()
 
 
+@pytest.mark.parametrize("cfg", [2, pytest.param(4, marks=pytest.mark.slow)])
+def test_resident_gauss_jordan_equals_blocked_bitwise(cfg, monkeypatch):
+    """The one-launch resident inversion performs the blocked path's arithmetic in the same order:
+    solutions agree bit for bit (config 2 reaches interface sizes 128-512, config 4 also 1024)."""
+    wl = W.make_workload(cfg, nrhs=1)
+    sols = {}
+    for flag in ("0", "1"):
+        monkeypatch.setenv("RB_GJ_RESIDENT", flag)
+        T = _factored(wl)
+        sols[flag] = _solve(T, wl.rhs[:1])
+        T.close()
+    assert np.array_equal(sols["0"], sols["1"])
+
+
 @pytest.mark.slow
 def test_config2_matches_oracle():
     wl = W.make_workload(2)
