@@ -6,17 +6,18 @@
 // Gauss-Jordan elimination with partial pivoting, so that later applications are GEMMs.
 // Pivots are chosen as LAPACK's izamax does: largest |re|+|im| in the column, first on ties.
 //
-// m <= 64: one CTA per matrix holds the whole matrix in shared memory.
-// m  > 64: blocked Gauss-Jordan.  Per panel of nb columns:
-//   1. gj_panel: one CTA per matrix, one matrix row per thread in registers, runs the
-//      unblocked elimination on the panel (pivot search below the diagonal, row exchange,
-//      scaling, elimination of every other row), leaving the accumulated transform W in the
-//      panel columns;
-//   2. gj_apply: for every other column, applies the panel's row exchanges and then
+// m <= 32: one CTA per matrix holds the whole matrix in shared memory (gj_small).
+// m  > 32: blocked Gauss-Jordan by panels of nb = 8 columns.  Per panel:
+//   1. elimination of the panel: the pivot search below the diagonal, row exchange, scaling and
+//      elimination of every other row, leaving the accumulated transform W in the panel columns;
+//   2. update of every other column: the panel's row exchanges, then
 //      A[i, rest] += W[i,:] Z for rows outside the panel and A[P, rest] = W_P Z for the panel
 //      rows, Z = A[P, rest] after the exchanges.  (Writing the panel rows as Z + (W_P - I) Z
 //      instead cancels catastrophically: W_P's diagonal holds the reciprocal pivots, ~h^2 for
 //      the FD matrices here.)
+//   The resident kernel (gj_resident) runs the whole batch in one cooperative launch with the
+//   columns held in shared memory; gj_panel + gj_apply, two launches per panel, are the same
+//   arithmetic in the same order, used when the batch does not fit on the device at once.
 // After the last panel the column exchanges are undone in reverse order (gj_unscramble).
 #include <cstdlib>
 #include "rb_gemm_tile.cuh"
@@ -25,12 +26,12 @@
 namespace rb {
 
 int gj_panel_width(int m) {
-    if (m <= GJ_SMALL_MAX) return 0;
+    if (m < GJ_BLOCKED_MIN) return 0;
     return 8;
 }
 
 // one complex element per matrix: the resident path's two flag words
-long long gj_workspace_elems(int m) { return m <= GJ_SMALL_MAX ? 0 : 1; }
+long long gj_workspace_elems(int m) { return m < GJ_BLOCKED_MIN ? 0 : 1; }
 
 // warp argmax: larger value wins, equal values go to the smaller index
 __device__ __forceinline__ void argmax_warp(double& v, int& i) {
@@ -659,7 +660,7 @@ static bool resident_enabled() {
 
 cudaError_t gj_invert_batch(const GJDesc* d_desc, int count, int m, void* work, int* d_status, cudaStream_t s) {
     if (count <= 0 || m <= 0) return cudaSuccess;
-    if (m <= GJ_SMALL_MAX) {
+    if (m < GJ_BLOCKED_MIN) {
         const size_t sh = (size_t)m * m * sizeof(z);
         static bool attr = false;
         if (!attr) {
@@ -675,12 +676,14 @@ cudaError_t gj_invert_batch(const GJDesc* d_desc, int count, int m, void* work, 
     if (resident_enabled() && work) {
         bool done = false;
         cudaError_t e = cudaSuccess;
-        if (m <= 128) e = gj_resident<8, 128, 1>(d_desc, count, m, work, d_status, s, &done);
+        if (m <= 64) e = gj_resident<8, 64, 1>(d_desc, count, m, work, d_status, s, &done);
+        else if (m <= 128) e = gj_resident<8, 128, 1>(d_desc, count, m, work, d_status, s, &done);
         else if (m <= 256) e = gj_resident<8, 256, 1>(d_desc, count, m, work, d_status, s, &done);
         else if (m <= 512) e = gj_resident<8, 512, 1>(d_desc, count, m, work, d_status, s, &done);
         else if (m <= 1024) e = gj_resident<8, 512, 2>(d_desc, count, m, work, d_status, s, &done);
         if (e != cudaSuccess || done) return e;
     }
+    if (m <= 64) return gj_blocked<8, 64>(d_desc, count, m, d_status, s);
     if (m <= 256) return gj_blocked<8, 256>(d_desc, count, m, d_status, s);
     if (m <= 512) return gj_blocked<8, 512>(d_desc, count, m, d_status, s);
     if (m <= 1024) return gj_blocked<8, 1024>(d_desc, count, m, d_status, s);

@@ -21,7 +21,8 @@ struct GJDesc {
     int* ipiv;     // m
     z* Zb;         // workspace: the resident path's flag words (gj_workspace_elems)
 };
-constexpr int GJ_SMALL_MAX = 64;
+constexpr int GJ_SMALL_MAX = 64;       // largest matrix the whole-matrix kernel holds
+constexpr int GJ_BLOCKED_MIN = 33;     // from this size on: resident (else blocked) path
 int gj_panel_width(int m);                         // nb of the blocked path (0 for the small path)
 long long gj_workspace_elems(int m);               // complex elements of Zb per matrix
 // work: the count descriptors' Zb areas, contiguous (count * gj_workspace_elems(m) elements)
