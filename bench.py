@@ -283,31 +283,21 @@ def zgemm_peak_tflops(torch, dev):
 
 def our_arm(args):
     import torch
-    import torch.distributed as dist
 
     import robinsolver_b200 as rb
     from robinsolver_b200 import _lib
     from robinsolver_b200 import workloads as W
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
+    from robinsolver_b200.replicas import Replicas
+
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    # replicas only: each rank runs the whole workload on its GPU; no data-path collective
+    rep = Replicas("nccl", device=dev, timeout_s=300)
+    world, rank = rep.world, rep.rank
+    barrier = rep.barrier
+    max_over_ranks = rep.max
 
     nrhs = args.nrhs or W.CONFIGS[args.config]["nrhs"]
     wl = W.make_workload(args.config, nrhs=nrhs)
@@ -364,8 +354,7 @@ def our_arm(args):
     fl, sl = T.launch_counts()
     launches = (fl + sl) * args.steps
     step_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
-    total_ms = max_over_ranks(ev[0].elapsed_time(ev[-1]))
-    value = world * nrhs * args.steps / (total_ms * 1e-3)
+    value, total_ms = rep.rate(nrhs * args.steps, ev[0].elapsed_time(ev[-1]))
 
     # factor / solve split from the library's own events on the last step
     T.factor_samples(kv)
@@ -468,8 +457,7 @@ def our_arm(args):
         }
         print(json.dumps(out), flush=True)
     T.close()
-    if world > 1:
-        dist.destroy_process_group()
+    rep.close()
     return 0
 
 
