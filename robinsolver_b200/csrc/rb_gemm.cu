@@ -6,7 +6,9 @@
 // Robin-to-Robin matrix) and the scatter into the parent's face order happen inside the loads
 // and the epilogue instead of in copy kernels.
 //
-// FP64 has no tcgen05 kind; the arithmetic is DFMA with register tiling (rb_gemm_tile.cuh).
+// FP64 has no tcgen05 kind: the large problems run on the FP64 tensor-core MMA
+// (mma.sync m8n8k4 .f64, rb_gemm_dmma.cuh), the small ones and the solve on DFMA register tiles
+// (rb_gemm_tile.cuh).
 #include <cstdlib>
 #include <cstring>
 
@@ -31,8 +33,8 @@ zgemm_desc_kernel(const GemmDesc* __restrict__ descs) {
     zgemm_tile<BM, BN, TM, TN, BK, STAGES>(sd, blockIdx.x, dfma_smem);
 }
 
-template <int BM, int BN, int WM, int WN>
-__global__ void __launch_bounds__(32 * WM * WN, 1) zgemm_dmma_kernel(const GemmDesc* __restrict__ descs) {
+template <int BM, int BN, int WM, int WN, int MINB>
+__global__ void __launch_bounds__(32 * WM * WN, MINB) zgemm_dmma_kernel(const GemmDesc* __restrict__ descs) {
     extern __shared__ z dmma_smem[];
     __shared__ GemmDesc sd;
     {
@@ -44,13 +46,17 @@ __global__ void __launch_bounds__(32 * WM * WN, 1) zgemm_dmma_kernel(const GemmD
     zgemm_tile_dmma<BM, BN, WM, WN>(sd, blockIdx.x, dmma_smem);
 }
 
-template <int BM, int BN, int WM, int WN>
+// MINB CTAs per SM: the carveout is set to the largest shared-memory share so that they fit
+template <int BM, int BN, int WM, int WN, int MINB>
 static cudaError_t launch_dmma(const GemmBatch& b, cudaStream_t s) {
     using Cfg = DmmaCfg<BM, BN, WM, WN>;
     static bool attr = false;
     if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(zgemm_dmma_kernel<BM, BN, WM, WN>,
+        cudaError_t e = cudaFuncSetAttribute(zgemm_dmma_kernel<BM, BN, WM, WN, MINB>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(zgemm_dmma_kernel<BM, BN, WM, WN, MINB>,
+                                 cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
         if (e != cudaSuccess) return e;
         attr = true;
     }
@@ -58,7 +64,7 @@ static cudaError_t launch_dmma(const GemmBatch& b, cudaStream_t s) {
     for (int off = 0; off < b.count; off += 65535) {
         const int cnt = (b.count - off) < 65535 ? (b.count - off) : 65535;
         dim3 grid(tiles, cnt);
-        zgemm_dmma_kernel<BM, BN, WM, WN><<<grid, Cfg::NT, Cfg::SMEM_BYTES, s>>>(b.d_desc + off);
+        zgemm_dmma_kernel<BM, BN, WM, WN, MINB><<<grid, Cfg::NT, Cfg::SMEM_BYTES, s>>>(b.d_desc + off);
         note_launch();
     }
     return cudaGetLastError();
@@ -108,10 +114,10 @@ cudaError_t launch_gemm_batch(const GemmBatch& b, cudaStream_t s) {
         return launch_cfg<16, 16, 2, 2, 8, 6, 8>(b, s);
     if (mm <= 32 || nn <= 32) return launch_cfg<32, 32, 4, 2, 8, 4, 4>(b, s);
     const bool big = mm >= 256 && nn >= 128 && (long long)b.count * ((mm + 127) / 128) * ((nn + 63) / 64) >= 148;
-    if (use_dmma() && !b.fixed_order) {
-        if (big) return launch_dmma<128, 64, 4, 2>(b, s);
-        return launch_dmma<64, 64, 2, 4>(b, s);
-    }
+    // FP64 tensor cores: 64x64 tiles of 8 warps, two CTAs per SM (16 warps to hide the MMA and
+    // shared-memory latencies); measured faster than 128x64 tiles at one CTA per SM on every
+    // merge shape from 64x256x64 x256 to 2048x4096x1024 x2
+    if (use_dmma() && !b.fixed_order) return launch_dmma<64, 64, 2, 4, 2>(b, s);
     // large problems: 8x4 complex register tile per thread (1.5 B of shared memory per DFMA)
     if (big) return launch_cfg<128, 64, 8, 4, 4, 4, 1>(b, s);
     return launch_cfg<64, 64, 4, 4, 8, 4, 1>(b, s);

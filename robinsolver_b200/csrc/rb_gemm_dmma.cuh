@@ -36,7 +36,7 @@ template <int BM, int BN, int WM, int WN>
 struct DmmaCfg {
     static constexpr int NT = 32 * WM * WN;     // threads
     static constexpr int BK = 8;                // complex k per stage (2 MMA k-steps)
-    static constexpr int STAGES = 3;
+    static constexpr int STAGES = 4;
     static constexpr int LDA = BM + 2;          // complex elements per k-row of an A stage
     static constexpr int LDB = BN + 2;
     static constexpr int TMW = BM / WM / 8;     // MMA tiles per warp along M
