@@ -43,6 +43,12 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "Factor time + solves/s on 1024² 2D Helmholtz, mixed vs FP64 GPU @1e-10; p99 ms"
 
+# DRAM bytes (read + write) per launch of each stage's kernels in one step of the 1024^2 / L=12
+# workload, from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, one pass):
+# profiles/zgemm_tc_1024sq_L12_fp64.md.  ncu cannot run inside this script, so the figure is
+# carried here and reported for the bench's own workload only.
+DRAM_BYTES_PER_LAUNCH = {4: {"zgemm_tc": 2.356e8, "zgemm_dfma": 6.45e7}}
+
 
 def parse():
     ap = argparse.ArgumentParser()
@@ -444,8 +450,11 @@ def our_arm(args):
             "backward_error": bw,
             "roofline": {
                 "bound": "tensor", "pipe": "fp64", "kernel": dname, "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None, "traffic": None,
+                "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None,
+                "traffic": DRAM_BYTES_PER_LAUNCH.get(args.config, {}).get(dname),
                 "launches": dcnt, "ms_total": dms, "share_of_step": shares.get(dname),
+                "flop_count": "algorithmic 8mnk per complex GEMM (the tensor-core kernel issues three real "
+                              "MMAs per complex product, so achieved can exceed a four-product peak)",
                 "peak_source": "complex128 cuBLAS GEMM 4096^3 measured in this run (no FP64 entry in "
                                "MEASURED_PEAKS.json)",
                 "shares": shares,

@@ -102,24 +102,39 @@ static cudaError_t launch_cfg(const GemmBatch& b, cudaStream_t s) {
     return cudaGetLastError();
 }
 
-cudaError_t launch_gemm_batch(const GemmBatch& b, cudaStream_t s) {
-    static_assert(sizeof(GemmDesc) % 8 == 0, "descriptor copy assumes 8-byte words");
-    if (b.count == 0 || b.max_m == 0 || b.max_n == 0) return cudaSuccess;
+// the kernel shape a batch runs on
+enum class GemmShape { Dfma16, Dfma32, Dmma64, Dfma128x64, Dfma64 };
+static GemmShape gemm_shape(const GemmBatch& b) {
     const int mm = b.max_m, nn = b.max_n;
-    if (mm <= 16 && nn <= 16) return launch_cfg<16, 16, 2, 2, 8, 6, 8>(b, s);
+    if (mm <= 16 && nn <= 16) return GemmShape::Dfma16;
     // every DFMA shape sums an element's products in the same order, so the shape can follow the
     // available parallelism: small-n batches (the solve) that would leave SMs idle with 32x32
     // tiles take 16x16 tiles
-    if (nn <= 32 && (long long)b.count * ((mm + 31) / 32) * ((nn + 31) / 32) < 2 * 148)
-        return launch_cfg<16, 16, 2, 2, 8, 6, 8>(b, s);
-    if (mm <= 32 || nn <= 32) return launch_cfg<32, 32, 4, 2, 8, 4, 4>(b, s);
-    const bool big = mm >= 256 && nn >= 128 && (long long)b.count * ((mm + 127) / 128) * ((nn + 63) / 64) >= 148;
+    if (nn <= 32 && (long long)b.count * ((mm + 31) / 32) * ((nn + 31) / 32) < 2 * 148) return GemmShape::Dfma16;
+    if (mm <= 32 || nn <= 32) return GemmShape::Dfma32;
     // FP64 tensor cores: 64x64 tiles of 8 warps, two CTAs per SM (16 warps to hide the MMA and
     // shared-memory latencies); measured faster than 128x64 tiles at one CTA per SM on every
     // merge shape from 64x256x64 x256 to 2048x4096x1024 x2
-    if (use_dmma() && !b.fixed_order) return launch_dmma<64, 64, 2, 4, 2>(b, s);
+    if (use_dmma() && !b.fixed_order) return GemmShape::Dmma64;
     // large problems: 8x4 complex register tile per thread (1.5 B of shared memory per DFMA)
-    if (big) return launch_cfg<128, 64, 8, 4, 4, 4, 1>(b, s);
+    const bool big = mm >= 256 && nn >= 128 && (long long)b.count * ((mm + 127) / 128) * ((nn + 63) / 64) >= 148;
+    return big ? GemmShape::Dfma128x64 : GemmShape::Dfma64;
+}
+
+const char* gemm_stage_name(const GemmBatch& b) {
+    return gemm_shape(b) == GemmShape::Dmma64 ? "zgemm_tc" : "zgemm_dfma";
+}
+
+cudaError_t launch_gemm_batch(const GemmBatch& b, cudaStream_t s) {
+    static_assert(sizeof(GemmDesc) % 8 == 0, "descriptor copy assumes 8-byte words");
+    if (b.count == 0 || b.max_m == 0 || b.max_n == 0) return cudaSuccess;
+    switch (gemm_shape(b)) {
+        case GemmShape::Dfma16: return launch_cfg<16, 16, 2, 2, 8, 6, 8>(b, s);
+        case GemmShape::Dfma32: return launch_cfg<32, 32, 4, 2, 8, 4, 4>(b, s);
+        case GemmShape::Dmma64: return launch_dmma<64, 64, 2, 4, 2>(b, s);
+        case GemmShape::Dfma128x64: return launch_cfg<128, 64, 8, 4, 4, 4, 1>(b, s);
+        case GemmShape::Dfma64: break;
+    }
     return launch_cfg<64, 64, 4, 4, 8, 4, 1>(b, s);
 }
 

@@ -13,6 +13,8 @@ void set_thread_error(const char* msg);
 
 // ---- batched GEMM ---------------------------------------------------------------------------------
 cudaError_t launch_gemm_batch(const GemmBatch& b, cudaStream_t s);
+// stage-timer name of the engine a batch runs on: "zgemm_tc" (FP64 tensor cores) or "zgemm_dfma"
+const char* gemm_stage_name(const GemmBatch& b);
 
 // ---- batched Gauss-Jordan inversion (in place, partial pivoting by |re|+|im|) ----------------------
 struct GJDesc {

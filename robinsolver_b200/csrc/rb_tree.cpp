@@ -468,6 +468,9 @@ static int ensure_factor_storage(rb_tree* t) {
         if ((rc_ = ltimer_end(t))) return rc_;                                                   \
     } while (0)
 
+// a GEMM batch, timed under the name of the engine it runs on
+#define RB_GEMM(batch, stream) RB_TIMED(gemm_stage_name(batch), (batch).flops, launch_gemm_batch(batch, stream))
+
 static double gj_flops(int m, int count) { return 8.0 * (double)m * m * m * count; }
 // arithmetic of one structured leaf factor: b block inverses (8 a^3 each) and two block sweeps
 // of S^T Z = C^T with nb right-hand sides (8 a^2 nb per block and sweep)
@@ -506,10 +509,10 @@ static int run_factor(rb_tree* t, const z* dk) {
         RB_TIMED("merge_form", 0.0, merge_form_s(cs, p.nnodes, p.m, p.o1, t->zeta, t->nu, t->dinv[l], t->sinv[l], s));
         RB_TIMED("gj_invert", gj_flops(p.m, p.nnodes), gj_invert_batch(t->gj_s[l].d_desc, p.nnodes, p.m, t->gj_work, t->d_status, s));
         if (fork) RB_CK(cudaStreamWaitEvent(s, t->ev_join[l], 0));
-        else RB_TIMED("zgemm", t->fM1[l].flops, launch_gemm_batch(t->fM1[l], s));
-        RB_TIMED("zgemm", t->fM2[l].flops, launch_gemm_batch(t->fM2[l], s));
-        RB_TIMED("zgemm", t->fM3[l].flops, launch_gemm_batch(t->fM3[l], s));
-        RB_TIMED("zgemm", t->fM4[l].flops, launch_gemm_batch(t->fM4[l], s));
+        else RB_GEMM(t->fM1[l], s);
+        RB_GEMM(t->fM2[l], s);
+        RB_GEMM(t->fM3[l], s);
+        RB_GEMM(t->fM4[l], s);
         if ((rc = timer_end(t))) return rc;
     }
     return RB_OK;
@@ -645,12 +648,12 @@ static int run_solve(rb_tree* t, int k) {
     cudaStream_t s = t->stream;
     int rc;
     if ((rc = timer_begin(t, "forward"))) return rc;
-    RB_TIMED("zgemm", t->sL0.flops, launch_gemm_batch(t->sL0, s));
+    RB_GEMM(t->sL0, s);
     for (int l = L - 1; l >= 0; --l) {
-        RB_TIMED("zgemm", t->sF12[l].flops, launch_gemm_batch(t->sF12[l], s));
-        RB_TIMED("zgemm", t->sF3[l].flops, launch_gemm_batch(t->sF3[l], s));
-        RB_TIMED("zgemm", t->sF4[l].flops, launch_gemm_batch(t->sF4[l], s));
-        if (l > 0) RB_TIMED("zgemm", t->sF5[l].flops, launch_gemm_batch(t->sF5[l], s));
+        RB_GEMM(t->sF12[l], s);
+        RB_GEMM(t->sF3[l], s);
+        RB_GEMM(t->sF4[l], s);
+        if (l > 0) RB_GEMM(t->sF5[l], s);
     }
     if ((rc = timer_end(t))) return rc;
     if ((rc = timer_begin(t, "backward"))) return rc;
@@ -658,10 +661,10 @@ static int run_solve(rb_tree* t, int k) {
         const PlanLevel& p = P.lv[l];
         RB_TIMED("sweep_aux", 0.0, sweep_scatter_down(p.nnodes, k, p.nb, p.nbc, p.m, p.o1, p.o2, p.n1, p.n2, t->d_pmap1[l],
                                      t->d_pmap2[l], t->gbuf[l], t->gbuf[l + 1], s));
-        RB_TIMED("zgemm", t->sB1[l].flops, launch_gemm_batch(t->sB1[l], s));
-        RB_TIMED("zgemm", t->sB23[l].flops, launch_gemm_batch(t->sB23[l], s));
-        RB_TIMED("zgemm", t->sB4[l].flops, launch_gemm_batch(t->sB4[l], s));
-        RB_TIMED("zgemm", t->sB5[l].flops, launch_gemm_batch(t->sB5[l], s));
+        RB_GEMM(t->sB1[l], s);
+        RB_GEMM(t->sB23[l], s);
+        RB_GEMM(t->sB4[l], s);
+        RB_GEMM(t->sB5[l], s);
         RB_TIMED("sweep_aux", 0.0, sweep_add_interface(p.nnodes, k, p.nbc, p.m, p.o1, p.o2, t->tmp, t->gbuf[l + 1], s));
     }
     if ((rc = timer_end(t))) return rc;
