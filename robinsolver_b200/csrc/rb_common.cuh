@@ -101,6 +101,13 @@ struct GemmBatch {
     // DFMA kernels only: every DFMA tile shape accumulates an element's k-sum in the same order,
     // so results do not depend on the batch's sizes (used for the solve, whose n = RHS count)
     bool fixed_order = false;
+    // split-K (fixed-order batches only): k is cut into ksplit ranges of kchunk, whose raw sums
+    // go to work (pstride elements per range and problem, ld max_m) and are then added in range
+    // order.  ksplit depends on count, m and k only, never on n.
+    int ksplit = 1;
+    int kchunk = 0;
+    z* work = nullptr;
+    long long pstride = 0;
 };
 
 }  // namespace rb

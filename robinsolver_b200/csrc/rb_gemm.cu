@@ -9,6 +9,7 @@
 // FP64 has no tcgen05 kind: the large problems run on the FP64 tensor-core MMA
 // (mma.sync m8n8k4 .f64, rb_gemm_dmma.cuh), the small ones and the solve on DFMA register tiles
 // (rb_gemm_tile.cuh).
+#include <algorithm>
 #include <cstdlib>
 #include <cstring>
 
@@ -31,6 +32,40 @@ zgemm_desc_kernel(const GemmDesc* __restrict__ descs) {
     }
     __syncthreads();
     zgemm_tile<BM, BN, TM, TN, BK, STAGES>(sd, blockIdx.x, dfma_smem);
+}
+
+// split-K pass: blockIdx.z picks the k range; raw sums go to the batch's workspace
+template <int BM, int BN, int TM, int TN, int BK, int STAGES, int MINB>
+__global__ void __launch_bounds__((BM / TM) * (BN / TN), MINB)
+zgemm_split_kernel(const GemmDesc* __restrict__ descs, int kchunk, z* work, long long pstride, int ldp, int ksplit) {
+    constexpr int NT = (BM / TM) * (BN / TN);
+    extern __shared__ z dfma_smem[];
+    __shared__ GemmDesc sd;
+    {
+        const unsigned long long* src = reinterpret_cast<const unsigned long long*>(descs + blockIdx.y);
+        unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sd);
+        for (int w = threadIdx.x; w < (int)(sizeof(GemmDesc) / 8); w += NT) dst[w] = src[w];
+    }
+    __syncthreads();
+    const int kb = blockIdx.z * kchunk;
+    z* part = work + ((long long)blockIdx.y * ksplit + blockIdx.z) * pstride;
+    zgemm_tile<BM, BN, TM, TN, BK, STAGES, true>(sd, blockIdx.x, dfma_smem, kb, kb + kchunk, part, ldp);
+}
+
+// split-K reduction: the ranges' sums added in range order, then the usual epilogue
+__global__ void __launch_bounds__(256) zgemm_reduce_kernel(const GemmDesc* __restrict__ descs, const z* __restrict__ work,
+                                                          long long pstride, int ldp, int ksplit) {
+    const GemmDesc& g = descs[blockIdx.y];
+    const int m = g.m, n = g.n;
+    const long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= (long long)m * n) return;
+    const int i = (int)(e % m), j = (int)(e / m);
+    const z* p = work + (long long)blockIdx.y * ksplit * pstride + i + (long long)j * ldp;
+    z acc = p[0];
+    for (int r = 1; r < ksplit; ++r) acc = zadd(acc, p[r * pstride]);
+    z v = zmul(g.alpha, acc);
+    if (g.C.p && !(i >= g.nobeta_r0 && i < g.nobeta_r1)) zfma(v, g.beta, g.C.p[vrow(g.C, i) + (long long)vcol(g.C, j) * g.C.ld]);
+    g.D.p[vrow(g.D, i) + (long long)vcol(g.D, j) * g.D.ld] = v;
 }
 
 template <int BM, int BN, int WM, int WN, int MINB>
@@ -102,6 +137,29 @@ static cudaError_t launch_cfg(const GemmBatch& b, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+template <int BM, int BN, int TM, int TN, int BK, int STAGES, int MINB>
+static cudaError_t launch_split(const GemmBatch& b, cudaStream_t s) {
+    constexpr int NT = (BM / TM) * (BN / TN);
+    constexpr size_t SMEM = DfmaCfg<BM, BN, BK, STAGES>::SMEM_BYTES;
+    static bool attr = false;
+    if (!attr && SMEM > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(zgemm_split_kernel<BM, BN, TM, TN, BK, STAGES, MINB>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+        if (e != cudaSuccess) return e;
+    }
+    attr = true;
+    if (b.count > 65535 || b.ksplit > 65535) return cudaErrorInvalidValue;
+    const int tiles = ((b.max_m + BM - 1) / BM) * ((b.max_n + BN - 1) / BN);
+    zgemm_split_kernel<BM, BN, TM, TN, BK, STAGES, MINB><<<dim3(tiles, b.count, b.ksplit), NT, SMEM, s>>>(
+        b.d_desc, b.kchunk, b.work, b.pstride, b.max_m, b.ksplit);
+    note_launch();
+    const long long elems = (long long)b.max_m * b.max_n;
+    zgemm_reduce_kernel<<<dim3((unsigned)((elems + 255) / 256), b.count), 256, 0, s>>>(b.d_desc, b.work, b.pstride,
+                                                                                     b.max_m, b.ksplit);
+    note_launch();
+    return cudaGetLastError();
+}
+
 // the kernel shape a batch runs on
 enum class GemmShape { Dfma16, Dfma32, Dmma64, Dfma128x64, Dfma64 };
 static GemmShape gemm_shape(const GemmBatch& b) {
@@ -121,6 +179,31 @@ static GemmShape gemm_shape(const GemmBatch& b) {
     return big ? GemmShape::Dfma128x64 : GemmShape::Dfma64;
 }
 
+long long gemm_plan_split(GemmBatch& b) {
+    b.ksplit = 1;
+    b.kchunk = 0;
+    b.pstride = 0;
+    // fixed-order batches always run on DFMA tiles, whose shapes share one summation order, so
+    // the split (and the rounding) depends on count, m and k only
+    if (!b.fixed_order || b.count == 0 || b.max_k < 128) return 0;
+    // CTAs with one column tile (n-independent), against about four waves of two CTAs per SM
+    const long long ctas = (long long)b.count * ((b.max_m + 15) / 16);
+    long long sp = (4 * 148 + ctas - 1) / ctas;
+    sp = std::min<long long>(sp, 16);
+    sp = std::min<long long>(sp, b.max_k / 64);
+    if (sp < 2) return 0;
+    const int kc = (int)(((b.max_k + sp - 1) / sp + 7) / 8 * 8);
+    b.kchunk = kc;
+    b.ksplit = (b.max_k + kc - 1) / kc;
+    if (b.ksplit < 2) {
+        b.ksplit = 1;
+        b.kchunk = 0;
+        return 0;
+    }
+    b.pstride = (long long)b.max_m * b.max_n;
+    return (long long)b.count * b.ksplit * b.pstride;
+}
+
 const char* gemm_stage_name(const GemmBatch& b) {
     return gemm_shape(b) == GemmShape::Dmma64 ? "zgemm_tc" : "zgemm_dfma";
 }
@@ -128,7 +211,14 @@ const char* gemm_stage_name(const GemmBatch& b) {
 cudaError_t launch_gemm_batch(const GemmBatch& b, cudaStream_t s) {
     static_assert(sizeof(GemmDesc) % 8 == 0, "descriptor copy assumes 8-byte words");
     if (b.count == 0 || b.max_m == 0 || b.max_n == 0) return cudaSuccess;
-    switch (gemm_shape(b)) {
+    const GemmShape shape = gemm_shape(b);
+    if (b.ksplit > 1 && b.work) {
+        if (shape == GemmShape::Dfma16) return launch_split<16, 16, 2, 2, 8, 6, 8>(b, s);
+        if (shape == GemmShape::Dfma32) return launch_split<32, 32, 4, 2, 8, 4, 4>(b, s);
+        if (shape == GemmShape::Dfma128x64) return launch_split<128, 64, 8, 4, 4, 4, 1>(b, s);
+        if (shape == GemmShape::Dfma64) return launch_split<64, 64, 4, 4, 8, 4, 1>(b, s);
+    }
+    switch (shape) {
         case GemmShape::Dfma16: return launch_cfg<16, 16, 2, 2, 8, 6, 8>(b, s);
         case GemmShape::Dfma32: return launch_cfg<32, 32, 4, 2, 8, 4, 4>(b, s);
         case GemmShape::Dmma64: return launch_dmma<64, 64, 2, 4, 2>(b, s);

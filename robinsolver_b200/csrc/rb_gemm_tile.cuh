@@ -19,8 +19,11 @@ struct DfmaCfg {
     static constexpr size_t SMEM_BYTES = (size_t)STAGES * STAGE_Z * sizeof(z);
 };
 
-template <int BM, int BN, int TM, int TN, int BK, int STAGES>
-__device__ __forceinline__ void zgemm_tile(const GemmDesc& sd, int tile, z* smem) {
+// With PARTIAL, only k in [kbeg, kend) is summed and the raw sums go to part (element (i, j) at
+// part[i + j * ldp]) for a later fixed-order reduction over the k ranges (split-K).
+template <int BM, int BN, int TM, int TN, int BK, int STAGES, bool PARTIAL = false>
+__device__ __forceinline__ void zgemm_tile(const GemmDesc& sd, int tile, z* smem, int kbeg = 0, int kend = 0,
+                                           z* part = nullptr, int ldp = 0) {
     using Cfg = DfmaCfg<BM, BN, BK, STAGES>;
     constexpr int NT = (BM / TM) * (BN / TN);
     constexpr int RG = BM / TM;
@@ -31,7 +34,9 @@ __device__ __forceinline__ void zgemm_tile(const GemmDesc& sd, int tile, z* smem
     static_assert(A_PER * NT == BM * BK && B_PER * NT == BK * BN, "tile/thread mismatch");
 
     const int tid = threadIdx.x;
-    const int m = sd.m, n = sd.n, K = sd.k;
+    const int m = sd.m, n = sd.n;
+    const int K = PARTIAL ? min(sd.k, kend) : sd.k;
+    const int kb0 = PARTIAL ? kbeg : 0;
     const int tiles_m = (m + BM - 1) / BM;
     const int tmi = tile % tiles_m;
     const int tni = tile / tiles_m;
@@ -55,11 +60,11 @@ __device__ __forceinline__ void zgemm_tile(const GemmDesc& sd, int tile, z* smem
         bcol_ok[e] = j < n;
         bcol[e] = bcol_ok[e] ? (long long)vcol(B, j) * B.ld : 0;
     }
-    const int ktiles = (K + BK - 1) / BK;
+    const int ktiles = K > kb0 ? (K - kb0 + BK - 1) / BK : 0;
     auto issue = [&](int kt) {
         z* As = smem + (kt % STAGES) * Cfg::STAGE_Z;
         z* Bs = As + BK * BM;
-        const int k0 = kt * BK;
+        const int k0 = kb0 + kt * BK;
 #pragma unroll
         for (int e = 0; e < A_PER; ++e) {
             const int kk = akk0 + e * (NT / BM);
@@ -114,6 +119,19 @@ __device__ __forceinline__ void zgemm_tile(const GemmDesc& sd, int tile, z* smem
     }
     cp_async_wait<0>();
 
+    if (PARTIAL) {
+#pragma unroll
+        for (int i = 0; i < TM; ++i) {
+            const int gi = m0 + tr + i * RG;
+            if (gi >= m) continue;
+#pragma unroll
+            for (int j = 0; j < TN; ++j) {
+                const int gj = n0 + tc + j * CG;
+                if (gj < n) part[gi + (long long)gj * ldp] = acc[i][j];
+            }
+        }
+        return;
+    }
     const z alpha = sd.alpha, beta = sd.beta;
     const ZView C = sd.C;
     const ZOut D = sd.D;

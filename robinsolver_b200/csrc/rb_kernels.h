@@ -13,6 +13,9 @@ void set_thread_error(const char* msg);
 
 // ---- batched GEMM ---------------------------------------------------------------------------------
 cudaError_t launch_gemm_batch(const GemmBatch& b, cudaStream_t s);
+// Chooses split-K for a fixed-order batch (sets ksplit, kchunk, pstride) and returns the
+// workspace it needs in complex elements (0: no split); the caller sets b.work.
+long long gemm_plan_split(GemmBatch& b);
 // stage-timer name of the engine a batch runs on: "zgemm_tc" (FP64 tensor cores) or "zgemm_dfma"
 const char* gemm_stage_name(const GemmBatch& b);
 

@@ -395,6 +395,8 @@ __global__ void __launch_bounds__(128) leaf_warp_factor_kernel(LeafGeom g, int n
         if (live) leaf_bpoint2(A, b, c, ax, q1, q2);
         const double hr = ax == 0 ? L.hx : L.hy;
         const double c1 = -3.0 / hr, c2 = (1.0 / 3.0) / hr;
+        // Y(c, nb+s) = f_c Q(c, s): the backward sweep stores its final values already scaled
+        const z fc = zmul(zmk(0.0, 2.0 * g.kb), ax == 0 ? L.rdx : L.rdy);
         z v[A];
 #pragma unroll
         for (int i = 0; i < A; ++i) v[i] = zmk(0.0, 0.0);
@@ -423,6 +425,10 @@ __global__ void __launch_bounds__(128) leaf_warp_factor_kernel(LeafGeom g, int n
             }
         }
         // backward: z_{j-1} = v_{j-1} - Sig_{j-1}^-T Lo_j z_j, z_{b-1} = v_{b-1}
+        if (live) {
+#pragma unroll
+            for (int i = 0; i < A; ++i) Yl[c + (size_t)(nb + (b - 1) * A + i) * nb] = zmul(fc, v[i]);
+        }
         for (int j = b - 1; j >= 1; --j) {
             const z lam = block_lo(L, b, j + 1);
             __syncwarp();
@@ -438,34 +444,25 @@ __global__ void __launch_bounds__(128) leaf_warp_factor_kernel(LeafGeom g, int n
 #pragma unroll
                 for (int q = 0; q < A; ++q) zfms(acc, sm[q + i * A], lz[q]);
                 v[i] = acc;
-                if (live) Yl[c + (size_t)(nb + (j - 1) * A + i) * nb] = acc;
+                if (live) Yl[c + (size_t)(nb + (j - 1) * A + i) * nb] = zmul(fc, acc);
             }
         }
     }
     __syncwarp();
-    // ---- Y = R A^-1 from Q(r, s) = Z(s, r) = Y(r, nb+s) -------------------------------------------
+    // ---- Y(:, 0:nb) from the scaled Y(r, nb+s) = f_r Q(r, s) ----------------------------------------
     for (int e = lane; e < nb * nb; e += 32) {
         const int rr = e % nb, c = e / nb;
         int ax, p1, p2, axc, q1, q2;
         leaf_bpoint2(A, b, rr, ax, p1, p2);
         leaf_bpoint2(A, b, c, axc, q1, q2);
         const z rd = ax == 0 ? L.rdx : L.rdy;
-        const z f = zmul(zmk(0.0, 2.0 * g.kb), rd);
         const z wd = axc == 0 ? zscale(L.wbx, L.rdx) : zscale(L.wby, L.rdy);
-        z val = zneg(zmul(zmul(f, wd), Yl[rr + (size_t)(nb + q1) * nb]));
+        z val = zneg(zmul(wd, Yl[rr + (size_t)(nb + q1) * nb]));
         if (c == rr) {
             const double hr2 = ax == 0 ? L.hx : L.hy;
             val = zadd(val, zmul(zmk((8.0 / 3.0) / hr2, -g.kb), rd));
         }
         Yl[e] = val;
-    }
-    __syncwarp();
-    for (int e = lane; e < nb * ab; e += 32) {
-        const int rr = e % nb;
-        int ax, p1, p2;
-        leaf_bpoint2(A, b, rr, ax, p1, p2);
-        const z f = zmul(zmk(0.0, 2.0 * g.kb), ax == 0 ? L.rdx : L.rdy);
-        Yl[(size_t)nb * nb + e] = zmul(f, Yl[(size_t)nb * nb + e]);
     }
 }
 

@@ -637,6 +637,22 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
         for (GemmBatch* gb : {&t->sF12[l], &t->sF3[l], &t->sF4[l], &t->sF5[l], &t->sB1[l], &t->sB23[l], &t->sB4[l],
                               &t->sB5[l]})
             gb->fixed_order = true;
+    // split-K for the long-k, few-CTA solve GEMMs; one workspace serves them all (one stream)
+    {
+        std::vector<GemmBatch*> all{&t->sL0};
+        for (int l = 0; l < L; ++l)
+            for (GemmBatch* gb : {&t->sF12[l], &t->sF3[l], &t->sF4[l], &t->sF5[l], &t->sB1[l], &t->sB23[l],
+                                  &t->sB4[l], &t->sB5[l]})
+                all.push_back(gb);
+        long long wmax = 0;
+        for (GemmBatch* gb : all) wmax = std::max(wmax, gemm_plan_split(*gb));
+        if (wmax > 0) {
+            z* ws = nullptr;
+            if ((rc = alloc_n(t, t->solve_bufs, (size_t)wmax, &ws))) return rc;
+            for (GemmBatch* gb : all)
+                if (gb->ksplit > 1) gb->work = ws;
+        }
+    }
     t->built_rhs = nrhs;
     return RB_OK;
 }
