@@ -59,6 +59,11 @@ extern "C" {
 #define RB_FLAG_SKIP_ROOT_RTR 1   /* do not form the root's own RtR (the solve never reads it)         */
 #define RB_FLAG_VERBOSE       2   /* print the reference's progress lines to stdout                   */
 #define RB_FLAG_NO_GRAPHS     4   /* launch every kernel directly instead of replaying CUDA graphs     */
+#define RB_FLAG_MERGE_DS      8   /* interface solve as the reference writes it, inv(D) and inv(S)
+                                     (compute_RTR, robin_tree_module.f90:449-470), instead of the
+                                     default single inversion of K = nu^2 I - (zeta I - T2_ii)(zeta I -
+                                     T1_ii); the default also falls back to inv(D), inv(S) by itself
+                                     when |nu| < 0.1 max(1, |zeta|)                                    */
 
 typedef struct rb_tree rb_tree;
 

@@ -35,6 +35,7 @@ RB_POINTS_SOLUTION = 3
 RB_FLAG_SKIP_ROOT_RTR = 1
 RB_FLAG_VERBOSE = 2
 RB_FLAG_NO_GRAPHS = 4
+RB_FLAG_MERGE_DS = 8
 
 # every entry point include/robin_b200.h declares
 EXPORTS = [

@@ -108,7 +108,7 @@ PRECISIONS = {"fp64": _lib.RB_PREC_FP64, "mixed": _lib.RB_PREC_MIXED}
 class robin_tree:
     """robin_tree (robin_tree_module.f90:55-77) backed by a device-resident factorization."""
 
-    def __init__(self, device_budget: int = 0, skip_root_rtr: bool = False):
+    def __init__(self, device_budget: int = 0, skip_root_rtr: bool = False, merge_ds: bool = False):
         self.bndry_params = None
         self.nlvls = 0
         self.ell_op = None
@@ -120,6 +120,7 @@ class robin_tree:
         self._info = None
         self._budget = int(device_budget)
         self._skip_root = bool(skip_root_rtr)
+        self._merge_ds = bool(merge_ds)     # the reference's inv(D), inv(S) interface solve
 
     # -- handle ----------------------------------------------------------------------------------
     def close(self):
@@ -157,7 +158,8 @@ class robin_tree:
             g.bndry_params[2 * q + 1] = bp[i, j].imag
         g.ordering = int(opts.ordering)
         g.flags = (_lib.RB_FLAG_VERBOSE if opts.debug.txt_output else 0) | \
-                  (_lib.RB_FLAG_SKIP_ROOT_RTR if self._skip_root else 0)
+                  (_lib.RB_FLAG_SKIP_ROOT_RTR if self._skip_root else 0) | \
+                  (_lib.RB_FLAG_MERGE_DS if self._merge_ds else 0)
         g.device_budget = self._budget
         h = _lib.C.c_void_p()
         _check(lib.rb_tree_create(_lib.C.byref(g), _lib.C.byref(h)))

@@ -48,6 +48,22 @@ cudaError_t merge_form_s(ChildStore c, int nnodes, int m, int o1, z zeta, z nu, 
     return cudaGetLastError();
 }
 
+// K = nu^2 I for every node (the GEMM K -= A2 A1 then completes K = nu^2 I - A2 A1)
+__global__ void merge_form_k_kernel(int m, z nu2, z* __restrict__ dst) {
+    const int node = blockIdx.y;
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= m * m) return;
+    const int r = idx % m, q = idx / m;
+    dst[(long long)node * m * m + idx] = r == q ? nu2 : zmk(0.0, 0.0);
+}
+
+cudaError_t merge_form_k(int nnodes, int m, z nu, z* dst, cudaStream_t s) {
+    dim3 grid((m * m + 255) / 256, nnodes);
+    merge_form_k_kernel<<<grid, 256, 0, s>>>(m, zmul(nu, nu), dst);
+    note_launch();
+    return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------------------------------
 // backward sweep: children's non-interface g from the parent's g (robin_tree_module.f90:1045-1075)
 __global__ void sweep_scatter_down_kernel(int nrhs, int nbp, int nbc, int m, int o1, int o2, int n1, int n2,

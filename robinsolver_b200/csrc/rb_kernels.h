@@ -61,6 +61,8 @@ cudaError_t merge_form_d(ChildStore c, int nnodes, int m, int o2, z zeta, z* dst
 // S = zeta*I - T1_ii - nu^2 * Dinv for every parent node (child1 = 2*node).
 cudaError_t merge_form_s(ChildStore c, int nnodes, int m, int o1, z zeta, z nu, const z* dinv, z* dst,
                          cudaStream_t s);
+// K = nu^2 I for every node, into dst + node*m*m.
+cudaError_t merge_form_k(int nnodes, int m, z nu, z* dst, cudaStream_t s);
 
 // ---- sweep helpers --------------------------------------------------------------------------------------
 // children's g on their non-interface faces from the parent's g (backward sweep):

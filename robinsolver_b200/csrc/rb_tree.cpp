@@ -7,18 +7,26 @@
 // Factor (robin_tree_factor -> compute_RTR, robin_tree_module.f90:96-185, 375-650):
 //   leaves:  block-tridiagonal factor of S = A_ii - A_ib A_bb^-1 A_bi from the potential
 //            samples and Y = R A^-1 (RtR in its first nb columns), one CTA per leaf (rb_leaf.cu)
-//   level l = L-1 .. 0, all nodes of the level in one launch per stage:
-//            inv(D), D = zeta I - T2_ii;  inv(S), S = zeta I - T1_ii - nu^2 inv(D)
-//            Y2R = inv(D) T2_iN;  Y1 = inv(S) [T1_iN, -nu Y2R];  Y2 = [0, Y2R] - nu inv(D) Y1
+//   level l = L-1 .. 0, all nodes of the level in one launch per stage.  [Y1; Y2] =
+//   M^-1 blockdiag(T1_iN, T2_iN) solves the interface system M = [[A1, nu I], [nu I, A2]],
+//   A1 = zeta I - T1_ii, A2 = zeta I - T2_ii, then
 //            parent RtR = T_NN + [T1_Ni Y1; T2_Ni Y2], scattered into the parent's face order
-//   (Y1 = [C11, -C12] and Y2 = [-C21, C22] in the reference's names, :482-615.)
+//   (Y1 = [C11, -C12] and Y2 = [-C21, C22] in the reference's names, :482-615).  Two forms:
+//   K form (default): one inversion per node, K = nu^2 I - A2 A1 (for the impedance pair zeta = 0,
+//            nu = -1 this is the familiar I - T2_ii T1_ii), Y1 = inv(K) [-A2 T1_iN, nu T2_iN],
+//            Y2 = ([T1_iN, 0] - A1 Y1) / nu;
+//   D/S form (the reference's, RB_FLAG_MERGE_DS, or |nu| small against |zeta|):
+//            inv(D), D = A2;  inv(S), S = A1 - nu^2 inv(D);  Y2R = inv(D) T2_iN;
+//            Y1 = inv(S) [T1_iN, -nu Y2R];  Y2 = [0, Y2R] - nu inv(D) Y1.
 // Solve (forward_sub / backward_sub, robin_tree_module.f90:813-1146), all RHS at once:
 //   forward:  leaf h = Y(:, nb:) f;  per level (g1_i, g2_i) = M^-1 (h1_i, h2_i) and the parent's
 //             h = h_N + T_Ni g_i
 //   backward: root g = boundary data; per level children's g_N from the parent, Tg = T_iN g_N,
 //             g_i += M^-1 Tg;  leaf u = A^-1 [g; f] through the leaf's block factors.
-//   M^-1 (x1, x2): w = inv(D) x2; y1 = inv(S)(x1 - nu w); y2 = w - nu inv(D) y1 (apply_invm, :1252).
+//   M^-1 (x1, x2), K form: y1 = inv(K)(nu x2 - A2 x1), y2 = (x1 - A1 y1) / nu;  D/S form:
+//   w = inv(D) x2; y1 = inv(S)(x1 - nu w); y2 = w - nu inv(D) y1 (apply_invm, :1252).
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <cstdio>
 #include <cstring>
@@ -88,7 +96,10 @@ struct rb_tree {
     z* leaf_sinv = nullptr;
     z* leaf_Y = nullptr;
     std::vector<z*> rtr;             // per level < L
-    std::vector<z*> dinv, sinv;      // per level < L
+    std::vector<z*> dinv, sinv;      // per level < L: inv(D), inv(S); in the K form A2, A1
+    // K form of the interface solve (nu not small): one inversion per node instead of two
+    bool kform = false;
+    std::vector<z*> kinv;            // per level < L, K form only
     std::vector<int*> d_pmap1, d_pmap2;
     int* d_status = nullptr;
     // factor workspace
@@ -97,8 +108,8 @@ struct rb_tree {
     z* gj_work = nullptr;
     int* gj_ipiv = nullptr;
     // factor launch batches
-    std::vector<GJBatch> gj_d, gj_s;
-    std::vector<GemmBatch> fM1, fM2, fM3, fM4;
+    std::vector<GJBatch> gj_d, gj_s, gj_k;
+    std::vector<GemmBatch> fK, fM1, fM2, fM3, fM4;
     bool factor_ready = false;
 
     // solve storage
@@ -348,6 +359,7 @@ static int ensure_factor_storage(rb_tree* t) {
     t->rtr.assign(L, nullptr);
     t->dinv.assign(L, nullptr);
     t->sinv.assign(L, nullptr);
+    t->kinv.assign(L, nullptr);
     t->d_pmap1.assign(L, nullptr);
     t->d_pmap2.assign(L, nullptr);
     size_t ymax = 0;
@@ -357,6 +369,8 @@ static int ensure_factor_storage(rb_tree* t) {
             if ((rc = alloc_n(t, t->bufs, (size_t)p.nnodes * p.nb * p.nb, &t->rtr[l]))) return rc;
         if ((rc = alloc_n(t, t->bufs, (size_t)p.nnodes * p.m * p.m, &t->dinv[l]))) return rc;
         if ((rc = alloc_n(t, t->bufs, (size_t)p.nnodes * p.m * p.m, &t->sinv[l]))) return rc;
+        if (t->kform)
+            if ((rc = alloc_n(t, t->bufs, (size_t)p.nnodes * p.m * p.m, &t->kinv[l]))) return rc;
         if ((rc = alloc_n(t, t->bufs, p.pmap1.size(), &t->d_pmap1[l]))) return rc;
         if ((rc = alloc_n(t, t->bufs, p.pmap2.size(), &t->d_pmap2[l]))) return rc;
         RB_CK(cudaMemcpy(t->d_pmap1[l], p.pmap1.data(), p.pmap1.size() * sizeof(int), cudaMemcpyHostToDevice));
@@ -388,16 +402,23 @@ static int ensure_factor_storage(rb_tree* t) {
     };
     t->gj_d.resize(L);
     t->gj_s.resize(L);
-    t->fM1.resize(L); t->fM2.resize(L); t->fM3.resize(L); t->fM4.resize(L);
+    t->gj_k.resize(L);
+    t->fK.resize(L); t->fM1.resize(L); t->fM2.resize(L); t->fM3.resize(L); t->fM4.resize(L);
     const z one = zmk(1.0, 0.0);
+    const z mone = zmk(-1.0, 0.0);
     const z mnu = zneg(t->nu);
+    const z rnu = zrcp(t->nu), mrnu = zneg(rnu);
     for (int l = 0; l < L; ++l) {
         const PlanLevel& p = P.lv[l];
         const int m = p.m, n1 = p.n1, n2 = p.n2, o1 = p.o1, o2 = p.o2, nn = p.nnodes;
-        if ((rc = upload_gj(t, t->bufs, gj_descs(t->dinv[l], (long long)m * m, m, nn, m), m, t->gj_d[l]))) return rc;
-        if ((rc = upload_gj(t, t->bufs, gj_descs(t->sinv[l], (long long)m * m, m, nn, m), m, t->gj_s[l]))) return rc;
+        if (t->kform) {
+            if ((rc = upload_gj(t, t->bufs, gj_descs(t->kinv[l], (long long)m * m, m, nn, m), m, t->gj_k[l]))) return rc;
+        } else {
+            if ((rc = upload_gj(t, t->bufs, gj_descs(t->dinv[l], (long long)m * m, m, nn, m), m, t->gj_d[l]))) return rc;
+            if ((rc = upload_gj(t, t->bufs, gj_descs(t->sinv[l], (long long)m * m, m, nn, m), m, t->gj_s[l]))) return rc;
+        }
         const ChildStore cs = child_store(t, l);
-        std::vector<GemmDesc> m1, m2, m3, m4;
+        std::vector<GemmDesc> mk, m1, m2, m3, m4;
         for (int i = 0; i < nn; ++i) {
             const z* r1 = cs.rtr + (2LL * i) * cs.stride;
             const z* r2 = cs.rtr + (2LL * i + 1) * cs.stride;
@@ -406,6 +427,30 @@ static int ensure_factor_storage(rb_tree* t) {
             z* sv = t->sinv[l] + (long long)i * m * m;
             z* y1 = t->Y1 + (long long)i * m * (n1 + n2);
             z* y2 = t->Y2 + (long long)i * m * (n1 + n2);
+            if (t->kform) {
+                // [Y1; Y2] = M^-1 blockdiag(T1_iN, T2_iN), M = [[A1, nu I], [nu I, A2]]:
+                //   Y1 = K^-1 [-A2 T1_iN, nu T2_iN],  Y2 = ([T1_iN, 0] - A1 Y1) / nu,  K = nu^2 I - A2 A1
+                z* kv = t->kinv[l] + (long long)i * m * m;
+                const ZView t1in = band_view(r1 + o1, ld, INT_MAX, 0, o1, m);
+                const ZView t2in = band_view(r2 + o2, ld, INT_MAX, 0, o2, m);
+                {   // K = nu^2 I - A2 A1
+                    GemmDesc g = gdesc(m, m, m, zview(dv, m), zview(sv, m), zout(kv, m), mone);
+                    g.C = zview(kv, m); g.beta = one;
+                    mk.push_back(g);
+                }
+                // B1 = -A2 T1_iN, held in Y2's first n1 columns until Y2 is formed
+                m1.push_back(gdesc(m, n1, m, zview(dv, m), t1in, zout(y2, m), mone));
+                // Y1 = [K^-1 B1, nu K^-1 T2_iN]
+                m2.push_back(gdesc(m, n1, m, zview(kv, m), zview(y2, m), zout(y1, m), one));
+                m2.push_back(gdesc(m, n2, m, zview(kv, m), t2in, zout(y1 + (long long)m * n1, m), t->nu));
+                {   // Y2 = (X1 - A1 Y1) / nu, X1 = [T1_iN, 0]
+                    GemmDesc g = gdesc(m, n1, m, zview(sv, m), zview(y1, m), zout(y2, m), mrnu);
+                    g.C = t1in; g.beta = rnu;
+                    m3.push_back(g);
+                    m3.push_back(gdesc(m, n2, m, zview(sv, m), zview(y1 + (long long)m * n1, m),
+                                       zout(y2 + (long long)m * n1, m), mrnu));
+                }
+            } else {
             // Y2R = inv(D) T2_iN
             m1.push_back(gdesc(m, n2, m, zview(dv, m), band_view(r2 + o2, ld, INT_MAX, 0, o2, m),
                                zout(y2 + (long long)m * n1, m), one));
@@ -421,6 +466,7 @@ static int ensure_factor_storage(rb_tree* t) {
                 g.C = zview(y2 + (long long)m * n1, m);
                 g.beta = one;
                 m3.push_back(g);
+            }
             }
             if (!(l == 0 && t->skip_root)) {
                 z* par = t->rtr[l] + (long long)i * p.nb * p.nb;
@@ -442,6 +488,7 @@ static int ensure_factor_storage(rb_tree* t) {
                 m4.push_back(g11); m4.push_back(g12); m4.push_back(g21); m4.push_back(g22);
             }
         }
+        if ((rc = upload_gemm(t, t->bufs, mk, t->fK[l]))) return rc;
         if ((rc = upload_gemm(t, t->bufs, m1, t->fM1[l]))) return rc;
         if ((rc = upload_gemm(t, t->bufs, m2, t->fM2[l]))) return rc;
         if ((rc = upload_gemm(t, t->bufs, m3, t->fM3[l]))) return rc;
@@ -496,20 +543,41 @@ static int run_factor(rb_tree* t, const z* dk) {
         const PlanLevel& p = P.lv[l];
         const ChildStore cs = child_store(t, l);
         if ((rc = timer_begin(t, l < 17 ? lvl_names[l] : "merge_deep"))) return rc;
-        RB_TIMED("merge_form", 0.0, merge_form_d(cs, p.nnodes, p.m, p.o2, t->zeta, t->dinv[l], s));
-        RB_TIMED("gj_invert", gj_flops(p.m, p.nnodes), gj_invert_batch(t->gj_d[l].d_desc, p.nnodes, p.m, t->gj_work, t->d_status, s));
-        // Y2R = inv(D) T2_iN needs only inv(D): on the second stream it overlaps the S inversion
-        const bool fork = t->timing == 0;
-        if (fork) {
-            RB_CK(cudaEventRecord(t->ev_fork[l], s));
-            RB_CK(cudaStreamWaitEvent(t->stream2, t->ev_fork[l], 0));
-            RB_LAUNCH(launch_gemm_batch(t->fM1[l], t->stream2));
-            RB_CK(cudaEventRecord(t->ev_join[l], t->stream2));
+        if (t->kform) {
+            // A2 = zeta I - T2_ii, A1 = zeta I - T1_ii; B1 = -A2 T1_iN on the second stream beside
+            // K = nu^2 I - A2 A1 and its inversion
+            RB_TIMED("merge_form", 0.0, merge_form_d(cs, p.nnodes, p.m, p.o2, t->zeta, t->dinv[l], s));
+            RB_TIMED("merge_form", 0.0, merge_form_s(cs, p.nnodes, p.m, p.o1, t->zeta, zmk(0.0, 0.0), t->dinv[l],
+                                                     t->sinv[l], s));
+            const bool fork = t->timing == 0;
+            if (fork) {
+                RB_CK(cudaEventRecord(t->ev_fork[l], s));
+                RB_CK(cudaStreamWaitEvent(t->stream2, t->ev_fork[l], 0));
+                RB_LAUNCH(launch_gemm_batch(t->fM1[l], t->stream2));
+                RB_CK(cudaEventRecord(t->ev_join[l], t->stream2));
+            }
+            RB_TIMED("merge_form", 0.0, merge_form_k(p.nnodes, p.m, t->nu, t->kinv[l], s));
+            RB_GEMM(t->fK[l], s);
+            RB_TIMED("gj_invert", gj_flops(p.m, p.nnodes),
+                     gj_invert_batch(t->gj_k[l].d_desc, p.nnodes, p.m, t->gj_work, t->d_status, s));
+            if (fork) RB_CK(cudaStreamWaitEvent(s, t->ev_join[l], 0));
+            else RB_GEMM(t->fM1[l], s);
+        } else {
+            RB_TIMED("merge_form", 0.0, merge_form_d(cs, p.nnodes, p.m, p.o2, t->zeta, t->dinv[l], s));
+            RB_TIMED("gj_invert", gj_flops(p.m, p.nnodes), gj_invert_batch(t->gj_d[l].d_desc, p.nnodes, p.m, t->gj_work, t->d_status, s));
+            // Y2R = inv(D) T2_iN needs only inv(D): on the second stream it overlaps the S inversion
+            const bool fork = t->timing == 0;
+            if (fork) {
+                RB_CK(cudaEventRecord(t->ev_fork[l], s));
+                RB_CK(cudaStreamWaitEvent(t->stream2, t->ev_fork[l], 0));
+                RB_LAUNCH(launch_gemm_batch(t->fM1[l], t->stream2));
+                RB_CK(cudaEventRecord(t->ev_join[l], t->stream2));
+            }
+            RB_TIMED("merge_form", 0.0, merge_form_s(cs, p.nnodes, p.m, p.o1, t->zeta, t->nu, t->dinv[l], t->sinv[l], s));
+            RB_TIMED("gj_invert", gj_flops(p.m, p.nnodes), gj_invert_batch(t->gj_s[l].d_desc, p.nnodes, p.m, t->gj_work, t->d_status, s));
+            if (fork) RB_CK(cudaStreamWaitEvent(s, t->ev_join[l], 0));
+            else RB_GEMM(t->fM1[l], s);
         }
-        RB_TIMED("merge_form", 0.0, merge_form_s(cs, p.nnodes, p.m, p.o1, t->zeta, t->nu, t->dinv[l], t->sinv[l], s));
-        RB_TIMED("gj_invert", gj_flops(p.m, p.nnodes), gj_invert_batch(t->gj_s[l].d_desc, p.nnodes, p.m, t->gj_work, t->d_status, s));
-        if (fork) RB_CK(cudaStreamWaitEvent(s, t->ev_join[l], 0));
-        else RB_GEMM(t->fM1[l], s);
         RB_GEMM(t->fM2[l], s);
         RB_GEMM(t->fM3[l], s);
         RB_GEMM(t->fM4[l], s);
@@ -549,7 +617,8 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
     t->gx_solve_rhs = 0;
     // descriptor batches for this RHS count (allocated in solve_bufs too)
     const int k = nrhs;
-    const z one = zmk(1.0, 0.0), mnu = zneg(t->nu);
+    const z one = zmk(1.0, 0.0), mone = zmk(-1.0, 0.0), mnu = zneg(t->nu);
+    const z rnu = zrcp(t->nu), mrnu = zneg(rnu);
     std::vector<GemmDesc> v;
     for (int i = 0; i < nl; ++i)
         v.push_back(gdesc(nb, k, ab, zview(t->leaf_Y + (long long)i * nb * n + (long long)nb * nb, nb),
@@ -574,18 +643,31 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
             z* h2 = t->hbuf[l + 1] + (2LL * i + 1) * nbc * k;
             z* g1 = t->gbuf[l + 1] + (2LL * i) * nbc * k;
             z* g2 = t->gbuf[l + 1] + (2LL * i + 1) * nbc * k;
-            // forward: g2_i = inv(D) h2_i ; g1_i = inv(S) h1_i
-            f12.push_back(gdesc(m, k, m, zview(dv, m), zview(h2 + o2, nbc), zout(g2 + o2, nbc), one));
-            f12.push_back(gdesc(m, k, m, zview(sv, m), zview(h1 + o1, nbc), zout(g1 + o1, nbc), one));
-            {   // g1_i -= nu inv(S) g2_i
-                GemmDesc g = gdesc(m, k, m, zview(sv, m), zview(g2 + o2, nbc), zout(g1 + o1, nbc), mnu);
-                g.C = zview(g1 + o1, nbc); g.beta = one;
-                f3.push_back(g);
-            }
-            {   // g2_i -= nu inv(D) g1_i
-                GemmDesc g = gdesc(m, k, m, zview(dv, m), zview(g1 + o1, nbc), zout(g2 + o2, nbc), mnu);
-                g.C = zview(g2 + o2, nbc); g.beta = one;
-                f4.push_back(g);
+            if (t->kform) {
+                // forward (g1, g2) = M^-1 (h1, h2): t = nu h2 - A2 h1 (in g2), g1 = K^-1 t,
+                // g2 = (h1 - A1 g1) / nu
+                z* kv = t->kinv[l] + (long long)i * m * m;
+                GemmDesc gt = gdesc(m, k, m, zview(dv, m), zview(h1 + o1, nbc), zout(g2 + o2, nbc), mone);
+                gt.C = zview(h2 + o2, nbc); gt.beta = t->nu;
+                f12.push_back(gt);
+                f3.push_back(gdesc(m, k, m, zview(kv, m), zview(g2 + o2, nbc), zout(g1 + o1, nbc), one));
+                GemmDesc g2d = gdesc(m, k, m, zview(sv, m), zview(g1 + o1, nbc), zout(g2 + o2, nbc), mrnu);
+                g2d.C = zview(h1 + o1, nbc); g2d.beta = rnu;
+                f4.push_back(g2d);
+            } else {
+                // forward: g2_i = inv(D) h2_i ; g1_i = inv(S) h1_i
+                f12.push_back(gdesc(m, k, m, zview(dv, m), zview(h2 + o2, nbc), zout(g2 + o2, nbc), one));
+                f12.push_back(gdesc(m, k, m, zview(sv, m), zview(h1 + o1, nbc), zout(g1 + o1, nbc), one));
+                {   // g1_i -= nu inv(S) g2_i
+                    GemmDesc g = gdesc(m, k, m, zview(sv, m), zview(g2 + o2, nbc), zout(g1 + o1, nbc), mnu);
+                    g.C = zview(g1 + o1, nbc); g.beta = one;
+                    f3.push_back(g);
+                }
+                {   // g2_i -= nu inv(D) g1_i
+                    GemmDesc g = gdesc(m, k, m, zview(dv, m), zview(g1 + o1, nbc), zout(g2 + o2, nbc), mnu);
+                    g.C = zview(g2 + o2, nbc); g.beta = one;
+                    f4.push_back(g);
+                }
             }
             if (l > 0) {   // parent h = h_N + T_Ni g_i
                 z* hp = t->hbuf[l] + (long long)i * nbp * k;
@@ -610,17 +692,30 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
                                band_view(g1, nbc, o1, m, INT_MAX, 0), zout(tg1, m), one));
             b1.push_back(gdesc(m, k, n2, band_view(r2 + o2, ld, INT_MAX, 0, o2, m),
                                band_view(g2, nbc, o2, m, INT_MAX, 0), zout(tg2, m), one));
-            b23.push_back(gdesc(m, k, m, zview(dv, m), zview(tg2, m), zout(w, m), one));
-            b23.push_back(gdesc(m, k, m, zview(sv, m), zview(tg1, m), zout(y1, m), one));
-            {
-                GemmDesc g = gdesc(m, k, m, zview(sv, m), zview(w, m), zout(y1, m), mnu);
-                g.C = zview(y1, m); g.beta = one;
-                b4.push_back(g);
-            }
-            {
-                GemmDesc g = gdesc(m, k, m, zview(dv, m), zview(y1, m), zout(w, m), mnu);
-                g.C = zview(w, m); g.beta = one;
-                b5.push_back(g);
+            if (t->kform) {
+                // backward (y1, w) = M^-1 (tg1, tg2): t = nu tg2 - A2 tg1 (in w), y1 = K^-1 t,
+                // w = (tg1 - A1 y1) / nu
+                z* kv = t->kinv[l] + (long long)i * m * m;
+                GemmDesc gt = gdesc(m, k, m, zview(dv, m), zview(tg1, m), zout(w, m), mone);
+                gt.C = zview(tg2, m); gt.beta = t->nu;
+                b23.push_back(gt);
+                b4.push_back(gdesc(m, k, m, zview(kv, m), zview(w, m), zout(y1, m), one));
+                GemmDesc gw = gdesc(m, k, m, zview(sv, m), zview(y1, m), zout(w, m), mrnu);
+                gw.C = zview(tg1, m); gw.beta = rnu;
+                b5.push_back(gw);
+            } else {
+                b23.push_back(gdesc(m, k, m, zview(dv, m), zview(tg2, m), zout(w, m), one));
+                b23.push_back(gdesc(m, k, m, zview(sv, m), zview(tg1, m), zout(y1, m), one));
+                {
+                    GemmDesc g = gdesc(m, k, m, zview(sv, m), zview(w, m), zout(y1, m), mnu);
+                    g.C = zview(y1, m); g.beta = one;
+                    b4.push_back(g);
+                }
+                {
+                    GemmDesc g = gdesc(m, k, m, zview(dv, m), zview(y1, m), zout(w, m), mnu);
+                    g.C = zview(w, m); g.beta = one;
+                    b5.push_back(g);
+                }
             }
         }
         if ((rc = upload_gemm(t, t->solve_bufs, f12, t->sF12[l]))) return rc;
@@ -728,6 +823,13 @@ int rb_tree_create(const rb_geom* geom, rb_tree** out) {
     const z rden = zrcp(den);
     t->nu = zmul(zadd(zneg(zmul(b11, b22)), zmul(b12, b21)), rden);
     t->zeta = zmul(zadd(zmul(b11, b22), zmul(b12, b21)), rden);
+    // one inversion per merge (K = nu^2 I - A2 A1) unless nu is small against zeta, where the
+    // division by nu in Y2 = (X1 - A1 Y1) / nu would lose digits; then inv(D) and inv(S)
+    {
+        const double an = std::sqrt(t->nu.x * t->nu.x + t->nu.y * t->nu.y);
+        const double az = std::sqrt(t->zeta.x * t->zeta.x + t->zeta.y * t->zeta.y);
+        t->kform = !(geom->flags & RB_FLAG_MERGE_DS) && an >= 0.1 * std::max(1.0, az);
+    }
     t->budget = geom->device_budget;
     t->verbose = (geom->flags & RB_FLAG_VERBOSE) != 0;
     t->skip_root = (geom->flags & RB_FLAG_SKIP_ROOT_RTR) != 0;
@@ -738,7 +840,8 @@ int rb_tree_create(const rb_geom* geom, rb_tree** out) {
         const double ab = (double)Q.leaf_a() * Q.leaf_b();
         double need = (double)Q.nleaves() * (ab * Q.leaf_a() + (double)Q.leaf_nb() * Q.leaf_n() + ab) * 16.0;
         for (int l = 0; l < Q.L; ++l)
-            need += (double)Q.lv[l].nnodes * ((double)Q.lv[l].nb * Q.lv[l].nb + 2.0 * Q.lv[l].m * Q.lv[l].m) * 16.0;
+            need += (double)Q.lv[l].nnodes *
+                    ((double)Q.lv[l].nb * Q.lv[l].nb + (t->kform ? 3.0 : 2.0) * Q.lv[l].m * Q.lv[l].m) * 16.0;
         if (need > (double)t->budget) {
             g_create_error = "device budget exceeded: the factorization needs at least " +
                              std::to_string((long long)need) + " bytes, budget " + std::to_string(t->budget);

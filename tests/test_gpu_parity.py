@@ -30,10 +30,13 @@ def _solve(T, rhs):
     return np.stack([T.solution_array(r) for r in range(len(rhs))])
 
 
-def test_config1_rtr_every_level_matches_oracle():
+@pytest.mark.parametrize("merge_ds", [False, True])
+def test_config1_rtr_every_level_matches_oracle(merge_ds):
+    """Every node's RtR at every level, with the default single-inversion interface solve and
+    with the reference's inv(D)/inv(S) form."""
     wl = W.make_workload(1)
     O, _ = oracle_run(wl)
-    T = _factored(wl)
+    T = _factored(wl, merge_ds=merge_ds)
     for l in range(wl.L + 1):
         for i in range(len(O.levels[l])):
             assert rel_err(T.get_rtr(l, i), O.levels[l][i].rtr) < 1e-11, (l, i)
@@ -124,10 +127,11 @@ def test_resident_gauss_jordan_equals_blocked_bitwise(cfg, monkeypatch):
 
 
 @pytest.mark.slow
-def test_config2_matches_oracle():
+@pytest.mark.parametrize("merge_ds", [False, True])
+def test_config2_matches_oracle(merge_ds):
     wl = W.make_workload(2)
     O, U = oracle_run(wl)
-    T = _factored(wl)
+    T = _factored(wl, merge_ds=merge_ds)
     Ug = _solve(T, wl.rhs)
     errs = [rel_err(Ug[r], U[r]) for r in range(len(wl.rhs))]
     assert max(errs) < 3e-11, errs
