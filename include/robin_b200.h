@@ -59,6 +59,12 @@ extern "C" {
 #define RB_FLAG_SKIP_ROOT_RTR 1   /* do not form the root's own RtR (the solve never reads it)         */
 #define RB_FLAG_VERBOSE       2   /* print the reference's progress lines to stdout                   */
 #define RB_FLAG_NO_GRAPHS     4   /* launch every kernel directly instead of replaying CUDA graphs     */
+#define RB_FLAG_ASYNC_FACTOR 16   /* rb_tree_factor returns once the potential is copied and the
+                                     factor is enqueued; the next call that needs the factor
+                                     (rb_tree_solve, rb_get_solution, rb_tree_get_rtr,
+                                     rb_tree_times, another factor) waits for it and reports its
+                                     errors (RB_ERR_NUMERIC).  Host right-hand sides of
+                                     rb_tree_solve are then copied while the factor runs.        */
 #define RB_FLAG_MERGE_DS      8   /* interface solve as the reference writes it, inv(D) and inv(S)
                                      (compute_RTR, robin_tree_module.f90:449-470), instead of the
                                      default single inversion of K = nu^2 I - (zeta I - T2_ii)(zeta I -

@@ -36,6 +36,7 @@ RB_FLAG_SKIP_ROOT_RTR = 1
 RB_FLAG_VERBOSE = 2
 RB_FLAG_NO_GRAPHS = 4
 RB_FLAG_MERGE_DS = 8
+RB_FLAG_ASYNC_FACTOR = 16
 
 # every entry point include/robin_b200.h declares
 EXPORTS = [

@@ -108,7 +108,8 @@ PRECISIONS = {"fp64": _lib.RB_PREC_FP64, "mixed": _lib.RB_PREC_MIXED}
 class robin_tree:
     """robin_tree (robin_tree_module.f90:55-77) backed by a device-resident factorization."""
 
-    def __init__(self, device_budget: int = 0, skip_root_rtr: bool = False, merge_ds: bool = False):
+    def __init__(self, device_budget: int = 0, skip_root_rtr: bool = False, merge_ds: bool = False,
+                 async_factor: bool = False):
         self.bndry_params = None
         self.nlvls = 0
         self.ell_op = None
@@ -121,6 +122,7 @@ class robin_tree:
         self._budget = int(device_budget)
         self._skip_root = bool(skip_root_rtr)
         self._merge_ds = bool(merge_ds)     # the reference's inv(D), inv(S) interface solve
+        self._async = bool(async_factor)    # factor returns when enqueued (RB_FLAG_ASYNC_FACTOR)
 
     # -- handle ----------------------------------------------------------------------------------
     def close(self):
@@ -159,7 +161,8 @@ class robin_tree:
         g.ordering = int(opts.ordering)
         g.flags = (_lib.RB_FLAG_VERBOSE if opts.debug.txt_output else 0) | \
                   (_lib.RB_FLAG_SKIP_ROOT_RTR if self._skip_root else 0) | \
-                  (_lib.RB_FLAG_MERGE_DS if self._merge_ds else 0)
+                  (_lib.RB_FLAG_MERGE_DS if self._merge_ds else 0) | \
+                  (_lib.RB_FLAG_ASYNC_FACTOR if self._async else 0)
         g.device_budget = self._budget
         h = _lib.C.c_void_p()
         _check(lib.rb_tree_create(_lib.C.byref(g), _lib.C.byref(h)))
@@ -212,7 +215,8 @@ class robin_tree:
         self._info = self.info()
         if self.opts is not None:
             self.opts.h = np.array(self._info.h_last[:], dtype=np.float64)
-        self._update_times()
+        if not self._async:          # an asynchronous factor's time is taken by the solve
+            self._update_times()
 
     def _update_times(self):
         f = _lib.C.c_double()

@@ -78,7 +78,14 @@ struct rb_tree {
     Plan P;
     std::string err;
     cudaStream_t stream = nullptr;
-    cudaStream_t stream2 = nullptr;      // runs Y2R = inv(D) T2_iN beside the inversion of S
+    cudaStream_t stream2 = nullptr;      // runs one merge GEMM per level beside the level's inversion
+    cudaStream_t stream3 = nullptr;      // host -> device copies of the inputs, beside running work
+    cudaEvent_t ev_copy = nullptr;
+    // RB_FLAG_ASYNC_FACTOR: rb_tree_factor returns once the factor is enqueued; its completion,
+    // time and status are taken by the next call that needs them (settle_factor)
+    bool async_factor = false;
+    bool factor_pending = false;
+    int* h_status = nullptr;             // pinned copy of the factor's status word
     std::vector<cudaEvent_t> ev_fork, ev_join;
     int device = 0;
     bool factored = false;
@@ -344,6 +351,12 @@ static int ensure_factor_storage(rb_tree* t) {
     RB_CK(cudaGetDevice(&t->device));
     if (!t->stream) RB_CK(cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking));
     if (!t->stream2) RB_CK(cudaStreamCreateWithFlags(&t->stream2, cudaStreamNonBlocking));
+    if (!t->stream3) RB_CK(cudaStreamCreateWithFlags(&t->stream3, cudaStreamNonBlocking));
+    if (!t->ev_copy) RB_CK(cudaEventCreateWithFlags(&t->ev_copy, cudaEventDisableTiming));
+    if (!t->h_status) {
+        RB_CK(cudaMallocHost(&t->h_status, sizeof(int)));
+        *t->h_status = 0;
+    }
     t->ev_fork.assign(L, nullptr);
     t->ev_join.assign(L, nullptr);
     for (int l = 0; l < L; ++l) {
@@ -834,6 +847,7 @@ int rb_tree_create(const rb_geom* geom, rb_tree** out) {
     t->verbose = (geom->flags & RB_FLAG_VERBOSE) != 0;
     t->skip_root = (geom->flags & RB_FLAG_SKIP_ROOT_RTR) != 0;
     t->graphs = (geom->flags & RB_FLAG_NO_GRAPHS) == 0;
+    t->async_factor = (geom->flags & RB_FLAG_ASYNC_FACTOR) != 0;
     // refuse up front a problem the budget cannot hold (persistent factor storage only)
     if (t->budget > 0) {
         const Plan& Q = t->P;
@@ -867,6 +881,10 @@ int rb_tree_destroy(rb_tree* t) {
     for (auto& e : t->ev_pool) cudaEventDestroy(e);
     for (auto& e : t->ev_fork) if (e) cudaEventDestroy(e);
     for (auto& e : t->ev_join) if (e) cudaEventDestroy(e);
+    if (t->stream3) cudaStreamSynchronize(t->stream3);
+    if (t->ev_copy) cudaEventDestroy(t->ev_copy);
+    if (t->h_status) cudaFreeHost(t->h_status);
+    if (t->stream3) cudaStreamDestroy(t->stream3);
     if (t->stream2) cudaStreamDestroy(t->stream2);
     if (t->stream) cudaStreamDestroy(t->stream);
     delete t;
@@ -952,6 +970,24 @@ int rb_tree_sample_points(const rb_tree* t, int which, double* xyz) {
     return RB_ERR_INVALID;
 }
 
+// Waits for the last factor, takes its time and its status (zero pivots) and reports them.
+static int settle_factor(rb_tree* t) {
+    if (!t->factor_pending) return RB_OK;
+    t->factor_pending = false;
+    RB_CK(cudaEventSynchronize(t->ev[1]));
+    float ms = 0.f;
+    RB_CK(cudaEventElapsedTime(&ms, t->ev[0], t->ev[1]));
+    t->f_time = ms * 1e-3;
+    timers_collect(t);
+    if (*t->h_status) {
+        t->factored = false;
+        t->nrhs = 0;
+        return fail(t, RB_ERR_NUMERIC, "zero pivot met while inverting a leaf or interface matrix");
+    }
+    if (t->verbose) std::printf("RTR computation completed.\nFactorization completed.\n");
+    return RB_OK;
+}
+
 static int factor_common(rb_tree* t, const double* k, int precision, bool host, int sync) {
     if (!t) return RB_ERR_INVALID;
     if (!k) return fail(t, RB_ERR_INVALID, "rb_tree_factor: null potential samples");
@@ -959,6 +995,9 @@ static int factor_common(rb_tree* t, const double* k, int precision, bool host, 
         return fail(t, RB_ERR_UNSUPPORTED, "precision mode " + std::to_string(precision) + " is not implemented");
     int rc = ensure_factor_storage(t);
     if (rc) return rc;
+    // a previous factor nobody waited for: report it, unless this call asks not to wait at all
+    if (!host && !sync) t->factor_pending = false;
+    else if ((rc = settle_factor(t))) return rc;
     const Plan& P = t->P;
     const size_t nint = (size_t)P.nleaves() * P.leaf_a() * P.leaf_b();
     t->factored = false;
@@ -967,30 +1006,31 @@ static int factor_common(rb_tree* t, const double* k, int precision, bool host, 
         timers_collect(t);
         t->stage_ms.clear();
     }
-    // the factor always reads the handle's own copy, so one captured graph serves every call
-    RB_CK(cudaMemcpyAsync(t->d_k, k, nint * sizeof(z), host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice,
-                          t->stream));
     for (auto& e : t->ev)
         if (!e) RB_CK(cudaEventCreate(&e));
+    // the factor always reads the handle's own copy, so one captured graph serves every call.  A
+    // host array is copied on the copy stream and waited for here, so that the caller may reuse
+    // it as soon as this returns, even when the factor itself is still running.
+    if (host) {
+        RB_CK(cudaStreamWaitEvent(t->stream3, t->ev[1], 0));      // the last factor read d_k
+        RB_CK(cudaMemcpyAsync(t->d_k, k, nint * sizeof(z), cudaMemcpyHostToDevice, t->stream3));
+        RB_CK(cudaEventRecord(t->ev_copy, t->stream3));
+        RB_CK(cudaStreamSynchronize(t->stream3));
+        RB_CK(cudaStreamWaitEvent(t->stream, t->ev_copy, 0));
+    } else {
+        RB_CK(cudaMemcpyAsync(t->d_k, k, nint * sizeof(z), cudaMemcpyDeviceToDevice, t->stream));
+    }
     const long long l0 = launch_count();
     RB_CK(cudaEventRecord(t->ev[0], t->stream));
     if ((rc = run_graphed(t, t->gx_factor, t->gx_factor_launches, t->factor_runs,
                           [&] { return run_factor(t, t->d_k); })))
         return rc;
+    RB_CK(cudaMemcpyAsync(t->h_status, t->d_status, sizeof(int), cudaMemcpyDeviceToHost, t->stream));
     RB_CK(cudaEventRecord(t->ev[1], t->stream));
     t->factor_launches = launch_count() - l0;
-    if (host || sync) {
-        RB_CK(cudaStreamSynchronize(t->stream));
-        int st = 0;
-        RB_CK(cudaMemcpy(&st, t->d_status, sizeof(int), cudaMemcpyDeviceToHost));
-        if (st) return fail(t, RB_ERR_NUMERIC, "zero pivot met while inverting a leaf or interface matrix");
-        float ms = 0.f;
-        RB_CK(cudaEventElapsedTime(&ms, t->ev[0], t->ev[1]));
-        t->f_time = ms * 1e-3;
-        timers_collect(t);
-        if (t->verbose) std::printf("RTR computation completed.\nFactorization completed.\n");
-    }
     t->factored = true;
+    t->factor_pending = true;
+    if ((host && !t->async_factor) || (!host && sync)) return settle_factor(t);
     return RB_OK;
 }
 
@@ -1011,9 +1051,19 @@ static int solve_common(rb_tree* t, int nrhs, const double* f, const double* g, 
     const size_t nroot = (size_t)P.lv[0].nb;
     const cudaMemcpyKind kind = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
     t->nrhs = 0;
+    if (host) {
+        // host right-hand sides go up on the copy stream, beside a factor that may still run on
+        // the main stream; the copy waits until the last solve has read its buffers
+        RB_CK(cudaStreamWaitEvent(t->stream3, t->ev[3], 0));
+        RB_CK(cudaMemcpyAsync(t->d_f, f, nrhs * nint * sizeof(z), kind, t->stream3));
+        RB_CK(cudaMemcpyAsync(t->gbuf[0], g, nrhs * nroot * sizeof(z), kind, t->stream3));
+        RB_CK(cudaEventRecord(t->ev_copy, t->stream3));
+        RB_CK(cudaStreamWaitEvent(t->stream, t->ev_copy, 0));
+    } else {
+        RB_CK(cudaMemcpyAsync(t->d_f, f, nrhs * nint * sizeof(z), kind, t->stream));
+        RB_CK(cudaMemcpyAsync(t->gbuf[0], g, nrhs * nroot * sizeof(z), kind, t->stream));
+    }
     RB_CK(cudaEventRecord(t->ev[2], t->stream));
-    RB_CK(cudaMemcpyAsync(t->d_f, f, nrhs * nint * sizeof(z), kind, t->stream));
-    RB_CK(cudaMemcpyAsync(t->gbuf[0], g, nrhs * nroot * sizeof(z), kind, t->stream));
     const long long l0 = launch_count();
     if (t->gx_solve_rhs != nrhs) {     // the solve sequence depends on the RHS count
         drop_graph(t->gx_solve);
@@ -1026,6 +1076,7 @@ static int solve_common(rb_tree* t, int nrhs, const double* f, const double* g, 
     RB_CK(cudaEventRecord(t->ev[3], t->stream));
     if (host || sync) {
         RB_CK(cudaStreamSynchronize(t->stream));
+        if ((rc = settle_factor(t))) return rc;
         float ms = 0.f;
         RB_CK(cudaEventElapsedTime(&ms, t->ev[2], t->ev[3]));
         t->s_time = ms * 1e-3;
@@ -1046,6 +1097,7 @@ int rb_tree_solve_device(rb_tree* t, int nrhs, const double* f, const double* g,
 int rb_get_solution(const rb_tree* tc, int irhs, double* u, double* boxes) {
     rb_tree* t = const_cast<rb_tree*>(tc);
     if (!t || !u) return RB_ERR_INVALID;
+    if (int rc = settle_factor(t)) return rc;
     if (!t->factored) return fail(t, RB_ERR_NOT_FACTORED, "Error in GET_SOLUTION: Robin Tree not factored.");
     if (irhs < 0 || irhs >= t->nrhs) return fail(t, RB_ERR_NO_SOLUTION, "get_solution: no solution for this right-hand side");
     const Plan& P = t->P;
@@ -1075,8 +1127,10 @@ int rb_get_solution_device(const rb_tree* tc, double* du, int sync) {
     return RB_OK;
 }
 
-int rb_tree_times(const rb_tree* t, double* f_time, double* s_time) {
+int rb_tree_times(const rb_tree* tc, double* f_time, double* s_time) {
+    rb_tree* t = const_cast<rb_tree*>(tc);
     if (!t) return RB_ERR_INVALID;
+    if (int rc = settle_factor(t)) return rc;
     if (f_time) *f_time = t->f_time;
     if (s_time) *s_time = t->s_time;
     return RB_OK;
@@ -1125,6 +1179,7 @@ int rb_tree_level_shape(const rb_tree* t, int level, int32_t* shape) {
 int rb_tree_get_rtr(const rb_tree* tc, int level, int node, double* out) {
     rb_tree* t = const_cast<rb_tree*>(tc);
     if (!t || !out) return RB_ERR_INVALID;
+    if (int rc = settle_factor(t)) return rc;
     if (!t->factored) return fail(t, RB_ERR_NOT_FACTORED, "Error: Robin Tree must be factored first.");
     const Plan& P = t->P;
     if (level < 0 || level > P.L || node < 0 || node >= P.lv[level].nnodes)

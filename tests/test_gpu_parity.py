@@ -89,6 +89,22 @@ def test_batched_rhs_equal_individual_solves(nrhs, check):
     T.close()
 
 
+def test_async_factor_gives_the_same_solution():
+    """With RB_FLAG_ASYNC_FACTOR the factor call returns before the factor has run and the solve's
+    right-hand sides are copied beside it; the solve waits for the factor, and the solutions are
+    bit-identical to the blocking call sequence."""
+    wl = W.make_workload(2, N=128, L=6, nrhs=3)
+    T = _factored(wl)
+    Ta = _factored(wl, async_factor=True)
+    for _ in range(2):                       # the second round replays the captured graphs
+        Ua = _solve(Ta, wl.rhs)
+        assert np.array_equal(_solve(T, wl.rhs), Ua)
+        assert Ta.f_time > 0.0
+        Ta.factor(wl.L, *gpu_tree(wl)[1:])
+    T.close()
+    Ta.close()
+
+
 def test_resolve_and_refactor_have_no_stale_state():
     wl = W.make_workload(1)
     T = _factored(wl)
