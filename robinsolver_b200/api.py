@@ -109,7 +109,7 @@ class robin_tree:
     """robin_tree (robin_tree_module.f90:55-77) backed by a device-resident factorization."""
 
     def __init__(self, device_budget: int = 0, skip_root_rtr: bool = False, merge_ds: bool = False,
-                 async_factor: bool = False):
+                 async_factor: bool = False, graphs: bool = True):
         self.bndry_params = None
         self.nlvls = 0
         self.ell_op = None
@@ -123,6 +123,7 @@ class robin_tree:
         self._skip_root = bool(skip_root_rtr)
         self._merge_ds = bool(merge_ds)     # the reference's inv(D), inv(S) interface solve
         self._async = bool(async_factor)    # factor returns when enqueued (RB_FLAG_ASYNC_FACTOR)
+        self._graphs = bool(graphs)         # replay factor/solve as CUDA graphs (else RB_FLAG_NO_GRAPHS)
 
     # -- handle ----------------------------------------------------------------------------------
     def close(self):
@@ -162,7 +163,8 @@ class robin_tree:
         g.flags = (_lib.RB_FLAG_VERBOSE if opts.debug.txt_output else 0) | \
                   (_lib.RB_FLAG_SKIP_ROOT_RTR if self._skip_root else 0) | \
                   (_lib.RB_FLAG_MERGE_DS if self._merge_ds else 0) | \
-                  (_lib.RB_FLAG_ASYNC_FACTOR if self._async else 0)
+                  (_lib.RB_FLAG_ASYNC_FACTOR if self._async else 0) | \
+                  (0 if self._graphs else _lib.RB_FLAG_NO_GRAPHS)
         g.device_budget = self._budget
         h = _lib.C.c_void_p()
         _check(lib.rb_tree_create(_lib.C.byref(g), _lib.C.byref(h)))

@@ -161,10 +161,14 @@ static cudaError_t launch_split(const GemmBatch& b, cudaStream_t s) {
 }
 
 // the kernel shape a batch runs on
-enum class GemmShape { Dfma16, Dfma32, Dmma64, Dfma128x64, Dfma64 };
+enum class GemmShape { Dfma16, Dfma32, Dmma32, Dmma64, Dfma128x64, Dfma64 };
 static GemmShape gemm_shape(const GemmBatch& b) {
     const int mm = b.max_m, nn = b.max_n;
     if (mm <= 16 && nn <= 16) return GemmShape::Dfma16;
+    // FP64 tensor cores, small problems (both sides <= 192: the merges below 128x256 boxes):
+    // 32x32 tiles of 4 warps, up to six CTAs per SM; measured 1.0-1.6x the 64x64 tile and
+    // 1.3-1.4x the DFMA tiles on the merge shapes 16x48x16 .. 192x192x64
+    if (use_dmma() && !b.fixed_order && mm <= 192 && nn <= 192) return GemmShape::Dmma32;
     // every DFMA shape sums an element's products in the same order, so the shape can follow the
     // available parallelism: small-n batches (the solve) that would leave SMs idle with 32x32
     // tiles take 16x16 tiles
@@ -205,7 +209,8 @@ long long gemm_plan_split(GemmBatch& b) {
 }
 
 const char* gemm_stage_name(const GemmBatch& b) {
-    return gemm_shape(b) == GemmShape::Dmma64 ? "zgemm_tc" : "zgemm_dfma";
+    const GemmShape sh = gemm_shape(b);
+    return (sh == GemmShape::Dmma64 || sh == GemmShape::Dmma32) ? "zgemm_tc" : "zgemm_dfma";
 }
 
 cudaError_t launch_gemm_batch(const GemmBatch& b, cudaStream_t s) {
@@ -221,6 +226,7 @@ cudaError_t launch_gemm_batch(const GemmBatch& b, cudaStream_t s) {
     switch (shape) {
         case GemmShape::Dfma16: return launch_cfg<16, 16, 2, 2, 8, 6, 8>(b, s);
         case GemmShape::Dfma32: return launch_cfg<32, 32, 4, 2, 8, 4, 4>(b, s);
+        case GemmShape::Dmma32: return launch_dmma<32, 32, 2, 2, 6>(b, s);
         case GemmShape::Dmma64: return launch_dmma<64, 64, 2, 4, 2>(b, s);
         case GemmShape::Dfma128x64: return launch_cfg<128, 64, 8, 4, 4, 4, 1>(b, s);
         case GemmShape::Dfma64: break;

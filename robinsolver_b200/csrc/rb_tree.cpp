@@ -87,6 +87,9 @@ struct rb_tree {
     bool factor_pending = false;
     int* h_status = nullptr;             // pinned copy of the factor's status word
     std::vector<cudaEvent_t> ev_fork, ev_join;
+    // factor progress for a solve that overlaps it: [l] after level l's inversion, [L] after the leaves
+    std::vector<cudaEvent_t> ev_lvl;
+    bool factor_deferred = false;        // RB_FLAG_ASYNC_FACTOR: potential copied, factor not launched
     int device = 0;
     bool factored = false;
     double f_time = 0.0, s_time = 0.0;
@@ -359,6 +362,8 @@ static int ensure_factor_storage(rb_tree* t) {
     }
     t->ev_fork.assign(L, nullptr);
     t->ev_join.assign(L, nullptr);
+    t->ev_lvl.assign(L + 1, nullptr);
+    for (int l = 0; l <= L; ++l) RB_CK(cudaEventCreateWithFlags(&t->ev_lvl[l], cudaEventDisableTiming));
     for (int l = 0; l < L; ++l) {
         RB_CK(cudaEventCreateWithFlags(&t->ev_fork[l], cudaEventDisableTiming));
         RB_CK(cudaEventCreateWithFlags(&t->ev_join[l], cudaEventDisableTiming));
@@ -538,7 +543,8 @@ static double leaf_flops(const LeafGeom& g) {
     return 8.0 * g.a * g.a * g.a * g.b + 16.0 * g.a * g.a * (double)g.nb * g.b;
 }
 
-static int run_factor(rb_tree* t, const z* dk) {
+// rec (optional): events recorded as the factor progresses, for a solve on another stream
+static int run_factor(rb_tree* t, const z* dk, const std::vector<cudaEvent_t>* rec = nullptr) {
     const Plan& P = t->P;
     const int L = P.L, nl = P.nleaves();
     LeafGeom lg{P.leaf_a(), P.leaf_b(), P.leaf_nb(), P.leaf_n(), P.kb};
@@ -549,6 +555,7 @@ static int run_factor(rb_tree* t, const z* dk) {
     RB_TIMED("leaf_factor", leaf_flops(lg) * nl, leaf_block_factor(lg, nl, t->d_h, dk, t->leaf_sinv, t->leaf_Y,
                                                                     t->d_status, s));
     if ((rc = timer_end(t))) return rc;
+    if (rec) RB_CK(cudaEventRecord((*rec)[L], s));
     static const char* lvl_names[] = {"merge_l0", "merge_l1", "merge_l2", "merge_l3", "merge_l4", "merge_l5",
                                       "merge_l6", "merge_l7", "merge_l8", "merge_l9", "merge_l10", "merge_l11",
                                       "merge_l12", "merge_l13", "merge_l14", "merge_l15", "merge_l16"};
@@ -573,6 +580,7 @@ static int run_factor(rb_tree* t, const z* dk) {
             RB_GEMM(t->fK[l], s);
             RB_TIMED("gj_invert", gj_flops(p.m, p.nnodes),
                      gj_invert_batch(t->gj_k[l].d_desc, p.nnodes, p.m, t->gj_work, t->d_status, s));
+            if (rec) RB_CK(cudaEventRecord((*rec)[l], s));      // inv(K), A1, A2 of level l are ready
             if (fork) RB_CK(cudaStreamWaitEvent(s, t->ev_join[l], 0));
             else RB_GEMM(t->fM1[l], s);
         } else {
@@ -588,6 +596,7 @@ static int run_factor(rb_tree* t, const z* dk) {
             }
             RB_TIMED("merge_form", 0.0, merge_form_s(cs, p.nnodes, p.m, p.o1, t->zeta, t->nu, t->dinv[l], t->sinv[l], s));
             RB_TIMED("gj_invert", gj_flops(p.m, p.nnodes), gj_invert_batch(t->gj_s[l].d_desc, p.nnodes, p.m, t->gj_work, t->d_status, s));
+            if (rec) RB_CK(cudaEventRecord((*rec)[l], s));      // inv(D), inv(S) of level l are ready
             if (fork) RB_CK(cudaStreamWaitEvent(s, t->ev_join[l], 0));
             else RB_GEMM(t->fM1[l], s);
         }
@@ -765,15 +774,19 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
     return RB_OK;
 }
 
-static int run_solve(rb_tree* t, int k) {
+// The solve on stream s.  wait (optional): the factor's progress events (run_factor's rec); the
+// leaf forward GEMM waits for the leaves and forward level l for level l of a factor that runs
+// on another stream; the backward sweep reads only levels the forward sweep waited for.
+static int run_solve(rb_tree* t, int k, cudaStream_t s, const std::vector<cudaEvent_t>* wait = nullptr) {
     const Plan& P = t->P;
     const int L = P.L, nl = P.nleaves();
     LeafGeom lg{P.leaf_a(), P.leaf_b(), P.leaf_nb(), P.leaf_n(), P.kb};
-    cudaStream_t s = t->stream;
     int rc;
     if ((rc = timer_begin(t, "forward"))) return rc;
+    if (wait) RB_CK(cudaStreamWaitEvent(s, (*wait)[L], 0));
     RB_GEMM(t->sL0, s);
     for (int l = L - 1; l >= 0; --l) {
+        if (wait) RB_CK(cudaStreamWaitEvent(s, (*wait)[l], 0));
         RB_GEMM(t->sF12[l], s);
         RB_GEMM(t->sF3[l], s);
         RB_GEMM(t->sF4[l], s);
@@ -881,6 +894,7 @@ int rb_tree_destroy(rb_tree* t) {
     for (auto& e : t->ev_pool) cudaEventDestroy(e);
     for (auto& e : t->ev_fork) if (e) cudaEventDestroy(e);
     for (auto& e : t->ev_join) if (e) cudaEventDestroy(e);
+    for (auto& e : t->ev_lvl) if (e) cudaEventDestroy(e);
     if (t->stream3) cudaStreamSynchronize(t->stream3);
     if (t->ev_copy) cudaEventDestroy(t->ev_copy);
     if (t->h_status) cudaFreeHost(t->h_status);
@@ -970,8 +984,32 @@ int rb_tree_sample_points(const rb_tree* t, int which, double* xyz) {
     return RB_ERR_INVALID;
 }
 
-// Waits for the last factor, takes its time and its status (zero pivots) and reports them.
+// Enqueues the factor of t->d_k on the main stream: replayed as a graph, or launched directly
+// with progress events (rec) for a solve that overlaps it.
+static int launch_factor(rb_tree* t, const std::vector<cudaEvent_t>* rec) {
+    int rc;
+    const long long l0 = launch_count();
+    t->factor_deferred = false;
+    RB_CK(cudaEventRecord(t->ev[0], t->stream));
+    if (rec) {
+        if ((rc = run_factor(t, t->d_k, rec))) return rc;
+    } else if ((rc = run_graphed(t, t->gx_factor, t->gx_factor_launches, t->factor_runs,
+                                 [&] { return run_factor(t, t->d_k); }))) {
+        return rc;
+    }
+    RB_CK(cudaMemcpyAsync(t->h_status, t->d_status, sizeof(int), cudaMemcpyDeviceToHost, t->stream));
+    RB_CK(cudaEventRecord(t->ev[1], t->stream));
+    t->factor_launches = launch_count() - l0;
+    t->factor_pending = true;
+    return RB_OK;
+}
+
+// Waits for the last factor (launching it first if it was deferred), takes its time and its
+// status (zero pivots) and reports them.
 static int settle_factor(rb_tree* t) {
+    if (t->factor_deferred) {
+        if (int rc = launch_factor(t, nullptr)) return rc;
+    }
     if (!t->factor_pending) return RB_OK;
     t->factor_pending = false;
     RB_CK(cudaEventSynchronize(t->ev[1]));
@@ -995,7 +1033,9 @@ static int factor_common(rb_tree* t, const double* k, int precision, bool host, 
         return fail(t, RB_ERR_UNSUPPORTED, "precision mode " + std::to_string(precision) + " is not implemented");
     int rc = ensure_factor_storage(t);
     if (rc) return rc;
-    // a previous factor nobody waited for: report it, unless this call asks not to wait at all
+    // a previous factor nobody waited for: report it, unless this call asks not to wait at all;
+    // one that was deferred and never needed is dropped
+    t->factor_deferred = false;
     if (!host && !sync) t->factor_pending = false;
     else if ((rc = settle_factor(t))) return rc;
     const Plan& P = t->P;
@@ -1020,16 +1060,13 @@ static int factor_common(rb_tree* t, const double* k, int precision, bool host, 
     } else {
         RB_CK(cudaMemcpyAsync(t->d_k, k, nint * sizeof(z), cudaMemcpyDeviceToDevice, t->stream));
     }
-    const long long l0 = launch_count();
-    RB_CK(cudaEventRecord(t->ev[0], t->stream));
-    if ((rc = run_graphed(t, t->gx_factor, t->gx_factor_launches, t->factor_runs,
-                          [&] { return run_factor(t, t->d_k); })))
-        return rc;
-    RB_CK(cudaMemcpyAsync(t->h_status, t->d_status, sizeof(int), cudaMemcpyDeviceToHost, t->stream));
-    RB_CK(cudaEventRecord(t->ev[1], t->stream));
-    t->factor_launches = launch_count() - l0;
     t->factored = true;
-    t->factor_pending = true;
+    // RB_FLAG_ASYNC_FACTOR: nothing is launched yet; a solve that follows runs beside the factor
+    if (t->async_factor && t->timing == 0 && (host || !sync)) {
+        t->factor_deferred = true;
+        return RB_OK;
+    }
+    if ((rc = launch_factor(t, nullptr))) return rc;
     if ((host && !t->async_factor) || (!host && sync)) return settle_factor(t);
     return RB_OK;
 }
@@ -1051,33 +1088,52 @@ static int solve_common(rb_tree* t, int nrhs, const double* f, const double* g, 
     const size_t nroot = (size_t)P.lv[0].nb;
     const cudaMemcpyKind kind = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
     t->nrhs = 0;
-    if (host) {
-        // host right-hand sides go up on the copy stream, beside a factor that may still run on
-        // the main stream; the copy waits until the last solve has read its buffers
-        RB_CK(cudaStreamWaitEvent(t->stream3, t->ev[3], 0));
+    if (t->factor_deferred && t->timing == 0) {
+        // factor and solve together: the factor on the main stream, the solve on the copy stream
+        // right after its inputs, each solve level waiting for that level of the factor; the main
+        // stream then waits for the solve, so later calls see both finished
+        RB_CK(cudaEventRecord(t->ev_copy, t->stream));       // device inputs are ordered there
+        RB_CK(cudaStreamWaitEvent(t->stream3, t->ev_copy, 0));
         RB_CK(cudaMemcpyAsync(t->d_f, f, nrhs * nint * sizeof(z), kind, t->stream3));
         RB_CK(cudaMemcpyAsync(t->gbuf[0], g, nrhs * nroot * sizeof(z), kind, t->stream3));
-        RB_CK(cudaEventRecord(t->ev_copy, t->stream3));
-        RB_CK(cudaStreamWaitEvent(t->stream, t->ev_copy, 0));
+        if ((rc = launch_factor(t, &t->ev_lvl))) return rc;
+        const long long l0 = launch_count();
+        RB_CK(cudaEventRecord(t->ev[2], t->stream3));
+        if ((rc = run_solve(t, nrhs, t->stream3, &t->ev_lvl))) return rc;
+        RB_CK(cudaEventRecord(t->ev[3], t->stream3));
+        RB_CK(cudaStreamWaitEvent(t->stream, t->ev[3], 0));
+        t->solve_launches = launch_count() - l0;
     } else {
-        RB_CK(cudaMemcpyAsync(t->d_f, f, nrhs * nint * sizeof(z), kind, t->stream));
-        RB_CK(cudaMemcpyAsync(t->gbuf[0], g, nrhs * nroot * sizeof(z), kind, t->stream));
+        if (t->factor_deferred && (rc = launch_factor(t, nullptr))) return rc;
+        if (host) {
+            // host right-hand sides go up on the copy stream, beside a factor that may still run on
+            // the main stream; the copy waits until the last solve has read its buffers
+            RB_CK(cudaStreamWaitEvent(t->stream3, t->ev[3], 0));
+            RB_CK(cudaMemcpyAsync(t->d_f, f, nrhs * nint * sizeof(z), kind, t->stream3));
+            RB_CK(cudaMemcpyAsync(t->gbuf[0], g, nrhs * nroot * sizeof(z), kind, t->stream3));
+            RB_CK(cudaEventRecord(t->ev_copy, t->stream3));
+            RB_CK(cudaStreamWaitEvent(t->stream, t->ev_copy, 0));
+        } else {
+            RB_CK(cudaMemcpyAsync(t->d_f, f, nrhs * nint * sizeof(z), kind, t->stream));
+            RB_CK(cudaMemcpyAsync(t->gbuf[0], g, nrhs * nroot * sizeof(z), kind, t->stream));
+        }
+        RB_CK(cudaEventRecord(t->ev[2], t->stream));
+        const long long l0 = launch_count();
+        if (t->gx_solve_rhs != nrhs) {     // the solve sequence depends on the RHS count
+            drop_graph(t->gx_solve);
+            t->gx_solve_rhs = nrhs;
+            t->solve_runs = 0;
+        }
+        if ((rc = run_graphed(t, t->gx_solve, t->gx_solve_launches, t->solve_runs,
+                              [&] { return run_solve(t, nrhs, t->stream); })))
+            return rc;
+        t->solve_launches = launch_count() - l0;
+        RB_CK(cudaEventRecord(t->ev[3], t->stream));
     }
-    RB_CK(cudaEventRecord(t->ev[2], t->stream));
-    const long long l0 = launch_count();
-    if (t->gx_solve_rhs != nrhs) {     // the solve sequence depends on the RHS count
-        drop_graph(t->gx_solve);
-        t->gx_solve_rhs = nrhs;
-        t->solve_runs = 0;
-    }
-    if ((rc = run_graphed(t, t->gx_solve, t->gx_solve_launches, t->solve_runs, [&] { return run_solve(t, nrhs); })))
-        return rc;
-    t->solve_launches = launch_count() - l0;
-    RB_CK(cudaEventRecord(t->ev[3], t->stream));
     if (host || sync) {
         RB_CK(cudaStreamSynchronize(t->stream));
         if ((rc = settle_factor(t))) return rc;
-        float ms = 0.f;
+        float ms = 0.f;       // beside an overlapped factor this spans the wait for its levels too
         RB_CK(cudaEventElapsedTime(&ms, t->ev[2], t->ev[3]));
         t->s_time = ms * 1e-3;
         timers_collect(t);

@@ -90,9 +90,9 @@ def test_batched_rhs_equal_individual_solves(nrhs, check):
 
 
 def test_async_factor_gives_the_same_solution():
-    """With RB_FLAG_ASYNC_FACTOR the factor call returns before the factor has run and the solve's
-    right-hand sides are copied beside it; the solve waits for the factor, and the solutions are
-    bit-identical to the blocking call sequence."""
+    """With RB_FLAG_ASYNC_FACTOR the factor call only copies the potential; the solve that follows
+    launches factor and solve together, each solve level waiting for its factor level, and the
+    solutions are bit-identical to the blocking call sequence."""
     wl = W.make_workload(2, N=128, L=6, nrhs=3)
     T = _factored(wl)
     Ta = _factored(wl, async_factor=True)
@@ -101,8 +101,13 @@ def test_async_factor_gives_the_same_solution():
         assert np.array_equal(_solve(T, wl.rhs), Ua)
         assert Ta.f_time > 0.0
         Ta.factor(wl.L, *gpu_tree(wl)[1:])
+    # a deferred factor that no solve picks up is launched by the call that needs it
+    Tr = _factored(wl, async_factor=True)
+    for lvl in (wl.L, 1, 0):
+        assert np.array_equal(Tr.get_rtr(lvl, 0), T.get_rtr(lvl, 0))
     T.close()
     Ta.close()
+    Tr.close()
 
 
 def test_resolve_and_refactor_have_no_stale_state():
