@@ -55,6 +55,11 @@ extern "C" {
 #define RB_POINTS_BOUNDARY  2     /* face-local coordinates where bndry_rhs%g_face is sampled         */
 #define RB_POINTS_SOLUTION  3     /* every point of every leaf's u vector (check_solution's points)   */
 
+/* ---- field kinds for rb_tree_sample_device -------------------------------------------------- */
+#define RB_FIELD_BUMP_POTENTIAL 0 /* k = kb (1 + 0.3 sum_j a_j exp(-|x-c_j|^2/(2 w^2))) + i delta kb     */
+#define RB_FIELD_POINT_SOURCE   1 /* f = exp(-|x-x0|^2/(2 w^2)), g = 0                                 */
+#define RB_FIELD_PLANE_WAVE     2 /* f = 0, g = i kb (d.n - 1) exp(i kb d.x) (impedance data of the wave) */
+
 /* ---- flags in rb_geom.flags ----------------------------------------------------------------- */
 #define RB_FLAG_SKIP_ROOT_RTR 1   /* do not form the root's own RtR (the solve never reads it)         */
 #define RB_FLAG_VERBOSE       2   /* print the reference's progress lines to stdout                   */
@@ -198,6 +203,40 @@ int rb_tree_level_shape(const rb_tree* tree, int level, int32_t* shape);
  * (robin_tree_module.f90:782-793 for leaves, :538-615 for merges) assembled into one matrix.
  * RB_ERR_INVALID for the root when RB_FLAG_SKIP_ROOT_RTR is set. */
 int rb_tree_get_rtr(const rb_tree* tree, int level, int node, double* out);
+
+/* ---- beyond the reference's factor/solve: device-side inputs, error reports, persistence ---- */
+
+/* Samples a standard potential or right-hand-side family on the device, at exactly the points
+ * rb_tree_sample_points lists, so that the inputs of rb_tree_factor_device / rb_tree_solve_device
+ * never cross PCIe (the reference evaluates its callbacks point by point on the host,
+ * fd_module.f90:136-145, 427-431, 636-651).  Formulas and the rounding of their exponents
+ * follow the synthetic problems' host definitions; exp, sin and cos are CUDA's.
+ *  RB_FIELD_BUMP_POTENTIAL: params = kb, delta, w, then (cx, cy, a) for each of `count` bumps;
+ *                           writes n_interior values to d_f (d_g unused).
+ *  RB_FIELD_POINT_SOURCE:   params = (x0, y0, w) per right-hand side, `count` of them; writes
+ *                           count * n_interior f values to d_f and zeros to d_g (either may be NULL).
+ *  RB_FIELD_PLANE_WAVE:     params = (kb, dx, dy) per right-hand side (unit direction d); writes
+ *                           count * root_nb g values to d_g and zeros to d_f (either may be NULL).
+ * Runs on the handle's stream; asynchronous when `sync` is 0.  Needs only rb_tree_create. */
+int rb_tree_sample_device(rb_tree* tree, int kind, int count, const double* params, double* d_f,
+                          double* d_g, int sync);
+
+/* check_solution (robin_output_module.f90:84-134) on the device: per leaf, the norm of
+ * u - u_exact (rel = 0) or of (u - u_exact) / u_exact (rel = 1) for right-hand side `irhs` of
+ * the last solve, norm 1 (sum), 2 (Euclidean) or anything else (maximum) of the moduli.
+ * u_exact: nleaves * leaf_n complex at RB_POINTS_SOLUTION (host memory; _device: device memory).
+ * err: nleaves doubles (host).  The solution itself stays on the device. */
+int rb_check_solution(const rb_tree* tree, int irhs, const double* u_exact, int norm, int rel, double* err);
+int rb_check_solution_device(const rb_tree* tree, int irhs, const double* d_u_exact, int norm, int rel,
+                             double* err);
+
+/* Writes the factorized tree (its rb_geom and every array the solve reads: leaf factors, level
+ * RtR maps and interface inverses) to `path`, and rebuilds a handle from such a file, ready to
+ * solve, without factoring again.  No counterpart in the reference (its write_variable is a
+ * stub, robin_output_module.f90:157-221).  The file holds raw complex128 arrays of this
+ * library's layout; rb_tree_load refuses files of another version, tree or interface form. */
+int rb_tree_save(const rb_tree* tree, const char* path);
+int rb_tree_load(const char* path, rb_tree** out);
 
 /* Number of this library's kernels launched by the last factor and the last solve. */
 int rb_tree_launch_counts(const rb_tree* tree, int64_t* factor_launches, int64_t* solve_launches);

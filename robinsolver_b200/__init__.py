@@ -6,7 +6,7 @@ host-side mirror of the reference's Fortran interface plus the seeded benchmark 
 The API names load the shared library on first use (``robinsolver_b200.build`` and
 ``robinsolver_b200.workloads`` do not need it).
 """
-_API = ("RobinSolverError", "bndry_rhs", "debug_opts", "elliptic_operator", "elliptic_rhs",
+_API = ("RobinSolverError", "bndry_rhs", "check_solution", "debug_opts", "elliptic_operator", "elliptic_rhs",
         "get_solution", "leaf_solution", "robin_tree", "scalar_callback", "solve_opts")
 
 __all__ = list(_API)

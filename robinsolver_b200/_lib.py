@@ -37,6 +37,9 @@ RB_FLAG_VERBOSE = 2
 RB_FLAG_NO_GRAPHS = 4
 RB_FLAG_MERGE_DS = 8
 RB_FLAG_ASYNC_FACTOR = 16
+RB_FIELD_BUMP_POTENTIAL = 0
+RB_FIELD_POINT_SOURCE = 1
+RB_FIELD_PLANE_WAVE = 2
 
 # every entry point include/robin_b200.h declares
 EXPORTS = [
@@ -45,6 +48,7 @@ EXPORTS = [
     "rb_get_solution", "rb_get_solution_device", "rb_tree_times", "rb_tree_stream",
     "rb_tree_set_timing", "rb_tree_stage_times", "rb_tree_clear_stage_times", "rb_tree_level_shape", "rb_tree_get_rtr", "rb_tree_launch_counts",
     "rb_leaf_rtr_noalloc",
+    "rb_tree_sample_device", "rb_check_solution", "rb_check_solution_device", "rb_tree_save", "rb_tree_load",
 ]
 
 
@@ -107,6 +111,11 @@ def _load():
         "rb_tree_get_rtr": (C.c_int, [P, C.c_int, C.c_int, D]),
         "rb_tree_launch_counts": (C.c_int, [P, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]),
         "rb_leaf_rtr_noalloc": (C.c_int, [C.c_int, C.c_int, C.c_double, P, P, C.c_int, P, P]),
+        "rb_tree_sample_device": (C.c_int, [P, C.c_int, C.c_int, D, P, P, C.c_int]),
+        "rb_check_solution": (C.c_int, [P, C.c_int, D, C.c_int, C.c_int, D]),
+        "rb_check_solution_device": (C.c_int, [P, C.c_int, P, C.c_int, C.c_int, D]),
+        "rb_tree_save": (C.c_int, [P, C.c_char_p]),
+        "rb_tree_load": (C.c_int, [C.c_char_p, C.POINTER(P)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -309,6 +309,31 @@ class robin_tree:
         _check(lib.rb_tree_launch_counts(self._h, _lib.C.byref(f), _lib.C.byref(s)), self._h)
         return f.value, s.value
 
+    # -- beyond the reference: device-side inputs and persistence ------------------------------------
+    def sample_device(self, kind: int, count: int, params, d_f: int = 0, d_g: int = 0, sync: bool = True):
+        """rb_tree_sample_device: a standard potential / right-hand-side family evaluated on the
+        device into the device arrays at addresses d_f, d_g (0 for none)."""
+        par = np.ascontiguousarray(np.asarray(params, dtype=np.float64).ravel())
+        _check(lib.rb_tree_sample_device(self._h, int(kind), int(count), _lib.dptr(par),
+                                         _lib.C.c_void_p(int(d_f) or None), _lib.C.c_void_p(int(d_g) or None),
+                                         1 if sync else 0), self._h)
+
+    def save(self, path: str):
+        """Writes the factorized tree to `path` (rb_tree_save)."""
+        _check(lib.rb_tree_save(self._h, str(path).encode()), self._h)
+
+    @classmethod
+    def load(cls, path: str) -> "robin_tree":
+        """A factorized tree from a file written by save (rb_tree_load), ready to solve."""
+        h = _lib.C.c_void_p()
+        _check(lib.rb_tree_load(str(path).encode(), _lib.C.byref(h)))
+        T = cls()
+        T._h = h
+        T._info = T.info()
+        T.factored = True
+        T.nlvls = 0
+        return T
+
 
 def get_solution(T: robin_tree, irhs: int = 0):
     """get_solution(T, u) (robin_output_module.f90:48-75): leaf_solution per leaf, DFS order."""
@@ -323,3 +348,19 @@ def get_solution(T: robin_tree, irhs: int = 0):
         box = np.array([[boxes[i, 0], boxes[i, 2], boxes[i, 4]], [boxes[i, 1], boxes[i, 3], boxes[i, 5]]])
         out.append(leaf_solution(box=box, u=u[i].copy()))
     return out
+
+
+def check_solution(T: robin_tree, true_sol, irhs: int = 0, norm: str = "M", rel: bool = False) -> np.ndarray:
+    """check_solution(d, leaf_sol, true_sol, opts, error_vec, norm, rel)
+    (robin_output_module.f90:84-134) for right-hand side `irhs` of the last solve: per leaf, the
+    1-, 2- or max-norm ('1', '2', anything else) of u - u_exact, or of (u - u_exact)/u_exact when
+    `rel`.  `true_sol` is vectorised over an (npts, 3) array of points; the solution stays on the
+    device."""
+    if not T.factored:
+        raise RobinSolverError(_lib.RB_ERR_NOT_FACTORED, "Error in GET_SOLUTION: Robin Tree not factored.")
+    X = T.sample_points(_lib.RB_POINTS_SOLUTION)
+    ue = np.ascontiguousarray(np.asarray(true_sol(X), dtype=np.complex128))
+    err = np.zeros(T._info.nleaves, dtype=np.float64)
+    code = {"1": 1, "2": 2}.get(str(norm), 0)
+    _check(lib.rb_check_solution(T.handle, int(irhs), _lib.dptr(ue), code, 1 if rel else 0, _lib.dptr(err)), T.handle)
+    return err

@@ -64,6 +64,16 @@ cudaError_t merge_form_s(ChildStore c, int nnodes, int m, int o1, z zeta, z nu, 
 // K = nu^2 I for every node, into dst + node*m*m.
 cudaError_t merge_form_k(int nnodes, int m, z nu, z* dst, cudaStream_t s);
 
+// ---- device-side sampling and check_solution (rb_sample.cu) -------------------------------------------
+// pts: n points (x, y, z) as rb_tree_sample_points lists them; outputs complex128
+cudaError_t sample_bump(const double* pts, long long n, double kb, double delta, double w, int nbumps,
+                        const double* d_bumps, z* out, cudaStream_t s);
+cudaError_t sample_point_sources(const double* pts, long long n, int nrhs, const double* d_par, z* f, cudaStream_t s);
+cudaError_t sample_plane_waves(const double* pts, int nb, int ra, int rb, const double* dom4, int nrhs,
+                               const double* d_par, z* g, cudaStream_t s);
+cudaError_t check_solution(const z* u, const z* ue, int nleaves, int n, int norm, int rel, double* err,
+                           cudaStream_t s);
+
 // ---- sweep helpers --------------------------------------------------------------------------------------
 // children's g on their non-interface faces from the parent's g (backward sweep):
 // g_child[phys(t)] = g_parent[pmap[t]] for both children, every node and RHS.

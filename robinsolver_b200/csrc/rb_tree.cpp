@@ -90,6 +90,12 @@ struct rb_tree {
     // factor progress for a solve that overlaps it: [l] after level l's inversion, [L] after the leaves
     std::vector<cudaEvent_t> ev_lvl;
     bool factor_deferred = false;        // RB_FLAG_ASYNC_FACTOR: potential copied, factor not launched
+    // device-side sampling and check_solution: rb_tree_sample_points' points, cached on first use
+    double* d_pts[3] = {nullptr, nullptr, nullptr};     // potential, source, boundary
+    double* d_par = nullptr;
+    size_t par_cap = 0;
+    double* d_err = nullptr;
+    z* d_uex = nullptr;
     int device = 0;
     bool factored = false;
     double f_time = 0.0, s_time = 0.0;
@@ -356,6 +362,8 @@ static int ensure_factor_storage(rb_tree* t) {
     if (!t->stream2) RB_CK(cudaStreamCreateWithFlags(&t->stream2, cudaStreamNonBlocking));
     if (!t->stream3) RB_CK(cudaStreamCreateWithFlags(&t->stream3, cudaStreamNonBlocking));
     if (!t->ev_copy) RB_CK(cudaEventCreateWithFlags(&t->ev_copy, cudaEventDisableTiming));
+    for (auto& e : t->ev)
+        if (!e) RB_CK(cudaEventCreate(&e));
     if (!t->h_status) {
         RB_CK(cudaMallocHost(&t->h_status, sizeof(int)));
         *t->h_status = 0;
@@ -1258,3 +1266,212 @@ int rb_tree_launch_counts(const rb_tree* t, int64_t* fl, int64_t* sl) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------------
+// Device-side sampling, check_solution, save / load.
+
+static int ensure_points(rb_tree* t, int which, double** out) {
+    const int idx = which == RB_POINTS_POTENTIAL ? 0 : which == RB_POINTS_SOURCE ? 1 : 2;
+    if (!t->d_pts[idx]) {
+        const Plan& P = t->P;
+        const size_t n = which == RB_POINTS_BOUNDARY ? (size_t)P.lv[0].nb
+                                                     : (size_t)P.nleaves() * P.leaf_a() * P.leaf_b();
+        std::vector<double> h(3 * n);
+        int rc = rb_tree_sample_points(t, which, h.data());
+        if (rc) return rc;
+        if ((rc = alloc_n(t, t->bufs, 3 * n, &t->d_pts[idx]))) return rc;
+        RB_CK(cudaMemcpy(t->d_pts[idx], h.data(), 3 * n * sizeof(double), cudaMemcpyHostToDevice));
+    }
+    *out = t->d_pts[idx];
+    return RB_OK;
+}
+
+static int upload_params(rb_tree* t, const double* par, size_t n) {
+    if (n > t->par_cap) {
+        int rc = alloc_n(t, t->bufs, n, &t->d_par);
+        if (rc) return rc;
+        t->par_cap = n;
+    }
+    if (n) RB_CK(cudaMemcpyAsync(t->d_par, par, n * sizeof(double), cudaMemcpyHostToDevice, t->stream));
+    return RB_OK;
+}
+
+int rb_tree_sample_device(rb_tree* t, int kind, int count, const double* params, double* d_f, double* d_g,
+                          int sync) {
+    if (!t || !params || count < 0) return RB_ERR_INVALID;
+    if (t->P.d != 2) return fail(t, RB_ERR_UNSUPPORTED, "device sampling is 2D only");
+    int rc;
+    if (!t->stream) RB_CK(cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking));
+    const Plan& P = t->P;
+    const long long nint = (long long)P.nleaves() * P.leaf_a() * P.leaf_b();
+    const int nb = P.lv[0].nb;
+    cudaStream_t s = t->stream;
+    double* pts = nullptr;
+    if (kind == RB_FIELD_BUMP_POTENTIAL) {
+        if (!d_f) return fail(t, RB_ERR_INVALID, "rb_tree_sample_device: the potential needs d_f");
+        if ((rc = ensure_points(t, RB_POINTS_POTENTIAL, &pts))) return rc;
+        if ((rc = upload_params(t, params + 3, 3 * (size_t)count))) return rc;
+        RB_LAUNCH(sample_bump(pts, nint, params[0], params[1], params[2], count, t->d_par, (z*)d_f, s));
+    } else if (kind == RB_FIELD_POINT_SOURCE) {
+        if ((rc = ensure_points(t, RB_POINTS_SOURCE, &pts))) return rc;
+        if ((rc = upload_params(t, params, 3 * (size_t)count))) return rc;
+        if (d_f) RB_LAUNCH(sample_point_sources(pts, nint, count, t->d_par, (z*)d_f, s));
+        if (d_g) RB_CK(cudaMemsetAsync(d_g, 0, (size_t)count * nb * sizeof(z), s));
+    } else if (kind == RB_FIELD_PLANE_WAVE) {
+        if ((rc = ensure_points(t, RB_POINTS_BOUNDARY, &pts))) return rc;
+        if ((rc = upload_params(t, params, 3 * (size_t)count))) return rc;
+        const double dom4[4] = {t->geom.domain[0], t->geom.domain[1], t->geom.domain[2], t->geom.domain[3]};
+        if (d_g) RB_LAUNCH(sample_plane_waves(pts, nb, P.lv[0].a, P.lv[0].b, dom4, count, t->d_par, (z*)d_g, s));
+        if (d_f) RB_CK(cudaMemsetAsync(d_f, 0, (size_t)count * nint * sizeof(z), s));
+    } else {
+        return fail(t, RB_ERR_INVALID, "rb_tree_sample_device: unknown kind " + std::to_string(kind));
+    }
+    if (sync) RB_CK(cudaStreamSynchronize(s));
+    return RB_OK;
+}
+
+static int check_common(rb_tree* t, int irhs, const double* uex, bool host, int norm, int rel, double* err) {
+    if (!t || !uex || !err) return RB_ERR_INVALID;
+    int rc;
+    if ((rc = settle_factor(t))) return rc;
+    if (!t->factored) return fail(t, RB_ERR_NOT_FACTORED, "Error in GET_SOLUTION: Robin Tree not factored.");
+    if (irhs < 0 || irhs >= t->nrhs)
+        return fail(t, RB_ERR_NO_SOLUTION, "check_solution: no solution for this right-hand side");
+    const Plan& P = t->P;
+    const int nl = P.nleaves(), n = P.leaf_n();
+    const size_t per = (size_t)nl * n;
+    if (!t->d_err && (rc = alloc_n(t, t->bufs, (size_t)nl, &t->d_err))) return rc;
+    const z* ue = reinterpret_cast<const z*>(uex);
+    if (host) {
+        if (!t->d_uex && (rc = alloc_n(t, t->bufs, per, &t->d_uex))) return rc;
+        RB_CK(cudaMemcpyAsync(t->d_uex, uex, per * sizeof(z), cudaMemcpyHostToDevice, t->stream));
+        ue = t->d_uex;
+    }
+    RB_LAUNCH(check_solution(t->sol + (size_t)irhs * per, ue, nl, n, norm, rel, t->d_err, t->stream));
+    RB_CK(cudaMemcpyAsync(err, t->d_err, nl * sizeof(double), cudaMemcpyDeviceToHost, t->stream));
+    RB_CK(cudaStreamSynchronize(t->stream));
+    return RB_OK;
+}
+
+int rb_check_solution(const rb_tree* t, int irhs, const double* u_exact, int norm, int rel, double* err) {
+    return check_common(const_cast<rb_tree*>(t), irhs, u_exact, true, norm, rel, err);
+}
+int rb_check_solution_device(const rb_tree* t, int irhs, const double* d_u_exact, int norm, int rel, double* err) {
+    return check_common(const_cast<rb_tree*>(t), irhs, d_u_exact, false, norm, rel, err);
+}
+
+// Every buffer the solve reads after a factorization, in file order.
+static std::vector<std::pair<z*, size_t>> factor_sections(rb_tree* t) {
+    const Plan& P = t->P;
+    const size_t nl = P.nleaves(), a = P.leaf_a(), b = P.leaf_b(), nb = P.leaf_nb(), n = P.leaf_n();
+    std::vector<std::pair<z*, size_t>> v;
+    v.push_back({t->leaf_sinv, nl * b * a * a});
+    v.push_back({t->leaf_Y, nl * nb * n});
+    for (int l = 0; l < P.L; ++l) {
+        const PlanLevel& p = P.lv[l];
+        const size_t mm = (size_t)p.nnodes * p.m * p.m;
+        if (t->rtr[l]) v.push_back({t->rtr[l], (size_t)p.nnodes * p.nb * p.nb});
+        v.push_back({t->dinv[l], mm});
+        v.push_back({t->sinv[l], mm});
+        if (t->kform) v.push_back({t->kinv[l], mm});
+    }
+    return v;
+}
+
+struct SaveHeader {
+    char magic[8];
+    uint32_t version;
+    uint32_t geom_bytes;
+    rb_geom geom;
+    int32_t kform;
+    int32_t nsections;
+};
+static const char kMagic[8] = {'R', 'B', 'T', 'R', 'E', 'E', 'F', '1'};
+
+int rb_tree_save(const rb_tree* tc, const char* path) {
+    rb_tree* t = const_cast<rb_tree*>(tc);
+    if (!t || !path) return RB_ERR_INVALID;
+    int rc;
+    if ((rc = settle_factor(t))) return rc;
+    if (!t->factored) return fail(t, RB_ERR_NOT_FACTORED, "Error: Robin Tree must be factored first.");
+    RB_CK(cudaStreamSynchronize(t->stream));
+    const auto secs = factor_sections(t);
+    SaveHeader h{};
+    std::memcpy(h.magic, kMagic, 8);
+    h.version = 1;
+    h.geom_bytes = sizeof(rb_geom);
+    h.geom = t->geom;
+    h.kform = t->kform ? 1 : 0;
+    h.nsections = (int32_t)secs.size();
+    FILE* fp = std::fopen(path, "wb");
+    if (!fp) return fail(t, RB_ERR_INVALID, std::string("rb_tree_save: cannot open ") + path);
+    bool ok = std::fwrite(&h, sizeof(h), 1, fp) == 1;
+    std::vector<z> stage(std::min<size_t>(1 << 22, std::max<size_t>(1, secs.empty() ? 1 : secs[0].second)));
+    for (const auto& sec : secs) {
+        const uint64_t cnt = sec.second;
+        ok = ok && std::fwrite(&cnt, sizeof(cnt), 1, fp) == 1;
+        for (size_t off = 0; ok && off < sec.second; off += stage.size()) {
+            const size_t c = std::min(stage.size(), sec.second - off);
+            if (cudaMemcpy(stage.data(), sec.first + off, c * sizeof(z), cudaMemcpyDeviceToHost) != cudaSuccess) {
+                std::fclose(fp);
+                return fail(t, RB_ERR_CUDA, "rb_tree_save: device read failed");
+            }
+            ok = std::fwrite(stage.data(), sizeof(z), c, fp) == c;
+        }
+    }
+    ok = (std::fclose(fp) == 0) && ok;
+    if (!ok) return fail(t, RB_ERR_INVALID, std::string("rb_tree_save: write to ") + path + " failed");
+    return RB_OK;
+}
+
+int rb_tree_load(const char* path, rb_tree** out) {
+    if (!path || !out) return RB_ERR_INVALID;
+    *out = nullptr;
+    FILE* fp = std::fopen(path, "rb");
+    if (!fp) {
+        g_create_error = std::string("rb_tree_load: cannot open ") + path;
+        return RB_ERR_INVALID;
+    }
+    SaveHeader h{};
+    if (std::fread(&h, sizeof(h), 1, fp) != 1 || std::memcmp(h.magic, kMagic, 8) != 0 || h.version != 1 ||
+        h.geom_bytes != sizeof(rb_geom)) {
+        std::fclose(fp);
+        g_create_error = std::string("rb_tree_load: ") + path + " is not a factorized tree of this library";
+        return RB_ERR_INVALID;
+    }
+    rb_tree* t = nullptr;
+    int rc = rb_tree_create(&h.geom, &t);
+    if (rc) {
+        std::fclose(fp);
+        return rc;
+    }
+    auto bail = [&](int code, const std::string& msg) {
+        std::fclose(fp);
+        g_create_error = msg;
+        rb_tree_destroy(t);
+        return code;
+    };
+    if ((int)t->kform != h.kform) return bail(RB_ERR_INVALID, "rb_tree_load: interface form differs from the file's");
+    if ((rc = ensure_factor_storage(t))) return bail(rc, t->err);
+    const auto secs = factor_sections(t);
+    if ((int)secs.size() != h.nsections) return bail(RB_ERR_INVALID, "rb_tree_load: section count mismatch");
+    std::vector<z> stage(std::min<size_t>(1 << 22, std::max<size_t>(1, secs.empty() ? 1 : secs[0].second)));
+    for (const auto& sec : secs) {
+        uint64_t cnt = 0;
+        if (std::fread(&cnt, sizeof(cnt), 1, fp) != 1 || cnt != sec.second)
+            return bail(RB_ERR_INVALID, "rb_tree_load: section size mismatch (file truncated or of another tree)");
+        for (size_t off = 0; off < sec.second; off += stage.size()) {
+            const size_t c = std::min(stage.size(), sec.second - off);
+            if (std::fread(stage.data(), sizeof(z), c, fp) != c)
+                return bail(RB_ERR_INVALID, "rb_tree_load: file truncated");
+            if (cudaMemcpy(sec.first + off, stage.data(), c * sizeof(z), cudaMemcpyHostToDevice) != cudaSuccess)
+                return bail(RB_ERR_CUDA, "rb_tree_load: device write failed");
+        }
+    }
+    std::fclose(fp);
+    t->factored = true;
+    t->factor_pending = false;
+    t->factor_deferred = false;
+    *out = t;
+    return RB_OK;
+}

@@ -137,3 +137,27 @@ def test_non_dyadic_domain_plans_like_the_oracle(h_tgt, uniform):
     pot = np.concatenate([H.interior_points(g[0], g[1], h, lf.box) for (h, g), lf in zip(grids, leaves)])
     assert np.array_equal(T.sample_points(_lib.RB_POINTS_POTENTIAL), pot)
     T.close()
+
+
+def test_load_refuses_missing_and_foreign_files(tmp_path):
+    import ctypes
+    from robinsolver_b200 import _lib
+    h = ctypes.c_void_p()
+    assert _lib.lib.rb_tree_load(str(tmp_path / "none.rbt").encode(), ctypes.byref(h)) == _lib.RB_ERR_INVALID
+    assert "cannot open" in _lib.last_error(None)
+    bad = tmp_path / "bad.rbt"
+    bad.write_bytes(b"not a tree" * 20)
+    assert _lib.lib.rb_tree_load(str(bad).encode(), ctypes.byref(h)) == _lib.RB_ERR_INVALID
+    assert "not a factorized tree" in _lib.last_error(None)
+
+
+def test_save_needs_a_factorization(tmp_path):
+    import robinsolver_b200 as rb
+    from robinsolver_b200 import workloads as W
+    wl = W.make_workload(1)
+    T = rb.robin_tree()
+    T.bndry_params = wl.bndry_params
+    T.plan(wl.L, rb.elliptic_operator(d=2, domain=wl.domain, k=wl.potential), rb.solve_opts(h_tgt=wl.h_tgt, kb=wl.opts_kb))
+    with pytest.raises(rb.RobinSolverError):
+        T.save(tmp_path / "t.rbt")
+    T.close()
