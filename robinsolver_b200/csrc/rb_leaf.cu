@@ -36,6 +36,8 @@
 //     f_r = 2 i kb / d_r.
 // The leaf solve applies A^-1 [g; f] (fd_leaf_solve + fd_leaf_update, fd_module.f90:390-566)
 // through the same block factors: t = f - A_ib A_bb^-1 g, S u_i = t, u_b = (g - A_bi u_i)/d.
+#include <cstdlib>
+#include "rb_gemm_dmma.cuh"   // dmma884
 #include "rb_kernels.h"
 
 namespace rb {
@@ -470,8 +472,304 @@ size_t leaf_block_factor_smem(const LeafGeom& g) {
     return (2 * (size_t)g.a * g.a + 2 * (size_t)g.a * g.nb + g.a) * sizeof(z) + (g.a + 1) * sizeof(int) + 16;
 }
 
+// ---------------------------------------------------------------------------------------------------
+// Tensor-core leaf factor for 16 x b leaves with nb <= 64 boundary points: one warp per leaf, the
+// block LU of leaf_warp_factor_kernel, and the two sweeps of S^T Z = C^T as FP64 tensor-core
+// products (mma.sync m8n8k4 .f64, four real products per complex one) over chunks of 32
+// right-hand sides: block step j is V_j = Sig_j^-T R_j with R_j (16 x 32) in shared memory.
+// The forward step of block j runs as soon as the LU has Sig_j^-1 in the warp's shared memory,
+// so the forward sweep never reloads it; the backward sweep reloads one block per step.
+//   forward:  R_0 = C_0;  V_j = Sig_j^-T R_j;  R_{j+1} = C_{j+1} - Up_j V_j
+//   backward: Z_{b-1} = V_{b-1};  Z_{j-1} = V_{j-1} - Sig_{j-1}^-T (Lo_j Z_j)
+// C_j holds, per right-hand side c, c1 and c2 at the interior points next to boundary point c.
+constexpr int LTC_CH = 2;        // chunks of 32 right-hand sides (nb <= 64)
+constexpr int LTC_LDR = 18;      // padded leading dimension of the R buffers (bank spread)
+
+// acc (2 x 4 tiles of 8x8, complex as re/im) += A B,  A(i,k) = As[k + 16 i],  B(k,c) = Bs[k + LTC_LDR c]
+__device__ __forceinline__ void ltc_mma(const z* As, const z* Bs, double (&cre)[2][4][2], double (&cim)[2][4][2],
+                                        int lane) {
+    const int lr = lane >> 2, lc = lane & 3;
+#pragma unroll
+    for (int ks = 0; ks < 4; ++ks) {
+        double ar[2], ai[2], nai[2], br[4], bi[4];
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi) {
+            const z a = As[(4 * ks + lc) + 16 * (8 * mi + lr)];
+            ar[mi] = a.x;
+            ai[mi] = a.y;
+            nai[mi] = -a.y;
+        }
+#pragma unroll
+        for (int ni = 0; ni < 4; ++ni) {
+            const z b = Bs[(4 * ks + lc) + LTC_LDR * (8 * ni + lr)];
+            br[ni] = b.x;
+            bi[ni] = b.y;
+        }
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) dmma884(cre[mi][ni][0], cre[mi][ni][1], ar[mi], br[ni]);
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) dmma884(cim[mi][ni][0], cim[mi][ni][1], ar[mi], bi[ni]);
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) dmma884(cre[mi][ni][0], cre[mi][ni][1], nai[mi], bi[ni]);
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+            for (int ni = 0; ni < 4; ++ni) dmma884(cim[mi][ni][0], cim[mi][ni][1], ai[mi], br[ni]);
+    }
+}
+
+// R_j's sparse part: lane c (a right-hand side of chunk ch) adds c1, c2 where its two interior
+// points fall in block j (interior index q = 16 j + row)
+__device__ __forceinline__ void ltc_add_c(z* R, int ch, int j, int lane, int b, int nb, const LeafConst& L) {
+    const int c = 32 * ch + lane;
+    if (c >= nb) return;
+    int ax, q1, q2;
+    leaf_bpoint2(16, b, c, ax, q1, q2);
+    const double h = ax == 0 ? L.hx : L.hy;
+    const double c1 = -3.0 / h, c2 = (1.0 / 3.0) / h;
+    const int q0 = 16 * j;
+    if (q1 >= q0 && q1 < q0 + 16) R[(q1 - q0) + LTC_LDR * lane].x += c1;
+    if (q2 >= q0 && q2 < q0 + 16) R[(q2 - q0) + LTC_LDR * lane].x += c2;
+}
+
+__global__ void __launch_bounds__(128) leaf_tc_factor_kernel(LeafGeom g, int nleaves, const double* __restrict__ hh,
+                                                             const z* __restrict__ kv, z* __restrict__ sinv,
+                                                             z* __restrict__ Y, int* status) {
+    constexpr int A = 16, AA = 256;
+    extern __shared__ z ltc_smem[];
+    __shared__ int wpiv[4][2 * A];
+    const int lane = threadIdx.x & 31, wib = threadIdx.x >> 5;
+    const int leaf = blockIdx.x * 4 + wib;
+    if (leaf >= nleaves) return;
+    z* sm = ltc_smem + (size_t)wib * (AA + LTC_CH * LTC_LDR * 32);
+    z* R = sm + AA;                                  // LTC_CH buffers of LTC_LDR x 32
+    int* piv = wpiv[wib];
+    const int b = g.b, nb = g.nb, n = g.n, ab = A * b;
+    const int nch = (nb + 31) / 32;
+    const LeafConst L = leaf_const(hh, leaf, g.kb);
+    const z* kl = kv + (size_t)leaf * ab;
+    z* Sl = sinv + (size_t)leaf * b * AA;
+    z* Yl = Y + (size_t)leaf * nb * n;
+    const int r = lane & 15, hf = lane >> 4;
+    const int lr = lane >> 2, lc = lane & 3;
+    z a[8], prev[8];
+    bool ok = true;
+
+    // R_0 = C_0
+    for (int ch = 0; ch < nch; ++ch) {
+        z* Rc = R + ch * LTC_LDR * 32;
+        for (int e = lane; e < LTC_LDR * 32; e += 32) Rc[e] = zmk(0.0, 0.0);
+        __syncwarp();
+        ltc_add_c(Rc, ch, 0, lane, b, nb, L);
+    }
+    __syncwarp();
+
+    for (int j = 0; j < b; ++j) {
+        // ---- block LU step: Sig_j^-1 (leaf_warp_factor_kernel's Gauss-Jordan) -----------------------
+        const int jj = j + 1;
+        const z lm = jj > 1 ? zmul(block_lo(L, b, jj), block_up(L, b, jj - 1)) : zmk(0.0, 0.0);
+        const z kr = kl[j * A + r];
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            z v = block_d(L, A, b, jj, r, hf * 8 + e, kr);
+            if (jj > 1) zfms(v, lm, prev[e]);
+            a[e] = v;
+        }
+#pragma unroll
+        for (int k = 0; k < A; ++k) {
+            const int hk = k >> 3, ek = k & 7;
+            double mag = (hf == hk && r >= k) ? zabs1(a[ek]) : -1.0;
+            int idx = r;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double om = __shfl_xor_sync(0xffffffffu, mag, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+                if (om > mag || (om == mag && oi < idx)) { mag = om; idx = oi; }
+            }
+            const int p = idx;
+            if (lane == 0) piv[k] = p;
+            if (p != k) {
+                const int src = (r == k ? p : (r == p ? k : r)) + 16 * hf;
+#pragma unroll
+                for (int e = 0; e < 8; ++e) {
+                    const double x = __shfl_sync(0xffffffffu, a[e].x, src);
+                    const double y = __shfl_sync(0xffffffffu, a[e].y, src);
+                    a[e] = zmk(x, y);
+                }
+            }
+            const z pv = zmk(__shfl_sync(0xffffffffu, a[ek].x, k + 16 * hk),
+                             __shfl_sync(0xffffffffu, a[ek].y, k + 16 * hk));
+            if (pv.x == 0.0 && pv.y == 0.0) ok = false;
+            const z pinv = zrcp(pv);
+            const z f = zmk(__shfl_sync(0xffffffffu, a[ek].x, r + 16 * hk),
+                            __shfl_sync(0xffffffffu, a[ek].y, r + 16 * hk));
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const z pr = zmul(zmk(__shfl_sync(0xffffffffu, a[e].x, k + 16 * hf),
+                                      __shfl_sync(0xffffffffu, a[e].y, k + 16 * hf)), pinv);
+                const bool colk = (hf == hk) && (e == ek);
+                if (r == k) a[e] = colk ? pinv : pr;
+                else if (colk) a[e] = zneg(zmul(f, pinv));
+                else zfms(a[e], f, pr);
+            }
+        }
+        __syncwarp();
+        if (lane == 0) {
+            int sg[A];
+            for (int c = 0; c < A; ++c) sg[c] = c;
+            for (int k = A - 1; k >= 0; --k) {
+                const int p = piv[k];
+                const int t = sg[k];
+                sg[k] = sg[p];
+                sg[p] = t;
+            }
+            for (int c = 0; c < A; ++c) piv[A + sg[c]] = c;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int e = 0; e < 8; ++e) sm[r + piv[A + hf * 8 + e] * A] = a[e];
+        __syncwarp();
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            prev[e] = sm[r + (hf * 8 + e) * A];
+            Sl[(size_t)j * AA + r + (hf * 8 + e) * A] = prev[e];
+        }
+        __syncwarp();
+        // ---- forward step j for every chunk: V_j = Sig_j^-T R_j -----------------------------------
+        const z mup = block_up(L, b, jj);            // Up_j, for R_{j+1}
+        for (int ch = 0; ch < nch; ++ch) {
+            z* Rc = R + ch * LTC_LDR * 32;
+            double cre[2][4][2], cim[2][4][2];
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni) cre[mi][ni][0] = cre[mi][ni][1] = cim[mi][ni][0] = cim[mi][ni][1] = 0.0;
+            ltc_mma(sm, Rc, cre, cim, lane);
+            __syncwarp();                              // every lane has read R_j
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int i = 8 * mi + lr, cl = 8 * ni + 2 * lc + h, c = 32 * ch + cl;
+                        const z v = zmk(cre[mi][ni][h], cim[mi][ni][h]);
+                        if (c < nb) Yl[c + (size_t)(nb + j * A + i) * nb] = v;
+                        // next: R_{j+1} = C_{j+1} - Up_j V_j  (backward start: -Lo_b Z_{b-1})
+                        Rc[i + LTC_LDR * cl] = zneg(zmul(jj < b ? mup : block_lo(L, b, b), v));
+                    }
+            __syncwarp();
+            if (jj < b) ltc_add_c(Rc, ch, j + 1, lane, b, nb, L);
+        }
+        __syncwarp();
+    }
+    if (!ok && lane == 0) atomicOr(status, 1);
+
+    // ---- backward sweep, Y(c, nb+s) = f_c Q(c, s) stored already scaled -------------------------------
+    z fcl[4][2];                                      // f_c of this lane's columns, per chunk below
+    for (int j = b - 1; j >= 0; --j) {
+        // j >= 1: Z_{j-1} = V_{j-1} + Sig_{j-1}^-T R  with R = -Lo_j Z_j;  the final step (j = 0) only
+        // rescales block... handled by storing Z_{b-1} first
+        if (j == b - 1) {
+            for (int ch = 0; ch < nch; ++ch) {
+                // Z_{b-1} = V_{b-1}, scaled
+#pragma unroll
+                for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                    for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const int i = 8 * mi + lr, c = 32 * ch + 8 * ni + 2 * lc + h;
+                            if (c >= nb) continue;
+                            int ax, q1, q2;
+                            leaf_bpoint2(A, b, c, ax, q1, q2);
+                            const z fc = zmul(zmk(0.0, 2.0 * g.kb), ax == 0 ? L.rdx : L.rdy);
+                            z* yp = Yl + c + (size_t)(nb + j * A + i) * nb;
+                            *yp = zmul(fc, *yp);
+                        }
+            }
+        }
+        if (j == 0) break;
+#pragma unroll
+        for (int e = 0; e < 8; ++e) sm[r + (hf * 8 + e) * A] = Sl[(size_t)(j - 1) * AA + r + (hf * 8 + e) * A];
+        __syncwarp();
+        const z lamn = j >= 2 ? block_lo(L, b, j) : zmk(0.0, 0.0);   // Lo_{j-1}, for the next step
+        for (int ch = 0; ch < nch; ++ch) {
+            z* Rc = R + ch * LTC_LDR * 32;
+            double cre[2][4][2], cim[2][4][2];
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int i = 8 * mi + lr, c = 32 * ch + 8 * ni + 2 * lc + h;
+                        const z v = c < nb ? Yl[c + (size_t)(nb + (j - 1) * A + i) * nb] : zmk(0.0, 0.0);
+                        cre[mi][ni][h] = v.x;
+                        cim[mi][ni][h] = v.y;
+                        int ax, q1, q2;
+                        leaf_bpoint2(A, b, c < nb ? c : 0, ax, q1, q2);
+                        fcl[ni][h] = zmul(zmk(0.0, 2.0 * g.kb), ax == 0 ? L.rdx : L.rdy);
+                    }
+            ltc_mma(sm, Rc, cre, cim, lane);
+            __syncwarp();
+#pragma unroll
+            for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+                for (int ni = 0; ni < 4; ++ni)
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const int i = 8 * mi + lr, cl = 8 * ni + 2 * lc + h, c = 32 * ch + cl;
+                        const z zv = zmk(cre[mi][ni][h], cim[mi][ni][h]);
+                        if (c < nb) Yl[c + (size_t)(nb + (j - 1) * A + i) * nb] = zmul(fcl[ni][h], zv);
+                        Rc[i + LTC_LDR * cl] = zneg(zmul(lamn, zv));
+                    }
+            __syncwarp();
+        }
+    }
+    __syncwarp();
+    // ---- Y(:, 0:nb) from the scaled Y(r, nb+s) = f_r Q(r, s) ----------------------------------------
+    for (int e = lane; e < nb * nb; e += 32) {
+        const int rr = e % nb, c = e / nb;
+        int ax, p1, p2, axc, q1, q2;
+        leaf_bpoint2(A, b, rr, ax, p1, p2);
+        leaf_bpoint2(A, b, c, axc, q1, q2);
+        const z rd = ax == 0 ? L.rdx : L.rdy;
+        const z wd = axc == 0 ? zscale(L.wbx, L.rdx) : zscale(L.wby, L.rdy);
+        z val = zneg(zmul(wd, Yl[rr + (size_t)(nb + q1) * nb]));
+        if (c == rr) {
+            const double hr2 = ax == 0 ? L.hx : L.hy;
+            val = zadd(val, zmul(zmk((8.0 / 3.0) / hr2, -g.kb), rd));
+        }
+        Yl[e] = val;
+    }
+}
+
+static bool leaf_tc_enabled() {
+    const char* v = std::getenv("RB_LEAF_ENGINE");
+    return !(v && v[0] == 'd');       // RB_LEAF_ENGINE=dfma: the DFMA warp kernel (comparisons)
+}
+
 cudaError_t leaf_block_factor(const LeafGeom& g, int nleaves, const double* h, const z* k, z* sinv, z* Y,
                               int* status, cudaStream_t s) {
+    if (g.a == 16 && g.nb <= 32 * LTC_CH && leaf_tc_enabled()) {     // one warp per leaf, tensor cores
+        const size_t sh = 4 * (256 + (size_t)LTC_CH * LTC_LDR * 32) * sizeof(z);
+        static bool attr = false;
+        if (!attr) {
+            cudaError_t e = cudaFuncSetAttribute(leaf_tc_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+            if (e != cudaSuccess) return e;
+            attr = true;
+        }
+        leaf_tc_factor_kernel<<<(nleaves + 3) / 4, 128, sh, s>>>(g, nleaves, h, k, sinv, Y, status);
+        note_launch();
+        return cudaGetLastError();
+    }
     if (g.a == 16) {                        // one warp per leaf
         leaf_warp_factor_kernel<<<(nleaves + 3) / 4, 128, 0, s>>>(g, nleaves, h, k, sinv, Y, status);
         note_launch();
