@@ -109,6 +109,15 @@ struct GemmBatch {
     int kchunk = 0;
     z* work = nullptr;
     long long pstride = 0;
+    // every problem's k runs contiguously through both operands (gemm_k_contiguous), so operand
+    // copies may advance by a fixed stride per k-tile
+    bool kcontig = false;
 };
+
+// A(i, k) sits at A.p[row(i) + k * A.ld] and B(k, j) at B.p[k + col(j) * B.ld] for every k < K:
+// no map on A's columns or B's rows, and no skipped band that starts below K
+__host__ __device__ inline bool gemm_k_contiguous(const GemmDesc& g) {
+    return !g.A.cmap && (g.A.cl == 0 || g.A.cs >= g.k) && !g.B.rmap && (g.B.rl == 0 || g.B.rs >= g.k);
+}
 
 }  // namespace rb

@@ -105,6 +105,40 @@ static cudaError_t launch_dmma(const GemmBatch& b, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+template <int BM, int BN, int WM, int WN, int BK, int STAGES, int MINB>
+__global__ void __launch_bounds__(32 * WM * WN, MINB) zgemm_dmma_kc_kernel(const GemmDesc* __restrict__ descs) {
+    extern __shared__ z dmma_smem[];
+    __shared__ GemmDesc sd;
+    {
+        const unsigned long long* src = reinterpret_cast<const unsigned long long*>(descs + blockIdx.y);
+        unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sd);
+        for (int w = threadIdx.x; w < (int)(sizeof(GemmDesc) / 8); w += 32 * WM * WN) dst[w] = src[w];
+    }
+    __syncthreads();
+    zgemm_tile_dmma_kc<BM, BN, WM, WN, BK, STAGES>(sd, blockIdx.x, dmma_smem);
+}
+
+template <int BM, int BN, int WM, int WN, int BK, int STAGES, int MINB>
+static cudaError_t launch_dmma_kc(const GemmBatch& b, cudaStream_t s) {
+    using Cfg = DmmaKcCfg<BM, BN, WM, WN, BK, STAGES>;
+    auto kern = zgemm_dmma_kc_kernel<BM, BN, WM, WN, BK, STAGES, MINB>;
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    const int tiles = ((b.max_m + BM - 1) / BM) * ((b.max_n + BN - 1) / BN);
+    for (int off = 0; off < b.count; off += 65535) {
+        const int cnt = (b.count - off) < 65535 ? (b.count - off) : 65535;
+        kern<<<dim3(tiles, cnt), Cfg::NT, Cfg::SMEM_BYTES, s>>>(b.d_desc + off);
+        note_launch();
+    }
+    return cudaGetLastError();
+}
+
 // GEMM engine for the large problems: FP64 tensor-core MMA (default) or DFMA register tiles
 // (RB_GEMM_ENGINE=dfma, read once; a tuning knob for comparisons)
 static bool use_dmma() {
@@ -161,7 +195,7 @@ static cudaError_t launch_split(const GemmBatch& b, cudaStream_t s) {
 }
 
 // the kernel shape a batch runs on
-enum class GemmShape { Dfma16, Dfma32, Dmma32, Dmma64, Dfma128x64, Dfma64 };
+enum class GemmShape { Dfma16, Dfma32, Dmma32, Dmma64, DmmaKc64, Dfma128x64, Dfma64 };
 static GemmShape gemm_shape(const GemmBatch& b) {
     const int mm = b.max_m, nn = b.max_n;
     if (mm <= 16 && nn <= 16) return GemmShape::Dfma16;
@@ -177,7 +211,13 @@ static GemmShape gemm_shape(const GemmBatch& b) {
     // FP64 tensor cores: 64x64 tiles of 8 warps, two CTAs per SM (16 warps to hide the MMA and
     // shared-memory latencies); measured faster than 128x64 tiles at one CTA per SM on every
     // merge shape from 64x256x64 x256 to 2048x4096x1024 x2
-    if (use_dmma() && !b.fixed_order) return GemmShape::Dmma64;
+    if (use_dmma() && !b.fixed_order) {
+        // contiguous-k batches with k >= 128: 32x32 warp tiles on stride-advanced copies,
+        // measured 1.06-1.22x the tile above on the merge shapes 256x256x128 x256 ..
+        // 2048x4096x1024 x2 (0.95x on 256x768x256 x8 and 128x512x128 x64, under two waves)
+        if (b.kcontig && b.max_k >= 128) return GemmShape::DmmaKc64;
+        return GemmShape::Dmma64;
+    }
     // large problems: 8x4 complex register tile per thread (1.5 B of shared memory per DFMA)
     const bool big = mm >= 256 && nn >= 128 && (long long)b.count * ((mm + 127) / 128) * ((nn + 63) / 64) >= 148;
     return big ? GemmShape::Dfma128x64 : GemmShape::Dfma64;
@@ -210,7 +250,7 @@ long long gemm_plan_split(GemmBatch& b) {
 
 const char* gemm_stage_name(const GemmBatch& b) {
     const GemmShape sh = gemm_shape(b);
-    return (sh == GemmShape::Dmma64 || sh == GemmShape::Dmma32) ? "zgemm_tc" : "zgemm_dfma";
+    return (sh == GemmShape::Dmma64 || sh == GemmShape::Dmma32 || sh == GemmShape::DmmaKc64) ? "zgemm_tc" : "zgemm_dfma";
 }
 
 cudaError_t launch_gemm_batch(const GemmBatch& b, cudaStream_t s) {
@@ -228,6 +268,7 @@ cudaError_t launch_gemm_batch(const GemmBatch& b, cudaStream_t s) {
         case GemmShape::Dfma32: return launch_cfg<32, 32, 4, 2, 8, 4, 4>(b, s);
         case GemmShape::Dmma32: return launch_dmma<32, 32, 2, 2, 6>(b, s);
         case GemmShape::Dmma64: return launch_dmma<64, 64, 2, 4, 2>(b, s);
+        case GemmShape::DmmaKc64: return launch_dmma_kc<64, 64, 2, 2, 4, 8, 2>(b, s);
         case GemmShape::Dfma128x64: return launch_cfg<128, 64, 8, 4, 4, 4, 1>(b, s);
         case GemmShape::Dfma64: break;
     }

@@ -220,11 +220,13 @@ static int upload_gemm(rb_tree* t, std::vector<DevBuf>& list, const std::vector<
     int rc = alloc_n(t, list, h.size(), &b.d_desc);
     if (rc) return rc;
     RB_CK(cudaMemcpy(b.d_desc, h.data(), h.size() * sizeof(GemmDesc), cudaMemcpyHostToDevice));
+    b.kcontig = true;
     for (const auto& d : h) {
         b.max_m = std::max(b.max_m, d.m);
         b.max_n = std::max(b.max_n, d.n);
         b.max_k = std::max(b.max_k, d.k);
         b.flops += 8.0 * d.m * d.n * d.k;
+        b.kcontig = b.kcontig && gemm_k_contiguous(d);
     }
     return RB_OK;
 }
