@@ -31,6 +31,7 @@
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <functional>
 #include <vector>
 
 #include "robin_b200.h"
@@ -85,7 +86,9 @@ struct rb_tree {
     // time and status are taken by the next call that needs them (settle_factor)
     bool async_factor = false;
     bool factor_pending = false;
-    int* h_status = nullptr;             // pinned copy of the factor's status word
+    int* h_status = nullptr;             // pinned: [0] the factor's status word after the factor,
+                                         // [1] the same word as the overlapped solve saw it
+    bool solve_overlapped = false;       // the last solve ran beside its factor (on stream3)
     std::vector<cudaEvent_t> ev_fork, ev_join;
     // factor progress for a solve that overlaps it: [l] after level l's inversion, [L] after the leaves
     std::vector<cudaEvent_t> ev_lvl;
@@ -362,13 +365,19 @@ static int ensure_factor_storage(rb_tree* t) {
     RB_CK(cudaGetDevice(&t->device));
     if (!t->stream) RB_CK(cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking));
     if (!t->stream2) RB_CK(cudaStreamCreateWithFlags(&t->stream2, cudaStreamNonBlocking));
-    if (!t->stream3) RB_CK(cudaStreamCreateWithFlags(&t->stream3, cudaStreamNonBlocking));
+    if (!t->stream3) {
+        // the solve runs here beside a factor: at the highest priority its small, latency-bound
+        // kernels take SMs ahead of the factor's large GEMMs as their CTAs retire
+        int least = 0, greatest = 0;
+        RB_CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        RB_CK(cudaStreamCreateWithPriority(&t->stream3, cudaStreamNonBlocking, greatest));
+    }
     if (!t->ev_copy) RB_CK(cudaEventCreateWithFlags(&t->ev_copy, cudaEventDisableTiming));
     for (auto& e : t->ev)
         if (!e) RB_CK(cudaEventCreate(&e));
     if (!t->h_status) {
-        RB_CK(cudaMallocHost(&t->h_status, sizeof(int)));
-        *t->h_status = 0;
+        RB_CK(cudaMallocHost(&t->h_status, 2 * sizeof(int)));
+        t->h_status[0] = t->h_status[1] = 0;
     }
     t->ev_fork.assign(L, nullptr);
     t->ev_join.assign(L, nullptr);
@@ -554,7 +563,11 @@ static double leaf_flops(const LeafGeom& g) {
 }
 
 // rec (optional): events recorded as the factor progresses, for a solve on another stream
-static int run_factor(rb_tree* t, const z* dk, const std::vector<cudaEvent_t>* rec = nullptr) {
+// rec: progress events, one per level (the leaves at L), for a solve that overlaps the factor.
+// before_root_tail: enqueued once the root's interface inverse is ready (and rec[0] recorded),
+// ahead of the root's Y1, Y2 and own map, which then wait for it on the main stream.
+static int run_factor(rb_tree* t, const z* dk, const std::vector<cudaEvent_t>* rec = nullptr,
+                      const std::function<int()>* before_root_tail = nullptr) {
     const Plan& P = t->P;
     const int L = P.L, nl = P.nleaves();
     LeafGeom lg{P.leaf_a(), P.leaf_b(), P.leaf_nb(), P.leaf_n(), P.kb};
@@ -593,6 +606,7 @@ static int run_factor(rb_tree* t, const z* dk, const std::vector<cudaEvent_t>* r
             if (rec) RB_CK(cudaEventRecord((*rec)[l], s));      // inv(K), A1, A2 of level l are ready
             if (fork) RB_CK(cudaStreamWaitEvent(s, t->ev_join[l], 0));
             else RB_GEMM(t->fM1[l], s);
+            if (l == 0 && before_root_tail && (rc = (*before_root_tail)())) return rc;
         } else {
             RB_TIMED("merge_form", 0.0, merge_form_d(cs, p.nnodes, p.m, p.o2, t->zeta, t->dinv[l], s));
             RB_TIMED("gj_invert", gj_flops(p.m, p.nnodes), gj_invert_batch(t->gj_d[l].d_desc, p.nnodes, p.m, t->gj_work, t->d_status, s));
@@ -609,6 +623,7 @@ static int run_factor(rb_tree* t, const z* dk, const std::vector<cudaEvent_t>* r
             if (rec) RB_CK(cudaEventRecord((*rec)[l], s));      // inv(D), inv(S) of level l are ready
             if (fork) RB_CK(cudaStreamWaitEvent(s, t->ev_join[l], 0));
             else RB_GEMM(t->fM1[l], s);
+            if (l == 0 && before_root_tail && (rc = (*before_root_tail)())) return rc;
         }
         RB_GEMM(t->fM2[l], s);
         RB_GEMM(t->fM3[l], s);
@@ -995,21 +1010,32 @@ int rb_tree_sample_points(const rb_tree* t, int which, double* xyz) {
 }
 
 // Enqueues the factor of t->d_k on the main stream: replayed as a graph, or launched directly
-// with progress events (rec) for a solve that overlaps it.
-static int launch_factor(rb_tree* t, const std::vector<cudaEvent_t>* rec) {
+// with progress events (rec) for a solve that overlaps it (before_root_tail: see run_factor; the
+// launches it makes are its own).
+static int launch_factor(rb_tree* t, const std::vector<cudaEvent_t>* rec,
+                         const std::function<int()>* before_root_tail = nullptr) {
     int rc;
     const long long l0 = launch_count();
+    long long hook_launches = 0;
     t->factor_deferred = false;
     RB_CK(cudaEventRecord(t->ev[0], t->stream));
     if (rec) {
-        if ((rc = run_factor(t, t->d_k, rec))) return rc;
+        std::function<int()> counted;
+        if (before_root_tail)
+            counted = [&] {
+                const long long h0 = launch_count();
+                const int r = (*before_root_tail)();
+                hook_launches = launch_count() - h0;
+                return r;
+            };
+        if ((rc = run_factor(t, t->d_k, rec, before_root_tail ? &counted : nullptr))) return rc;
     } else if ((rc = run_graphed(t, t->gx_factor, t->gx_factor_launches, t->factor_runs,
                                  [&] { return run_factor(t, t->d_k); }))) {
         return rc;
     }
     RB_CK(cudaMemcpyAsync(t->h_status, t->d_status, sizeof(int), cudaMemcpyDeviceToHost, t->stream));
     RB_CK(cudaEventRecord(t->ev[1], t->stream));
-    t->factor_launches = launch_count() - l0;
+    t->factor_launches = launch_count() - l0 - hook_launches;
     t->factor_pending = true;
     return RB_OK;
 }
@@ -1033,6 +1059,21 @@ static int settle_factor(rb_tree* t) {
         return fail(t, RB_ERR_NUMERIC, "zero pivot met while inverting a leaf or interface matrix");
     }
     if (t->verbose) std::printf("RTR computation completed.\nFactorization completed.\n");
+    return RB_OK;
+}
+
+// Waits until the last solve's solution is in device memory and reports a failed factor.  After a
+// solve that ran beside its factor the factor may still be finishing the root's own map, which no
+// solve reads: its status word is complete once the root's interface inverse is, and the solve
+// copied it then.
+static int settle_solution(rb_tree* t) {
+    if (!t->solve_overlapped) return settle_factor(t);
+    RB_CK(cudaEventSynchronize(t->ev[3]));
+    if (t->h_status[1]) {
+        t->factored = false;
+        t->nrhs = 0;
+        return fail(t, RB_ERR_NUMERIC, "zero pivot met while inverting a leaf or interface matrix");
+    }
     return RB_OK;
 }
 
@@ -1098,21 +1139,37 @@ static int solve_common(rb_tree* t, int nrhs, const double* f, const double* g, 
     const size_t nroot = (size_t)P.lv[0].nb;
     const cudaMemcpyKind kind = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
     t->nrhs = 0;
+    t->solve_overlapped = false;
     if (t->factor_deferred && t->timing == 0) {
         // factor and solve together: the factor on the main stream, the solve on the copy stream
         // right after its inputs, each solve level waiting for that level of the factor; the main
-        // stream then waits for the solve, so later calls see both finished
+        // stream then waits for the solve, so later calls see both finished.  With host buffers
+        // the caller reads the solution back next, so the solve is put first: the root's Y1, Y2
+        // and own map (which no solve reads) wait for it and overlap the read-back instead of
+        // competing with the solve's last levels.
         RB_CK(cudaEventRecord(t->ev_copy, t->stream));       // device inputs are ordered there
         RB_CK(cudaStreamWaitEvent(t->stream3, t->ev_copy, 0));
         RB_CK(cudaMemcpyAsync(t->d_f, f, nrhs * nint * sizeof(z), kind, t->stream3));
         RB_CK(cudaMemcpyAsync(t->gbuf[0], g, nrhs * nroot * sizeof(z), kind, t->stream3));
-        if ((rc = launch_factor(t, &t->ev_lvl))) return rc;
-        const long long l0 = launch_count();
-        RB_CK(cudaEventRecord(t->ev[2], t->stream3));
-        if ((rc = run_solve(t, nrhs, t->stream3, &t->ev_lvl))) return rc;
-        RB_CK(cudaEventRecord(t->ev[3], t->stream3));
-        RB_CK(cudaStreamWaitEvent(t->stream, t->ev[3], 0));
-        t->solve_launches = launch_count() - l0;
+        const std::function<int()> enqueue_solve = [&]() -> int {
+            const long long l0 = launch_count();
+            RB_CK(cudaEventRecord(t->ev[2], t->stream3));
+            if (int r = run_solve(t, nrhs, t->stream3, &t->ev_lvl)) return r;
+            // every status write (leaf factor, interface inverses) precedes the root level's
+            // event, which the solve waited for
+            RB_CK(cudaMemcpyAsync(t->h_status + 1, t->d_status, sizeof(int), cudaMemcpyDeviceToHost, t->stream3));
+            RB_CK(cudaEventRecord(t->ev[3], t->stream3));
+            RB_CK(cudaStreamWaitEvent(t->stream, t->ev[3], 0));
+            t->solve_launches = launch_count() - l0;
+            return RB_OK;
+        };
+        if (host) {
+            if ((rc = launch_factor(t, &t->ev_lvl, &enqueue_solve))) return rc;
+        } else {
+            if ((rc = launch_factor(t, &t->ev_lvl))) return rc;
+            if ((rc = enqueue_solve())) return rc;
+        }
+        t->solve_overlapped = true;
     } else {
         if (t->factor_deferred && (rc = launch_factor(t, nullptr))) return rc;
         if (host) {
@@ -1141,8 +1198,12 @@ static int solve_common(rb_tree* t, int nrhs, const double* f, const double* g, 
         RB_CK(cudaEventRecord(t->ev[3], t->stream));
     }
     if (host || sync) {
-        RB_CK(cudaStreamSynchronize(t->stream));
-        if ((rc = settle_factor(t))) return rc;
+        if (t->solve_overlapped) {
+            if ((rc = settle_solution(t))) return rc;
+        } else {
+            RB_CK(cudaStreamSynchronize(t->stream));
+            if ((rc = settle_factor(t))) return rc;
+        }
         float ms = 0.f;       // beside an overlapped factor this spans the wait for its levels too
         RB_CK(cudaEventElapsedTime(&ms, t->ev[2], t->ev[3]));
         t->s_time = ms * 1e-3;
@@ -1163,13 +1224,15 @@ int rb_tree_solve_device(rb_tree* t, int nrhs, const double* f, const double* g,
 int rb_get_solution(const rb_tree* tc, int irhs, double* u, double* boxes) {
     rb_tree* t = const_cast<rb_tree*>(tc);
     if (!t || !u) return RB_ERR_INVALID;
-    if (int rc = settle_factor(t)) return rc;
+    if (int rc = (t->factor_deferred || t->nrhs == 0) ? settle_factor(t) : settle_solution(t)) return rc;
     if (!t->factored) return fail(t, RB_ERR_NOT_FACTORED, "Error in GET_SOLUTION: Robin Tree not factored.");
     if (irhs < 0 || irhs >= t->nrhs) return fail(t, RB_ERR_NO_SOLUTION, "get_solution: no solution for this right-hand side");
     const Plan& P = t->P;
     const size_t per = (size_t)P.nleaves() * P.leaf_n();
-    RB_CK(cudaMemcpyAsync(u, t->sol + (size_t)irhs * per, per * sizeof(z), cudaMemcpyDeviceToHost, t->stream));
-    RB_CK(cudaStreamSynchronize(t->stream));
+    // on the copy stream after the solve: a factor's remaining root work may run beside it
+    RB_CK(cudaStreamWaitEvent(t->stream3, t->ev[3], 0));
+    RB_CK(cudaMemcpyAsync(u, t->sol + (size_t)irhs * per, per * sizeof(z), cudaMemcpyDeviceToHost, t->stream3));
+    RB_CK(cudaStreamSynchronize(t->stream3));
     if (boxes) {
         const PlanLevel& lf = P.lv[P.L];
         for (int i = 0; i < lf.nnodes; ++i)
