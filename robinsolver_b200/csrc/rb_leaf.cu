@@ -37,6 +37,7 @@
 // The leaf solve applies A^-1 [g; f] (fd_leaf_solve + fd_leaf_update, fd_module.f90:390-566)
 // through the same block factors: t = f - A_ib A_bb^-1 g, S u_i = t, u_b = (g - A_bi u_i)/d.
 #include <cstdlib>
+#include <cstring>
 #include "rb_gemm_dmma.cuh"   // dmma884
 #include "rb_kernels.h"
 
@@ -790,6 +791,17 @@ cudaError_t leaf_block_factor(const LeafGeom& g, int nleaves, const double* h, c
 // RHS are processed in chunks of KC columns; shared memory: sig (a^2), w0, w1 (a x KC each).
 constexpr int LEAF_KC = 32;
 
+// leaf solve engine: the half-warp kernel for 16-point leaves (default) or the block kernel
+// (RB_LEAF_SOLVE=block, read once; a comparison knob)
+static bool leaf_solve_engine_hw() {
+    static int v = -1;
+    if (v < 0) {
+        const char* e = std::getenv("RB_LEAF_SOLVE");
+        v = (e && std::strcmp(e, "block") == 0) ? 0 : 1;
+    }
+    return v == 1;
+}
+
 __global__ void __launch_bounds__(256) leaf_block_solve_kernel(LeafGeom g, int nleaves, int nrhs,
                                                                const double* __restrict__ hh,
                                                                const z* __restrict__ f, const z* __restrict__ gb,
@@ -870,8 +882,155 @@ __global__ void __launch_bounds__(256) leaf_block_solve_kernel(LeafGeom g, int n
     }
 }
 
+// The same solve for leaves 16 points wide (a == 16), one CTA of 8 warps per leaf and 32
+// right-hand sides at a time.  Each half-warp owns a right-hand side column, lane i its row i,
+// so a block step's recurrence stays in the lane's registers and its 16-term products exchange
+// values through shared memory within the warp.  The next step's Sig_j^-1 block and its right-hand
+// side block (f_j forward, the stored w_j backward) are fetched with cp.async while the current
+// step runs: one block barrier per step, which also releases the buffer the next fetch
+// overwrites.  Same operations in the same order as leaf_block_solve_kernel.
+constexpr int LHW_KC = 32;
+__global__ void __launch_bounds__(256, 3) leaf_hw_solve_kernel(LeafGeom g, int nleaves, int nrhs,
+                                                            const double* __restrict__ hh,
+                                                            const z* __restrict__ f, const z* __restrict__ gb,
+                                                            const z* __restrict__ sinv, z* __restrict__ sol) {
+    constexpr int A = 16, AA = A * A, KC = LHW_KC, CPH = KC / 16;   // columns per half-warp
+    extern __shared__ z sm[];
+    const int leaf = blockIdx.x;
+    const int b = g.b, nb = g.nb, n = g.n, ab = A * b;
+    z* sig = sm;                       // [2][AA]: Sig_j^-1 of the current and the next step
+    z* blk = sig + 2 * AA;             // [2][A*KC]: the steps' right-hand side blocks
+    z* gsm = blk + 2 * A * KC;         // [KC][nb]: boundary data of the chunk
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int i = lane & 15, half = lane >> 4;
+    const LeafConst L = leaf_const(hh, leaf, g.kb);
+    const z* Sl = sinv + (size_t)leaf * b * AA;
+    const z wdx = zscale(L.wbx, L.rdx), wdy = zscale(L.wby, L.rdy);
+    const int nsteps = 2 * b - 1;      // forward blocks 0..b-1, then backward blocks b-2..0
+    for (int r0 = 0; r0 < nrhs; r0 += KC) {
+        const int kc = min(KC, nrhs - r0);
+        auto issue = [&](int st) {
+            const int j = st < b ? st : 2 * b - 2 - st;
+            z* sd = sig + (st & 1) * AA;
+            for (int e = tid; e < AA; e += 256) cp_async16(sd + e, Sl + (size_t)j * AA + e, 16);
+            z* bd = blk + (st & 1) * A * KC;
+            for (int e = tid; e < A * KC; e += 256) {
+                const int q = e % A, rc = e / A, rh = r0 + rc;
+                const z* src = nullptr;
+                if (rc < kc) {
+                    if (st >= b) src = sol + ((size_t)rh * nleaves + leaf) * n + nb + j * A + q;
+                    else if (f) src = f + ((size_t)rh * nleaves + leaf) * ab + j * A + q;
+                }
+                cp_async16(bd + e, src ? src : Sl, src ? 16 : 0);
+            }
+        };
+        for (int e = tid; e < nb * KC; e += 256) {
+            const int r = e % nb, rc = e / nb;
+            const bool ok = rc < kc;
+            cp_async16(gsm + e, ok ? gb + ((size_t)leaf * nrhs + r0 + rc) * nb + r : gb, ok ? 16 : 0);
+        }
+        issue(0);
+        cp_async_commit();
+        z w[CPH];                      // this lane's entry of the running block vector per column
+#pragma unroll
+        for (int c = 0; c < CPH; ++c) w[c] = zmk(0.0, 0.0);
+        for (int st = 0; st < nsteps; ++st) {
+            cp_async_wait<0>();
+            __syncthreads();           // step st's blocks landed; every thread is past step st-1
+            if (st + 1 < nsteps) issue(st + 1);
+            cp_async_commit();
+            const z* S = sig + (st & 1) * AA;
+            z* B = blk + (st & 1) * A * KC;
+            if (st < b) {
+                // forward: w_j = Sig_j^-1 (t_j - Lo_j w_{j-1}),  t = f - A_ib A_bb^-1 g
+                const int j = st, jj = j + 1;
+                const z lam = jj > 1 ? block_lo(L, b, jj) : zmk(0.0, 0.0);
+#pragma unroll
+                for (int c = 0; c < CPH; ++c) {
+                    const int rc = warp * (2 * CPH) + half + 2 * c;
+                    const z* gl = gsm + rc * nb;
+                    z t = B[i + rc * A];
+                    if (i == 0) zfms(t, wdx, gl[j]);
+                    if (i == A - 1) zfms(t, wdx, gl[b + j]);
+                    if (jj == 1) zfms(t, wdy, gl[2 * b + i]);
+                    if (jj == b) zfms(t, wdy, gl[2 * b + A + i]);
+                    if (jj > 1) zfms(t, lam, w[c]);
+                    B[i + rc * A] = t;
+                }
+                __syncwarp();
+                z acc[CPH];
+#pragma unroll
+                for (int c = 0; c < CPH; ++c) acc[c] = zmk(0.0, 0.0);
+#pragma unroll
+                for (int q = 0; q < A; ++q) {
+                    const z sq = S[i + q * A];
+#pragma unroll
+                    for (int c = 0; c < CPH; ++c) zfma(acc[c], sq, B[q + (warp * (2 * CPH) + half + 2 * c) * A]);
+                }
+#pragma unroll
+                for (int c = 0; c < CPH; ++c) {
+                    const int rc = warp * (2 * CPH) + half + 2 * c;
+                    w[c] = acc[c];
+                    if (rc < kc) sol[((size_t)(r0 + rc) * nleaves + leaf) * n + nb + j * A + i] = acc[c];
+                }
+            } else {
+                // backward: x_{b-1} = w_{b-1}; x_j = w_j - Sig_j^-1 Up_j x_{j+1}
+                const int j = 2 * b - 2 - st;
+                const z mu = block_up(L, b, j + 1);
+                z wj[CPH];
+#pragma unroll
+                for (int c = 0; c < CPH; ++c) {
+                    const int rc = warp * (2 * CPH) + half + 2 * c;
+                    wj[c] = B[i + rc * A];
+                    B[i + rc * A] = w[c];          // x_{j+1}, read by the other lanes of the half
+                }
+                __syncwarp();
+#pragma unroll
+                for (int q = 0; q < A; ++q) {
+                    const z sq = S[i + q * A];
+#pragma unroll
+                    for (int c = 0; c < CPH; ++c)
+                        zfms(wj[c], sq, zmul(mu, B[q + (warp * (2 * CPH) + half + 2 * c) * A]));
+                }
+#pragma unroll
+                for (int c = 0; c < CPH; ++c) {
+                    const int rc = warp * (2 * CPH) + half + 2 * c;
+                    w[c] = wj[c];
+                    if (rc < kc) sol[((size_t)(r0 + rc) * nleaves + leaf) * n + nb + j * A + i] = wj[c];
+                }
+            }
+        }
+        cp_async_wait<0>();
+        __syncthreads();               // every interior value of the chunk is stored
+        // boundary values u_b = (g - c1 u(p1) - c2 u(p2)) / d
+        for (int e = tid; e < nb * kc; e += 256) {
+            const int r = e % nb, rc = e / nb, rh = r0 + rc;
+            int ax, p1, p2;
+            leaf_bpoint2(A, b, r, ax, p1, p2);
+            const double h = ax == 0 ? L.hx : L.hy;
+            z* u = sol + ((size_t)rh * nleaves + leaf) * n;
+            z v = gsm[rc * nb + r];
+            v = zsub(v, zadd(zscale(-3.0 / h, u[nb + p1]), zscale((1.0 / 3.0) / h, u[nb + p2])));
+            u[r] = zmul(v, ax == 0 ? L.rdx : L.rdy);
+        }
+        __syncthreads();               // the buffers are refilled for the next chunk
+    }
+}
+
 cudaError_t leaf_block_solve(const LeafGeom& g, int nleaves, int nrhs, const double* h, const z* f, const z* gb,
                              const z* sinv, z* sol, cudaStream_t s) {
+    if (g.a == 16 && leaf_solve_engine_hw()) {
+        const size_t sh = ((size_t)2 * 256 + 2 * 16 * LHW_KC + (size_t)g.nb * LHW_KC) * sizeof(z);
+        static size_t set = 0;
+        if (sh > set) {
+            cudaError_t e = cudaFuncSetAttribute(leaf_hw_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+            if (e != cudaSuccess) return e;
+            set = sh;
+        }
+        leaf_hw_solve_kernel<<<nleaves, 256, sh, s>>>(g, nleaves, nrhs, h, f, gb, sinv, sol);
+        note_launch();
+        return cudaGetLastError();
+    }
     const size_t sh = ((size_t)g.a * g.a + 2 * (size_t)g.a * LEAF_KC) * sizeof(z);
     if (sh > 48 * 1024) {
         cudaError_t e = cudaFuncSetAttribute(leaf_block_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
