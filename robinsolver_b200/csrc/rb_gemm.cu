@@ -105,6 +105,86 @@ static cudaError_t launch_dmma(const GemmBatch& b, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// A view of the same matrix whose column j is column j + kb of v (B: row j is row j + kb)
+__device__ __forceinline__ ZView view_from_col(ZView v, int kb) {
+    if (v.cmap) {
+        v.cmap += kb;
+    } else if (v.cs >= kb) {
+        v.p += (long long)kb * v.ld;
+        if (v.cs != INT_MAX) v.cs -= kb;
+    } else {
+        v.p += (long long)(kb + v.cl) * v.ld;
+        v.cs = INT_MAX;
+        v.cl = 0;
+    }
+    return v;
+}
+__device__ __forceinline__ ZView view_from_row(ZView v, int kb) {
+    if (v.rmap) {
+        v.rmap += kb;
+    } else if (v.rs >= kb) {
+        v.p += kb;
+        if (v.rs != INT_MAX) v.rs -= kb;
+    } else {
+        v.p += kb + v.rl;
+        v.rs = INT_MAX;
+        v.rl = 0;
+    }
+    return v;
+}
+
+// split-K pass on the tensor cores: blockIdx.z picks the k range [kb, kb + kchunk); the range's
+// raw product (3M-combined, alpha = 1, no C) goes to the batch's workspace, laid out as the DFMA
+// split pass writes it, for zgemm_reduce_kernel.  Every output element still sums its k range in
+// MMA k-steps of 4 in order, so the result does not depend on n or on the tile shape.
+template <int BM, int BN, int WM, int WN, int MINB>
+__global__ void __launch_bounds__(32 * WM * WN, MINB)
+zgemm_dmma_split_kernel(const GemmDesc* __restrict__ descs, int kchunk, z* work, long long pstride, int ldp, int ksplit) {
+    extern __shared__ z dmma_smem[];
+    __shared__ GemmDesc sd;
+    {
+        const unsigned long long* src = reinterpret_cast<const unsigned long long*>(descs + blockIdx.y);
+        unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sd);
+        for (int w = threadIdx.x; w < (int)(sizeof(GemmDesc) / 8); w += 32 * WM * WN) dst[w] = src[w];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int kb = blockIdx.z * kchunk;
+        sd.A = view_from_col(sd.A, kb);
+        sd.B = view_from_row(sd.B, kb);
+        sd.k = max(0, min(sd.k, kb + kchunk) - kb);
+        sd.C = zview(nullptr, 1);
+        sd.alpha = zmk(1.0, 0.0);
+        sd.D = zout(work + ((long long)blockIdx.y * ksplit + blockIdx.z) * pstride, ldp);
+    }
+    __syncthreads();
+    zgemm_tile_dmma<BM, BN, WM, WN>(sd, blockIdx.x, dmma_smem);
+}
+
+template <int BM, int BN, int WM, int WN, int MINB>
+static cudaError_t launch_dmma_split(const GemmBatch& b, cudaStream_t s) {
+    using Cfg = DmmaCfg<BM, BN, WM, WN>;
+    auto kern = zgemm_dmma_split_kernel<BM, BN, WM, WN, MINB>;
+    static bool attr = false;
+    if (!attr) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM_BYTES);
+        if (e != cudaSuccess) return e;
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    if (b.count > 65535 || b.ksplit > 65535) return cudaErrorInvalidValue;
+    const int tiles = ((b.max_m + BM - 1) / BM) * ((b.max_n + BN - 1) / BN);
+    kern<<<dim3(tiles, b.count, b.ksplit), Cfg::NT, Cfg::SMEM_BYTES, s>>>(b.d_desc, b.kchunk, b.work, b.pstride,
+                                                                        b.max_m, b.ksplit);
+    note_launch();
+    const long long elems = (long long)b.max_m * b.max_n;
+    zgemm_reduce_kernel<<<dim3((unsigned)((elems + 255) / 256), b.count), 256, 0, s>>>(b.d_desc, b.work, b.pstride,
+                                                                                     b.max_m, b.ksplit);
+    note_launch();
+    return cudaGetLastError();
+}
+
 template <int BM, int BN, int WM, int WN, int BK, int STAGES, int MINB>
 __global__ void __launch_bounds__(32 * WM * WN, MINB) zgemm_dmma_kc_kernel(const GemmDesc* __restrict__ descs) {
     extern __shared__ z dmma_smem[];
@@ -195,9 +275,12 @@ static cudaError_t launch_split(const GemmBatch& b, cudaStream_t s) {
 }
 
 // the kernel shape a batch runs on
-enum class GemmShape { Dfma16, Dfma32, Dmma32, Dmma64, DmmaKc64, Dfma128x64, Dfma64 };
+enum class GemmShape { Dfma16, Dfma32, Dmma32, Dmma64, DmmaKc64, DmmaFixed, Dfma128x64, Dfma64 };
 static GemmShape gemm_shape(const GemmBatch& b) {
     const int mm = b.max_m, nn = b.max_n;
+    // fixed-order batches (the solve) on the tensor cores: one tile shape, split-K planned from
+    // count, m and k only; an element's sum runs over k in MMA steps of 4 in order whatever n is
+    if (use_dmma() && b.fixed_order) return GemmShape::DmmaFixed;
     if (mm <= 16 && nn <= 16) return GemmShape::Dfma16;
     // FP64 tensor cores, small problems (both sides <= 192: the merges below 128x256 boxes):
     // 32x32 tiles of 4 warps, up to six CTAs per SM; measured 1.0-1.6x the 64x64 tile and
@@ -227,8 +310,9 @@ long long gemm_plan_split(GemmBatch& b) {
     b.ksplit = 1;
     b.kchunk = 0;
     b.pstride = 0;
-    // fixed-order batches always run on DFMA tiles, whose shapes share one summation order, so
-    // the split (and the rounding) depends on count, m and k only
+    // fixed-order batches run on tiles that share one summation order (the tensor-core tile, or
+    // with RB_GEMM_ENGINE=dfma the DFMA tiles), so the split (and the rounding) depends on count,
+    // m and k only
     if (!b.fixed_order || b.count == 0 || b.max_k < 128) return 0;
     // CTAs with one column tile (n-independent), against about four waves of two CTAs per SM
     const long long ctas = (long long)b.count * ((b.max_m + 15) / 16);
@@ -250,6 +334,7 @@ long long gemm_plan_split(GemmBatch& b) {
 
 const char* gemm_stage_name(const GemmBatch& b) {
     const GemmShape sh = gemm_shape(b);
+    if (sh == GemmShape::DmmaFixed) return "zgemm_tc_fixed";
     return (sh == GemmShape::Dmma64 || sh == GemmShape::Dmma32 || sh == GemmShape::DmmaKc64) ? "zgemm_tc" : "zgemm_dfma";
 }
 
@@ -257,6 +342,8 @@ cudaError_t launch_gemm_batch(const GemmBatch& b, cudaStream_t s) {
     static_assert(sizeof(GemmDesc) % 8 == 0, "descriptor copy assumes 8-byte words");
     if (b.count == 0 || b.max_m == 0 || b.max_n == 0) return cudaSuccess;
     const GemmShape shape = gemm_shape(b);
+    if (shape == GemmShape::DmmaFixed)
+        return (b.ksplit > 1 && b.work) ? launch_dmma_split<32, 32, 2, 2, 6>(b, s) : launch_dmma<32, 32, 2, 2, 6>(b, s);
     if (b.ksplit > 1 && b.work) {
         if (shape == GemmShape::Dfma16) return launch_split<16, 16, 2, 2, 8, 6, 8>(b, s);
         if (shape == GemmShape::Dfma32) return launch_split<32, 32, 4, 2, 8, 4, 4>(b, s);
@@ -266,7 +353,8 @@ cudaError_t launch_gemm_batch(const GemmBatch& b, cudaStream_t s) {
     switch (shape) {
         case GemmShape::Dfma16: return launch_cfg<16, 16, 2, 2, 8, 6, 8>(b, s);
         case GemmShape::Dfma32: return launch_cfg<32, 32, 4, 2, 8, 4, 4>(b, s);
-        case GemmShape::Dmma32: return launch_dmma<32, 32, 2, 2, 6>(b, s);
+        case GemmShape::Dmma32:
+        case GemmShape::DmmaFixed: return launch_dmma<32, 32, 2, 2, 6>(b, s);
         case GemmShape::Dmma64: return launch_dmma<64, 64, 2, 4, 2>(b, s);
         case GemmShape::DmmaKc64: return launch_dmma_kc<64, 64, 2, 2, 4, 8, 2>(b, s);
         case GemmShape::Dfma128x64: return launch_cfg<128, 64, 8, 4, 4, 4, 1>(b, s);

@@ -21,8 +21,11 @@
 // Solve (forward_sub / backward_sub, robin_tree_module.f90:813-1146), all RHS at once:
 //   forward:  leaf h = Y(:, nb:) f;  per level (g1_i, g2_i) = M^-1 (h1_i, h2_i) and the parent's
 //             h = h_N + T_Ni g_i
-//   backward: root g = boundary data; per level children's g_N from the parent, Tg = T_iN g_N,
-//             g_i += M^-1 Tg;  leaf u = A^-1 [g; f] through the leaf's block factors.
+//   backward: root g = boundary data; per level children's g_N from the parent, and
+//             g_i += M^-1 T_iN g_N: at the root as Tg = T_iN g_N, g_i += M^-1 Tg (its Y1, Y2 are
+//             formed after the solve reaches it), below as g_i += [Y1; Y2] g_N with the level's
+//             stored Y (one GEMM per level instead of four dependent ones);
+//             leaf u = A^-1 [g; f] through the leaf's block factors.
 //   M^-1 (x1, x2), K form: y1 = inv(K)(nu x2 - A2 x1), y2 = (x1 - A1 y1) / nu;  D/S form:
 //   w = inv(D) x2; y1 = inv(S)(x1 - nu w); y2 = w - nu inv(D) y1 (apply_invm, :1252).
 #include <algorithm>
@@ -120,10 +123,11 @@ struct rb_tree {
     bool kform = false;
     std::vector<z*> kinv;            // per level < L, K form only
     std::vector<int*> d_pmap1, d_pmap2;
+    std::vector<int*> d_pmapc;       // per level < L: pmap1 then pmap2 (the columns of Y1 and Y2)
     int* d_status = nullptr;
-    // factor workspace
-    z* Y1 = nullptr;
-    z* Y2 = nullptr;
+    // per level < L: [Y1; Y2] = M^-1 blockdiag(T1_iN, T2_iN), nnodes x m x (n1 + n2) each; the
+    // backward sweep below the root applies them to the node's incoming data
+    std::vector<z*> Y1, Y2;
     z* gj_work = nullptr;
     int* gj_ipiv = nullptr;
     // factor launch batches
@@ -140,7 +144,7 @@ struct rb_tree {
     z* tmp = nullptr;
     z* sol = nullptr;
     GemmBatch sL0;
-    std::vector<GemmBatch> sF12, sF3, sF4, sF5, sB1, sB23, sB4, sB5;
+    std::vector<GemmBatch> sF12, sF3, sF4, sF5, sB1, sB23, sB4, sB5, sBY;
     std::vector<DevBuf> solve_bufs;
 
     // timing: 0 off, 1 per stage, 2 per launch
@@ -399,7 +403,9 @@ static int ensure_factor_storage(rb_tree* t) {
     t->kinv.assign(L, nullptr);
     t->d_pmap1.assign(L, nullptr);
     t->d_pmap2.assign(L, nullptr);
-    size_t ymax = 0;
+    t->d_pmapc.assign(L, nullptr);
+    t->Y1.assign(L, nullptr);
+    t->Y2.assign(L, nullptr);
     for (int l = 0; l < L; ++l) {
         const PlanLevel& p = P.lv[l];
         if (!(l == 0 && t->skip_root))
@@ -412,10 +418,14 @@ static int ensure_factor_storage(rb_tree* t) {
         if ((rc = alloc_n(t, t->bufs, p.pmap2.size(), &t->d_pmap2[l]))) return rc;
         RB_CK(cudaMemcpy(t->d_pmap1[l], p.pmap1.data(), p.pmap1.size() * sizeof(int), cudaMemcpyHostToDevice));
         RB_CK(cudaMemcpy(t->d_pmap2[l], p.pmap2.data(), p.pmap2.size() * sizeof(int), cudaMemcpyHostToDevice));
-        ymax = std::max(ymax, (size_t)p.nnodes * p.m * (p.n1 + p.n2));
+        std::vector<int> pc(p.pmap1);
+        pc.insert(pc.end(), p.pmap2.begin(), p.pmap2.end());
+        if ((rc = alloc_n(t, t->bufs, pc.size(), &t->d_pmapc[l]))) return rc;
+        RB_CK(cudaMemcpy(t->d_pmapc[l], pc.data(), pc.size() * sizeof(int), cudaMemcpyHostToDevice));
+        const size_t ny = (size_t)p.nnodes * p.m * (p.n1 + p.n2);
+        if ((rc = alloc_n(t, t->bufs, ny, &t->Y1[l]))) return rc;
+        if ((rc = alloc_n(t, t->bufs, ny, &t->Y2[l]))) return rc;
     }
-    if ((rc = alloc_n(t, t->bufs, ymax, &t->Y1))) return rc;
-    if ((rc = alloc_n(t, t->bufs, ymax, &t->Y2))) return rc;
     // Gauss-Jordan workspace: the largest batch of one level's nodes
     size_t wmax = 1, imax = 1;
     for (int l = 0; l < L; ++l) {
@@ -462,8 +472,8 @@ static int ensure_factor_storage(rb_tree* t) {
             const long long ld = cs.ld;
             z* dv = t->dinv[l] + (long long)i * m * m;
             z* sv = t->sinv[l] + (long long)i * m * m;
-            z* y1 = t->Y1 + (long long)i * m * (n1 + n2);
-            z* y2 = t->Y2 + (long long)i * m * (n1 + n2);
+            z* y1 = t->Y1[l] + (long long)i * m * (n1 + n2);
+            z* y2 = t->Y2[l] + (long long)i * m * (n1 + n2);
             if (t->kform) {
                 // [Y1; Y2] = M^-1 blockdiag(T1_iN, T2_iN), M = [[A1, nu I], [nu I, A2]]:
                 //   Y1 = K^-1 [-A2 T1_iN, nu T2_iN],  Y2 = ([T1_iN, 0] - A1 Y1) / nu,  K = nu^2 I - A2 A1
@@ -653,7 +663,7 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
             if (l > 0)
                 if ((rc = alloc_n(t, t->solve_bufs, (size_t)p.nnodes * p.nb * k, &t->hbuf[l]))) return rc;
             if ((rc = alloc_n(t, t->solve_bufs, (size_t)p.nnodes * p.nb * k, &t->gbuf[l]))) return rc;
-            if (l < L) tmax = std::max(tmax, (size_t)p.nnodes * 4 * p.m * k);
+            if (l == 0 && L > 0) tmax = (size_t)p.nnodes * 4 * p.m * k;   // the root's backward step
         }
         if ((rc = alloc_n(t, t->solve_bufs, tmax, &t->tmp))) return rc;
         if ((rc = alloc_n(t, t->solve_bufs, (size_t)k * nl * n, &t->sol))) return rc;
@@ -674,12 +684,12 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
     if ((rc = upload_gemm(t, t->solve_bufs, v, t->sL0))) return rc;
     t->sF12.assign(L, GemmBatch()); t->sF3.assign(L, GemmBatch()); t->sF4.assign(L, GemmBatch());
     t->sF5.assign(L, GemmBatch()); t->sB1.assign(L, GemmBatch()); t->sB23.assign(L, GemmBatch());
-    t->sB4.assign(L, GemmBatch()); t->sB5.assign(L, GemmBatch());
+    t->sB4.assign(L, GemmBatch()); t->sB5.assign(L, GemmBatch()); t->sBY.assign(L, GemmBatch());
     for (int l = 0; l < L; ++l) {
         const PlanLevel& p = P.lv[l];
         const int m = p.m, n1 = p.n1, n2 = p.n2, o1 = p.o1, o2 = p.o2, nbc = p.nbc, nbp = p.nb;
         const ChildStore cs = child_store(t, l);
-        std::vector<GemmDesc> f12, f3, f4, f5, b1, b23, b4, b5;
+        std::vector<GemmDesc> f12, f3, f4, f5, b1, b23, b4, b5, by;
         for (int i = 0; i < p.nnodes; ++i) {
             const z* r1 = cs.rtr + (2LL * i) * cs.stride;
             const z* r2 = cs.rtr + (2LL * i + 1) * cs.stride;
@@ -729,7 +739,23 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
                 gb.C = band_view(h2, nbc, o2, m, INT_MAX, 0); gb.beta = one;
                 f5.push_back(ga); f5.push_back(gb);
             }
-            // backward: tmp = [tg1 | tg2 | y2 | y1]
+            if (l > 0) {
+                // backward below the root: the interface values are the forward's particular part
+                // (already in g1, g2 at the interface) plus [Y1; Y2] g_N, g_N = the node's incoming
+                // values at the children's outer points (pmap1, pmap2 into the node's face order)
+                ZView gn = zview(t->gbuf[l] + (long long)i * nbp * k, nbp);
+                gn.rmap = t->d_pmapc[l];
+                GemmDesc gy1 = gdesc(m, k, n1 + n2, zview(t->Y1[l] + (long long)i * m * (n1 + n2), m), gn,
+                                     zout(g1 + o1, nbc), one);
+                gy1.C = zview(g1 + o1, nbc); gy1.beta = one;
+                GemmDesc gy2 = gdesc(m, k, n1 + n2, zview(t->Y2[l] + (long long)i * m * (n1 + n2), m), gn,
+                                     zout(g2 + o2, nbc), one);
+                gy2.C = zview(g2 + o2, nbc); gy2.beta = one;
+                by.push_back(gy1); by.push_back(gy2);
+                continue;
+            }
+            // backward at the root (its Y1, Y2 are formed after the solve starts there):
+            // tmp = [tg1 | tg2 | y2 | y1]
             z* tb = t->tmp + (long long)i * 4 * m * k;
             z* tg1 = tb;
             z* tg2 = tb + (long long)m * k;
@@ -773,18 +799,19 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
         if ((rc = upload_gemm(t, t->solve_bufs, b23, t->sB23[l]))) return rc;
         if ((rc = upload_gemm(t, t->solve_bufs, b4, t->sB4[l]))) return rc;
         if ((rc = upload_gemm(t, t->solve_bufs, b5, t->sB5[l]))) return rc;
+        if ((rc = upload_gemm(t, t->solve_bufs, by, t->sBY[l]))) return rc;
     }
     t->sL0.fixed_order = true;
     for (int l = 0; l < L; ++l)
         for (GemmBatch* gb : {&t->sF12[l], &t->sF3[l], &t->sF4[l], &t->sF5[l], &t->sB1[l], &t->sB23[l], &t->sB4[l],
-                              &t->sB5[l]})
+                              &t->sB5[l], &t->sBY[l]})
             gb->fixed_order = true;
     // split-K for the long-k, few-CTA solve GEMMs; one workspace serves them all (one stream)
     {
         std::vector<GemmBatch*> all{&t->sL0};
         for (int l = 0; l < L; ++l)
             for (GemmBatch* gb : {&t->sF12[l], &t->sF3[l], &t->sF4[l], &t->sF5[l], &t->sB1[l], &t->sB23[l],
-                                  &t->sB4[l], &t->sB5[l]})
+                                  &t->sB4[l], &t->sB5[l], &t->sBY[l]})
                 all.push_back(gb);
         long long wmax = 0;
         for (GemmBatch* gb : all) wmax = std::max(wmax, gemm_plan_split(*gb));
@@ -823,6 +850,10 @@ static int run_solve(rb_tree* t, int k, cudaStream_t s, const std::vector<cudaEv
         const PlanLevel& p = P.lv[l];
         RB_TIMED("sweep_aux", 0.0, sweep_scatter_down(p.nnodes, k, p.nb, p.nbc, p.m, p.o1, p.o2, p.n1, p.n2, t->d_pmap1[l],
                                      t->d_pmap2[l], t->gbuf[l], t->gbuf[l + 1], s));
+        if (l > 0) {
+            RB_GEMM(t->sBY[l], s);
+            continue;
+        }
         RB_GEMM(t->sB1[l], s);
         RB_GEMM(t->sB23[l], s);
         RB_GEMM(t->sB4[l], s);
@@ -893,7 +924,8 @@ int rb_tree_create(const rb_geom* geom, rb_tree** out) {
         double need = (double)Q.nleaves() * (ab * Q.leaf_a() + (double)Q.leaf_nb() * Q.leaf_n() + ab) * 16.0;
         for (int l = 0; l < Q.L; ++l)
             need += (double)Q.lv[l].nnodes *
-                    ((double)Q.lv[l].nb * Q.lv[l].nb + (t->kform ? 3.0 : 2.0) * Q.lv[l].m * Q.lv[l].m) * 16.0;
+                    ((double)Q.lv[l].nb * Q.lv[l].nb + (t->kform ? 3.0 : 2.0) * Q.lv[l].m * Q.lv[l].m +
+                     2.0 * Q.lv[l].m * (Q.lv[l].n1 + Q.lv[l].n2)) * 16.0;
         if (need > (double)t->budget) {
             g_create_error = "device budget exceeded: the factorization needs at least " +
                              std::to_string((long long)need) + " bytes, budget " + std::to_string(t->budget);
@@ -1439,6 +1471,11 @@ static std::vector<std::pair<z*, size_t>> factor_sections(rb_tree* t) {
         v.push_back({t->dinv[l], mm});
         v.push_back({t->sinv[l], mm});
         if (t->kform) v.push_back({t->kinv[l], mm});
+        if (l > 0) {
+            const size_t ny = (size_t)p.nnodes * p.m * (p.n1 + p.n2);
+            v.push_back({t->Y1[l], ny});
+            v.push_back({t->Y2[l], ny});
+        }
     }
     return v;
 }
@@ -1452,6 +1489,8 @@ struct SaveHeader {
     int32_t nsections;
 };
 static const char kMagic[8] = {'R', 'B', 'T', 'R', 'E', 'E', 'F', '1'};
+// 2: [Y1; Y2] of every level below the root follow each level's inverses
+static const uint32_t kSaveVersion = 2;
 
 int rb_tree_save(const rb_tree* tc, const char* path) {
     rb_tree* t = const_cast<rb_tree*>(tc);
@@ -1463,7 +1502,7 @@ int rb_tree_save(const rb_tree* tc, const char* path) {
     const auto secs = factor_sections(t);
     SaveHeader h{};
     std::memcpy(h.magic, kMagic, 8);
-    h.version = 1;
+    h.version = kSaveVersion;
     h.geom_bytes = sizeof(rb_geom);
     h.geom = t->geom;
     h.kform = t->kform ? 1 : 0;
@@ -1498,7 +1537,7 @@ int rb_tree_load(const char* path, rb_tree** out) {
         return RB_ERR_INVALID;
     }
     SaveHeader h{};
-    if (std::fread(&h, sizeof(h), 1, fp) != 1 || std::memcmp(h.magic, kMagic, 8) != 0 || h.version != 1 ||
+    if (std::fread(&h, sizeof(h), 1, fp) != 1 || std::memcmp(h.magic, kMagic, 8) != 0 || h.version != kSaveVersion ||
         h.geom_bytes != sizeof(rb_geom)) {
         std::fclose(fp);
         g_create_error = std::string("rb_tree_load: ") + path + " is not a factorized tree of this library";
