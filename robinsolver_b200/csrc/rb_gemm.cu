@@ -334,8 +334,11 @@ long long gemm_plan_split(GemmBatch& b) {
 
 const char* gemm_stage_name(const GemmBatch& b) {
     const GemmShape sh = gemm_shape(b);
+    // zgemm_tc: the contiguous-k tile (the large merge GEMMs); zgemm_tc_small: the other
+    // tensor-core factor tiles; zgemm_tc_fixed: the solve's
     if (sh == GemmShape::DmmaFixed) return "zgemm_tc_fixed";
-    return (sh == GemmShape::Dmma64 || sh == GemmShape::Dmma32 || sh == GemmShape::DmmaKc64) ? "zgemm_tc" : "zgemm_dfma";
+    if (sh == GemmShape::DmmaKc64) return "zgemm_tc";
+    return (sh == GemmShape::Dmma64 || sh == GemmShape::Dmma32) ? "zgemm_tc_small" : "zgemm_dfma";
 }
 
 cudaError_t launch_gemm_batch(const GemmBatch& b, cudaStream_t s) {

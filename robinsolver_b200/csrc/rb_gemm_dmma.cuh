@@ -47,15 +47,15 @@ __device__ __forceinline__ void dmma_store(const GemmDesc& sd, const double (&p1
     const z alpha = sd.alpha, beta = sd.beta;
     const ZView C = sd.C;
     const ZOut D = sd.D;
-    long long dcol[TNW][2], ccol[TNW][2];
+    int dcol[TNW][2], ccol[TNW][2];      // output / C column indices; -1: beyond n
 #pragma unroll
     for (int j = 0; j < TNW; ++j)
 #pragma unroll
         for (int h = 0; h < 2; ++h) {
             const int gj = c0 + j * 8 + 2 * lc + h;
             const bool ok = gj < n;
-            dcol[j][h] = ok ? (long long)vcol(D, gj) * D.ld : -1;
-            ccol[j][h] = ok && C.p ? (long long)vcol(C, gj) * C.ld : 0;
+            dcol[j][h] = ok ? vcol(D, gj) : -1;
+            ccol[j][h] = ok && C.p ? vcol(C, gj) : 0;
         }
 #pragma unroll
     for (int i = 0; i < TMW; ++i) {
@@ -68,7 +68,8 @@ __device__ __forceinline__ void dmma_store(const GemmDesc& sd, const double (&p1
 #pragma unroll
         for (int j = 0; j < TNW; ++j)
 #pragma unroll
-            for (int h = 0; h < 2; ++h) c[j][h] = (use_c && dcol[j][h] >= 0) ? C.p[crow + ccol[j][h]] : zmk(0.0, 0.0);
+            for (int h = 0; h < 2; ++h)
+                c[j][h] = (use_c && dcol[j][h] >= 0) ? C.p[crow + (long long)ccol[j][h] * C.ld] : zmk(0.0, 0.0);
 #pragma unroll
         for (int j = 0; j < TNW; ++j)
 #pragma unroll
@@ -78,7 +79,7 @@ __device__ __forceinline__ void dmma_store(const GemmDesc& sd, const double (&p1
                 const double im = p3[i][j][h] - p1[i][j][h] - p2[i][j][h];
                 z v = zmul(alpha, zmk(re, im));
                 if (use_c) zfma(v, beta, c[j][h]);
-                D.p[drow + dcol[j][h]] = v;
+                D.p[drow + (long long)dcol[j][h] * D.ld] = v;
             }
     }
 }
