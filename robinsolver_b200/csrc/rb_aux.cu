@@ -94,28 +94,4 @@ cudaError_t sweep_scatter_down(int nnodes, int nrhs, int nbp, int nbc, int m, in
     return cudaGetLastError();
 }
 
-// g_i += M^-1 (Tg): tmp per node = [tg1 | tg2 | y2 | y1], each m x nrhs (ld m)
-__global__ void sweep_add_interface_kernel(int nrhs, int nbc, int m, int o1, int o2, const z* __restrict__ tmp,
-                                           z* __restrict__ gchild) {
-    const int node = blockIdx.y;
-    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= m * nrhs) return;
-    const int r = idx % m, rh = idx / m;
-    const z* tb = tmp + (long long)node * 4 * m * nrhs;
-    const z y2 = tb[2LL * m * nrhs + idx];
-    const z y1 = tb[3LL * m * nrhs + idx];
-    z* g1 = gchild + ((long long)(2 * node) * nrhs + rh) * nbc + o1 + r;
-    z* g2 = gchild + ((long long)(2 * node + 1) * nrhs + rh) * nbc + o2 + r;
-    *g1 = zadd(*g1, y1);
-    *g2 = zadd(*g2, y2);
-}
-
-cudaError_t sweep_add_interface(int nnodes, int nrhs, int nbc, int m, int o1, int o2, const z* tmp, z* gchild,
-                                cudaStream_t s) {
-    dim3 grid((m * nrhs + 255) / 256, nnodes);
-    sweep_add_interface_kernel<<<grid, 256, 0, s>>>(nrhs, nbc, m, o1, o2, tmp, gchild);
-    note_launch();
-    return cudaGetLastError();
-}
-
 }  // namespace rb

@@ -80,8 +80,5 @@ cudaError_t check_solution(const z* u, const z* ue, int nleaves, int n, int norm
 cudaError_t sweep_scatter_down(int nnodes, int nrhs, int nbp, int nbc, int m, int o1, int o2, int n1,
                                int n2, const int* pmap1, const int* pmap2, const z* gpar, z* gchild,
                                cudaStream_t s);
-// g_i^(1) += y1, g_i^(2) += y2 (tmp holds per node [tg1 | tg2 | y2 | y1], each m x nrhs).
-cudaError_t sweep_add_interface(int nnodes, int nrhs, int nbc, int m, int o1, int o2, const z* tmp,
-                                z* gchild, cudaStream_t s);
 
 }  // namespace rb

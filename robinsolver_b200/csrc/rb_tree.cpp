@@ -21,11 +21,12 @@
 // Solve (forward_sub / backward_sub, robin_tree_module.f90:813-1146), all RHS at once:
 //   forward:  leaf h = Y(:, nb:) f;  per level (g1_i, g2_i) = M^-1 (h1_i, h2_i) and the parent's
 //             h = h_N + T_Ni g_i
-//   backward: root g = boundary data; per level children's g_N from the parent, and
-//             g_i += M^-1 T_iN g_N: at the root as Tg = T_iN g_N, g_i += M^-1 Tg (its Y1, Y2 are
-//             formed after the solve reaches it), below as g_i += [Y1; Y2] g_N with the level's
-//             stored Y (one GEMM per level instead of four dependent ones);
-//             leaf u = A^-1 [g; f] through the leaf's block factors.
+//   root:     its forward and backward steps are one, g_i = M^-1 (h_i + T_iN g_N) with g_N the
+//             boundary data; x = h + T_iN g_N (and in the K form nu x2 - A2 x1) runs before the
+//             root's inverse is ready
+//   backward: per level below the root, the children's g_N from the parent and
+//             g_i += M^-1 T_iN g_N = [Y1; Y2] g_N with the level's stored Y (one GEMM per level
+//             instead of four dependent ones); leaf u = A^-1 [g; f] through the leaf's block factors.
 //   M^-1 (x1, x2), K form: y1 = inv(K)(nu x2 - A2 x1), y2 = (x1 - A1 y1) / nu;  D/S form:
 //   w = inv(D) x2; y1 = inv(S)(x1 - nu w); y2 = w - nu inv(D) y1 (apply_invm, :1252).
 #include <algorithm>
@@ -95,6 +96,7 @@ struct rb_tree {
     std::vector<cudaEvent_t> ev_fork, ev_join;
     // factor progress for a solve that overlaps it: [l] after level l's inversion, [L] after the leaves
     std::vector<cudaEvent_t> ev_lvl;
+    cudaEvent_t ev_root_forms = nullptr; // the root's A2 (D) is formed, after level 1's maps
     bool factor_deferred = false;        // RB_FLAG_ASYNC_FACTOR: potential copied, factor not launched
     // device-side sampling and check_solution: rb_tree_sample_points' points, cached on first use
     double* d_pts[3] = {nullptr, nullptr, nullptr};     // potential, source, boundary
@@ -144,7 +146,8 @@ struct rb_tree {
     z* tmp = nullptr;
     z* sol = nullptr;
     GemmBatch sL0;
-    std::vector<GemmBatch> sF12, sF3, sF4, sF5, sB1, sB23, sB4, sB5, sBY;
+    std::vector<GemmBatch> sF12, sF3, sF4, sF5, sBY;
+    GemmBatch sR1;                   // root: x_i = h_i + T_iN g_N (no K^-1 needed)
     std::vector<DevBuf> solve_bufs;
 
     // timing: 0 off, 1 per stage, 2 per launch
@@ -387,6 +390,7 @@ static int ensure_factor_storage(rb_tree* t) {
     t->ev_join.assign(L, nullptr);
     t->ev_lvl.assign(L + 1, nullptr);
     for (int l = 0; l <= L; ++l) RB_CK(cudaEventCreateWithFlags(&t->ev_lvl[l], cudaEventDisableTiming));
+    if (!t->ev_root_forms) RB_CK(cudaEventCreateWithFlags(&t->ev_root_forms, cudaEventDisableTiming));
     for (int l = 0; l < L; ++l) {
         RB_CK(cudaEventCreateWithFlags(&t->ev_fork[l], cudaEventDisableTiming));
         RB_CK(cudaEventCreateWithFlags(&t->ev_join[l], cudaEventDisableTiming));
@@ -600,6 +604,7 @@ static int run_factor(rb_tree* t, const z* dk, const std::vector<cudaEvent_t>* r
             // A2 = zeta I - T2_ii, A1 = zeta I - T1_ii; B1 = -A2 T1_iN on the second stream beside
             // K = nu^2 I - A2 A1 and its inversion
             RB_TIMED("merge_form", 0.0, merge_form_d(cs, p.nnodes, p.m, p.o2, t->zeta, t->dinv[l], s));
+            if (rec && l == 0) RB_CK(cudaEventRecord(t->ev_root_forms, s));
             RB_TIMED("merge_form", 0.0, merge_form_s(cs, p.nnodes, p.m, p.o1, t->zeta, zmk(0.0, 0.0), t->dinv[l],
                                                      t->sinv[l], s));
             const bool fork = t->timing == 0;
@@ -619,6 +624,7 @@ static int run_factor(rb_tree* t, const z* dk, const std::vector<cudaEvent_t>* r
             if (l == 0 && before_root_tail && (rc = (*before_root_tail)())) return rc;
         } else {
             RB_TIMED("merge_form", 0.0, merge_form_d(cs, p.nnodes, p.m, p.o2, t->zeta, t->dinv[l], s));
+            if (rec && l == 0) RB_CK(cudaEventRecord(t->ev_root_forms, s));
             RB_TIMED("gj_invert", gj_flops(p.m, p.nnodes), gj_invert_batch(t->gj_d[l].d_desc, p.nnodes, p.m, t->gj_work, t->d_status, s));
             // Y2R = inv(D) T2_iN needs only inv(D): on the second stream it overlaps the S inversion
             const bool fork = t->timing == 0;
@@ -663,7 +669,7 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
             if (l > 0)
                 if ((rc = alloc_n(t, t->solve_bufs, (size_t)p.nnodes * p.nb * k, &t->hbuf[l]))) return rc;
             if ((rc = alloc_n(t, t->solve_bufs, (size_t)p.nnodes * p.nb * k, &t->gbuf[l]))) return rc;
-            if (l == 0 && L > 0) tmax = (size_t)p.nnodes * 4 * p.m * k;   // the root's backward step
+            if (l == 0 && L > 0) tmax = (size_t)p.nnodes * 2 * p.m * k;   // the root's x1, x2
         }
         if ((rc = alloc_n(t, t->solve_bufs, tmax, &t->tmp))) return rc;
         if ((rc = alloc_n(t, t->solve_bufs, (size_t)k * nl * n, &t->sol))) return rc;
@@ -683,13 +689,13 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
                           zout(t->hbuf[L] + (long long)i * nb * k, nb), one));
     if ((rc = upload_gemm(t, t->solve_bufs, v, t->sL0))) return rc;
     t->sF12.assign(L, GemmBatch()); t->sF3.assign(L, GemmBatch()); t->sF4.assign(L, GemmBatch());
-    t->sF5.assign(L, GemmBatch()); t->sB1.assign(L, GemmBatch()); t->sB23.assign(L, GemmBatch());
-    t->sB4.assign(L, GemmBatch()); t->sB5.assign(L, GemmBatch()); t->sBY.assign(L, GemmBatch());
+    t->sF5.assign(L, GemmBatch()); t->sBY.assign(L, GemmBatch());
+    t->sR1 = GemmBatch();
     for (int l = 0; l < L; ++l) {
         const PlanLevel& p = P.lv[l];
         const int m = p.m, n1 = p.n1, n2 = p.n2, o1 = p.o1, o2 = p.o2, nbc = p.nbc, nbp = p.nb;
         const ChildStore cs = child_store(t, l);
-        std::vector<GemmDesc> f12, f3, f4, f5, b1, b23, b4, b5, by;
+        std::vector<GemmDesc> f12, f3, f4, f5, by, rx;
         for (int i = 0; i < p.nnodes; ++i) {
             const z* r1 = cs.rtr + (2LL * i) * cs.stride;
             const z* r2 = cs.rtr + (2LL * i + 1) * cs.stride;
@@ -700,21 +706,36 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
             z* h2 = t->hbuf[l + 1] + (2LL * i + 1) * nbc * k;
             z* g1 = t->gbuf[l + 1] + (2LL * i) * nbc * k;
             z* g2 = t->gbuf[l + 1] + (2LL * i + 1) * nbc * k;
+            // the root's forward and backward steps are one: (g1, g2) = M^-1 (x1, x2) with
+            // x_i = h_i + T_iN g_N (the root's g_N is the boundary data), x in tmp
+            const bool root = l == 0;
+            z* tb = root ? t->tmp + (long long)i * 2 * m * k : nullptr;
+            const ZView x1 = root ? zview(tb, m) : zview(h1 + o1, nbc);
+            const ZView x2 = root ? zview(tb + (long long)m * k, m) : zview(h2 + o2, nbc);
+            if (root) {
+                GemmDesc gx1 = gdesc(m, k, n1, band_view(r1 + o1, ld, INT_MAX, 0, o1, m),
+                                     band_view(g1, nbc, o1, m, INT_MAX, 0), zout(tb, m), one);
+                gx1.C = zview(h1 + o1, nbc); gx1.beta = one;
+                GemmDesc gx2 = gdesc(m, k, n2, band_view(r2 + o2, ld, INT_MAX, 0, o2, m),
+                                     band_view(g2, nbc, o2, m, INT_MAX, 0), zout(tb + (long long)m * k, m), one);
+                gx2.C = zview(h2 + o2, nbc); gx2.beta = one;
+                rx.push_back(gx1); rx.push_back(gx2);
+            }
             if (t->kform) {
-                // forward (g1, g2) = M^-1 (h1, h2): t = nu h2 - A2 h1 (in g2), g1 = K^-1 t,
-                // g2 = (h1 - A1 g1) / nu
+                // (g1, g2) = M^-1 (x1, x2): t = nu x2 - A2 x1 (in g2), g1 = K^-1 t,
+                // g2 = (x1 - A1 g1) / nu
                 z* kv = t->kinv[l] + (long long)i * m * m;
-                GemmDesc gt = gdesc(m, k, m, zview(dv, m), zview(h1 + o1, nbc), zout(g2 + o2, nbc), mone);
-                gt.C = zview(h2 + o2, nbc); gt.beta = t->nu;
+                GemmDesc gt = gdesc(m, k, m, zview(dv, m), x1, zout(g2 + o2, nbc), mone);
+                gt.C = x2; gt.beta = t->nu;
                 f12.push_back(gt);
                 f3.push_back(gdesc(m, k, m, zview(kv, m), zview(g2 + o2, nbc), zout(g1 + o1, nbc), one));
                 GemmDesc g2d = gdesc(m, k, m, zview(sv, m), zview(g1 + o1, nbc), zout(g2 + o2, nbc), mrnu);
-                g2d.C = zview(h1 + o1, nbc); g2d.beta = rnu;
+                g2d.C = x1; g2d.beta = rnu;
                 f4.push_back(g2d);
             } else {
-                // forward: g2_i = inv(D) h2_i ; g1_i = inv(S) h1_i
-                f12.push_back(gdesc(m, k, m, zview(dv, m), zview(h2 + o2, nbc), zout(g2 + o2, nbc), one));
-                f12.push_back(gdesc(m, k, m, zview(sv, m), zview(h1 + o1, nbc), zout(g1 + o1, nbc), one));
+                // g2 = inv(D) x2 ; g1 = inv(S) x1
+                f12.push_back(gdesc(m, k, m, zview(dv, m), x2, zout(g2 + o2, nbc), one));
+                f12.push_back(gdesc(m, k, m, zview(sv, m), x1, zout(g1 + o1, nbc), one));
                 {   // g1_i -= nu inv(S) g2_i
                     GemmDesc g = gdesc(m, k, m, zview(sv, m), zview(g2 + o2, nbc), zout(g1 + o1, nbc), mnu);
                     g.C = zview(g1 + o1, nbc); g.beta = one;
@@ -752,67 +773,24 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
                                      zout(g2 + o2, nbc), one);
                 gy2.C = zview(g2 + o2, nbc); gy2.beta = one;
                 by.push_back(gy1); by.push_back(gy2);
-                continue;
-            }
-            // backward at the root (its Y1, Y2 are formed after the solve starts there):
-            // tmp = [tg1 | tg2 | y2 | y1]
-            z* tb = t->tmp + (long long)i * 4 * m * k;
-            z* tg1 = tb;
-            z* tg2 = tb + (long long)m * k;
-            z* w = tb + 2LL * m * k;
-            z* y1 = tb + 3LL * m * k;
-            b1.push_back(gdesc(m, k, n1, band_view(r1 + o1, ld, INT_MAX, 0, o1, m),
-                               band_view(g1, nbc, o1, m, INT_MAX, 0), zout(tg1, m), one));
-            b1.push_back(gdesc(m, k, n2, band_view(r2 + o2, ld, INT_MAX, 0, o2, m),
-                               band_view(g2, nbc, o2, m, INT_MAX, 0), zout(tg2, m), one));
-            if (t->kform) {
-                // backward (y1, w) = M^-1 (tg1, tg2): t = nu tg2 - A2 tg1 (in w), y1 = K^-1 t,
-                // w = (tg1 - A1 y1) / nu
-                z* kv = t->kinv[l] + (long long)i * m * m;
-                GemmDesc gt = gdesc(m, k, m, zview(dv, m), zview(tg1, m), zout(w, m), mone);
-                gt.C = zview(tg2, m); gt.beta = t->nu;
-                b23.push_back(gt);
-                b4.push_back(gdesc(m, k, m, zview(kv, m), zview(w, m), zout(y1, m), one));
-                GemmDesc gw = gdesc(m, k, m, zview(sv, m), zview(y1, m), zout(w, m), mrnu);
-                gw.C = zview(tg1, m); gw.beta = rnu;
-                b5.push_back(gw);
-            } else {
-                b23.push_back(gdesc(m, k, m, zview(dv, m), zview(tg2, m), zout(w, m), one));
-                b23.push_back(gdesc(m, k, m, zview(sv, m), zview(tg1, m), zout(y1, m), one));
-                {
-                    GemmDesc g = gdesc(m, k, m, zview(sv, m), zview(w, m), zout(y1, m), mnu);
-                    g.C = zview(y1, m); g.beta = one;
-                    b4.push_back(g);
-                }
-                {
-                    GemmDesc g = gdesc(m, k, m, zview(dv, m), zview(y1, m), zout(w, m), mnu);
-                    g.C = zview(w, m); g.beta = one;
-                    b5.push_back(g);
-                }
             }
         }
         if ((rc = upload_gemm(t, t->solve_bufs, f12, t->sF12[l]))) return rc;
         if ((rc = upload_gemm(t, t->solve_bufs, f3, t->sF3[l]))) return rc;
         if ((rc = upload_gemm(t, t->solve_bufs, f4, t->sF4[l]))) return rc;
         if ((rc = upload_gemm(t, t->solve_bufs, f5, t->sF5[l]))) return rc;
-        if ((rc = upload_gemm(t, t->solve_bufs, b1, t->sB1[l]))) return rc;
-        if ((rc = upload_gemm(t, t->solve_bufs, b23, t->sB23[l]))) return rc;
-        if ((rc = upload_gemm(t, t->solve_bufs, b4, t->sB4[l]))) return rc;
-        if ((rc = upload_gemm(t, t->solve_bufs, b5, t->sB5[l]))) return rc;
         if ((rc = upload_gemm(t, t->solve_bufs, by, t->sBY[l]))) return rc;
+        if (l == 0 && (rc = upload_gemm(t, t->solve_bufs, rx, t->sR1))) return rc;
     }
     t->sL0.fixed_order = true;
+    t->sR1.fixed_order = true;
     for (int l = 0; l < L; ++l)
-        for (GemmBatch* gb : {&t->sF12[l], &t->sF3[l], &t->sF4[l], &t->sF5[l], &t->sB1[l], &t->sB23[l], &t->sB4[l],
-                              &t->sB5[l], &t->sBY[l]})
-            gb->fixed_order = true;
+        for (GemmBatch* gb : {&t->sF12[l], &t->sF3[l], &t->sF4[l], &t->sF5[l], &t->sBY[l]}) gb->fixed_order = true;
     // split-K for the long-k, few-CTA solve GEMMs; one workspace serves them all (one stream)
     {
-        std::vector<GemmBatch*> all{&t->sL0};
+        std::vector<GemmBatch*> all{&t->sL0, &t->sR1};
         for (int l = 0; l < L; ++l)
-            for (GemmBatch* gb : {&t->sF12[l], &t->sF3[l], &t->sF4[l], &t->sF5[l], &t->sB1[l], &t->sB23[l],
-                                  &t->sB4[l], &t->sB5[l], &t->sBY[l]})
-                all.push_back(gb);
+            for (GemmBatch* gb : {&t->sF12[l], &t->sF3[l], &t->sF4[l], &t->sF5[l], &t->sBY[l]}) all.push_back(gb);
         long long wmax = 0;
         for (GemmBatch* gb : all) wmax = std::max(wmax, gemm_plan_split(*gb));
         if (wmax > 0) {
@@ -837,28 +815,34 @@ static int run_solve(rb_tree* t, int k, cudaStream_t s, const std::vector<cudaEv
     if ((rc = timer_begin(t, "forward"))) return rc;
     if (wait) RB_CK(cudaStreamWaitEvent(s, (*wait)[L], 0));
     RB_GEMM(t->sL0, s);
-    for (int l = L - 1; l >= 0; --l) {
+    for (int l = L - 1; l >= 1; --l) {
         if (wait) RB_CK(cudaStreamWaitEvent(s, (*wait)[l], 0));
         RB_GEMM(t->sF12[l], s);
         RB_GEMM(t->sF3[l], s);
         RB_GEMM(t->sF4[l], s);
-        if (l > 0) RB_GEMM(t->sF5[l], s);
+        RB_GEMM(t->sF5[l], s);
+    }
+    // the root: x = h + T_iN g_N needs level 1's maps (and the K form's first product, A2), not
+    // the root's inverse, so it runs as soon as the root's A2 is formed
+    if (L > 0) {
+        const PlanLevel& p = P.lv[0];
+        if (wait) RB_CK(cudaStreamWaitEvent(s, t->ev_root_forms, 0));
+        RB_TIMED("sweep_aux", 0.0, sweep_scatter_down(p.nnodes, k, p.nb, p.nbc, p.m, p.o1, p.o2, p.n1, p.n2,
+                                                      t->d_pmap1[0], t->d_pmap2[0], t->gbuf[0], t->gbuf[1], s));
+        RB_GEMM(t->sR1, s);
+        if (t->kform) RB_GEMM(t->sF12[0], s);
+        if (wait) RB_CK(cudaStreamWaitEvent(s, (*wait)[0], 0));
+        if (!t->kform) RB_GEMM(t->sF12[0], s);
+        RB_GEMM(t->sF3[0], s);
+        RB_GEMM(t->sF4[0], s);
     }
     if ((rc = timer_end(t))) return rc;
     if ((rc = timer_begin(t, "backward"))) return rc;
-    for (int l = 0; l < L; ++l) {
+    for (int l = 1; l < L; ++l) {
         const PlanLevel& p = P.lv[l];
         RB_TIMED("sweep_aux", 0.0, sweep_scatter_down(p.nnodes, k, p.nb, p.nbc, p.m, p.o1, p.o2, p.n1, p.n2, t->d_pmap1[l],
                                      t->d_pmap2[l], t->gbuf[l], t->gbuf[l + 1], s));
-        if (l > 0) {
-            RB_GEMM(t->sBY[l], s);
-            continue;
-        }
-        RB_GEMM(t->sB1[l], s);
-        RB_GEMM(t->sB23[l], s);
-        RB_GEMM(t->sB4[l], s);
-        RB_GEMM(t->sB5[l], s);
-        RB_TIMED("sweep_aux", 0.0, sweep_add_interface(p.nnodes, k, p.nbc, p.m, p.o1, p.o2, t->tmp, t->gbuf[l + 1], s));
+        RB_GEMM(t->sBY[l], s);
     }
     if ((rc = timer_end(t))) return rc;
     if ((rc = timer_begin(t, "leaf_recover"))) return rc;
@@ -952,6 +936,7 @@ int rb_tree_destroy(rb_tree* t) {
     for (auto& e : t->ev_fork) if (e) cudaEventDestroy(e);
     for (auto& e : t->ev_join) if (e) cudaEventDestroy(e);
     for (auto& e : t->ev_lvl) if (e) cudaEventDestroy(e);
+    if (t->ev_root_forms) cudaEventDestroy(t->ev_root_forms);
     if (t->stream3) cudaStreamSynchronize(t->stream3);
     if (t->ev_copy) cudaEventDestroy(t->ev_copy);
     if (t->h_status) cudaFreeHost(t->h_status);
