@@ -232,8 +232,7 @@ int rb_check_solution_device(const rb_tree* tree, int irhs, const double* d_u_ex
 
 /* Writes the factorized tree (its rb_geom and every array the solve reads: leaf factors, level
  * RtR maps, interface inverses and the levels' [Y1; Y2]) to `path`, and rebuilds a handle from
- * such a file, ready to
- * solve, without factoring again.  No counterpart in the reference (its write_variable is a
+ * such a file, ready to solve, without factoring again.  No counterpart in the reference (its write_variable is a
  * stub, robin_output_module.f90:157-221).  The file holds raw complex128 arrays of this
  * library's layout; rb_tree_load refuses files of another version, tree or interface form. */
 int rb_tree_save(const rb_tree* tree, const char* path);
