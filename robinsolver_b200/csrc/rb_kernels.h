@@ -16,7 +16,9 @@ cudaError_t launch_gemm_batch(const GemmBatch& b, cudaStream_t s);
 // Chooses split-K for a fixed-order batch (sets ksplit, kchunk, pstride) and returns the
 // workspace it needs in complex elements (0: no split); the caller sets b.work.
 long long gemm_plan_split(GemmBatch& b);
-// stage-timer name of the engine a batch runs on: "zgemm_tc" (FP64 tensor cores) or "zgemm_dfma"
+// stage-timer name of the kernel a batch runs on: "zgemm_tc" (the contiguous-k tensor-core tile
+// of the large merges), "zgemm_tc_small" (the other tensor-core factor tiles), "zgemm_tc_fixed"
+// (the solve's fixed-order tensor-core tile) or "zgemm_dfma" (DFMA register tiles)
 const char* gemm_stage_name(const GemmBatch& b);
 
 // ---- batched Gauss-Jordan inversion (in place, partial pivoting by |re|+|im|) ----------------------
