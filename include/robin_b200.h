@@ -69,7 +69,11 @@ extern "C" {
                                      (rb_tree_solve, rb_get_solution, rb_tree_get_rtr,
                                      rb_tree_times, another factor) waits for it and reports its
                                      errors (RB_ERR_NUMERIC).  Host right-hand sides of
-                                     rb_tree_solve are then copied while the factor runs.        */
+                                     rb_tree_solve are then copied while the factor runs, and
+                                     rb_tree_solve returns once the solution is complete: the
+                                     root's own RtR map, which no solve reads, may still be
+                                     computed behind it (rb_tree_get_rtr and the next factor
+                                     wait for it).                                              */
 #define RB_FLAG_MERGE_DS      8   /* interface solve as the reference writes it, inv(D) and inv(S)
                                      (compute_RTR, robin_tree_module.f90:449-470), instead of the
                                      default single inversion of K = nu^2 I - (zeta I - T2_ii)(zeta I -
