@@ -151,6 +151,20 @@ def test_load_refuses_missing_and_foreign_files(tmp_path):
     assert "not a factorized tree" in _lib.last_error(None)
 
 
+def test_load_refuses_another_file_version(tmp_path):
+    """A file of this library's magic but another format version (version 1 lacked the levels'
+    [Y1; Y2]) is refused from its header, before any device work."""
+    import ctypes
+    import struct
+    from robinsolver_b200 import _lib
+    old = tmp_path / "v1.rbt"
+    old.write_bytes(b"RBTREEF1" + struct.pack("<II", 1, ctypes.sizeof(_lib.rb_geom)) + bytes(1024))
+    h = ctypes.c_void_p()
+    assert _lib.lib.rb_tree_load(str(old).encode(), ctypes.byref(h)) == _lib.RB_ERR_INVALID
+    assert "not a factorized tree" in _lib.last_error(None)
+    assert not h.value
+
+
 def test_save_needs_a_factorization(tmp_path):
     import robinsolver_b200 as rb
     from robinsolver_b200 import workloads as W
