@@ -47,7 +47,12 @@ extern "C" {
 
 /* ---- precision modes for rb_tree_factor ----------------------------------------------------- */
 #define RB_PREC_FP64  0           /* every operation in complex128                                    */
-#define RB_PREC_MIXED 1           /* reserved: split-BF16 lower levels + FP64 refinement              */
+#define RB_PREC_MIXED 1           /* merge levels l >= 2 with interfaces of >= 128 points: GEMMs on the
+                                     tcgen05 tensor cores in split TF32 (FP32 accumulation, ~1e-6
+                                     relative); the top two levels, the interface inverses, the leaves
+                                     and the FD residual in FP64; every solve refined against the FP64
+                                     residual of the global FD system to the tree's tolerance
+                                     (rb_tree_set_refinement, default 1e-10 relative)                  */
 
 /* ---- sample-point kinds for rb_tree_sample_points ------------------------------------------- */
 #define RB_POINTS_POTENTIAL 0     /* interior cell centres where elliptic_operator%k is sampled       */
@@ -242,8 +247,83 @@ int rb_check_solution_device(const rb_tree* tree, int irhs, const double* d_u_ex
 int rb_tree_save(const rb_tree* tree, const char* path);
 int rb_tree_load(const char* path, rb_tree** out);
 
+/* Iterative refinement of solves against a RB_PREC_MIXED factorization.  The reference solves
+ * with its one FP64 factorization (robin_tree_solve, robin_tree_module.f90:198-233) and has no
+ * counterpart; this is the `tol` of a mixed-precision solve.  Each solve applies corrections
+ * d = M^-1 (b - A x), with the global FD system's residual b - A x in FP64, until every right-hand
+ * side's estimated relative max-norm error rho |d| / |x| (rho the observed contraction factor) is
+ * below tol / 10, or fails with RB_ERR_NUMERIC after max_iter corrections or when the iteration
+ * does not contract.  Defaults: tol = 1e-10, max_iter = 8.  Solves of an FP64 factorization are
+ * direct and ignore these settings. */
+int rb_tree_set_refinement(rb_tree* tree, double tol, int max_iter);
+
+/* The last mixed-precision solve: corrections applied, the largest contraction factor seen, the
+ * estimated relative error of the returned solutions and the last residual max |b - A x| / max |x|
+ * (any output pointer may be NULL). */
+int rb_tree_refine_info(const rb_tree* tree, int32_t* iters, double* contraction, double* est_err,
+                        double* residual);
+
 /* Number of this library's kernels launched by the last factor and the last solve. */
 int rb_tree_launch_counts(const rb_tree* tree, int64_t* factor_launches, int64_t* solve_launches);
+
+/* ---- serving: resident factorized trees and a continuously batched request loop ---------------
+ *
+ * No counterpart in the reference, which factors one tree and solves one right-hand side per call,
+ * once per process (robin_tree_solve, robin_tree_module.f90:198-233, 1014-1029).  A server owns
+ * several trees on the current device.  Each tree has a worker thread and its own CUDA streams, so
+ * the trees' work overlaps on the device.  Solve requests queued for a tree are merged, up to
+ * max_batch_rhs right-hand sides, into one batched sweep when the tree's previous work is done;
+ * requests arriving meanwhile form the next batch.  A factor request is ordered with its tree's
+ * solves: solves submitted before it use the old factorization.  A tree's first factorization
+ * reserves its estimated device footprint (factor storage, buffers of a full batch, input staging)
+ * against the server's budget and waits while other trees' reservations leave too little room.
+ * Latency is measured from the request's arrival stamp (server clock, rb_server_now; a negative
+ * stamp means the submit time) to its completion with the solution in host memory. */
+typedef struct rb_server rb_server;
+
+typedef struct rb_server_opts {
+    int64_t device_budget;     /* bytes the trees and their buffers may reserve together;
+                                  0 = 90% of the device memory free at creation                     */
+    int32_t max_batch_rhs;     /* most right-hand sides merged into one sweep (0: 64)               */
+    int32_t precision;         /* RB_PREC_FP64 or RB_PREC_MIXED for every factorization             */
+    double  tol;               /* refinement tolerance of mixed-precision solves (0: 1e-10)         */
+} rb_server_opts;
+
+typedef struct rb_server_stats {
+    int64_t solves, rhs, factors, batches, failed;   /* completed requests since the last reset    */
+    double  p50_ms, p99_ms, mean_ms, max_ms;         /* solve latency: arrival -> solution on host */
+    double  factor_p50_ms, factor_max_ms;            /* factor latency: arrival -> factor resident */
+    int64_t reserved_bytes;                          /* device memory reserved by the trees        */
+} rb_server_stats;
+
+int rb_server_create(const rb_server_opts* opts, rb_server** out);
+/* Stops the workers (queued requests fail), releases every tree and buffer. */
+int rb_server_destroy(rb_server* server);
+const char* rb_server_last_error(const rb_server* server);
+/* Seconds since the server was created: the clock of arrival stamps and latencies. */
+double rb_server_now(const rb_server* server);
+/* Registers a tree geometry (as rb_tree_create; rb_geom.device_budget and RB_FLAG_ASYNC_FACTOR
+ * are ignored) and starts its worker; device memory is reserved by its first factorization. */
+int rb_server_add_tree(rb_server* server, const rb_geom* geom, int32_t* tree_id);
+int rb_server_tree_info(rb_server* server, int32_t tree_id, rb_info* info);
+/* Factor request: host potential samples k (n_interior complex at RB_POINTS_POTENTIAL, copied
+ * before returning), or k = NULL and the RB_FIELD_BUMP_POTENTIAL parameters (kb, delta, w, then
+ * (cx, cy, a) per bump, field_count bumps; copied) sampled on the device. */
+int rb_server_submit_factor(rb_server* server, int32_t tree_id, const double* k, int field_count,
+                            const double* field_params, double arrival, int64_t* request);
+/* Solve request of nrhs <= max_batch_rhs right-hand sides: field = RB_FIELD_POINT_SOURCE or
+ * RB_FIELD_PLANE_WAVE with 3 parameters per right-hand side (as rb_tree_sample_device; copied),
+ * or field = -1 and host arrays f (nrhs * n_interior complex) and g (nrhs * root_nb complex), which
+ * must stay valid until the request completes (NULL = zero).  u: host buffer of
+ * nrhs * nleaves * leaf_n complex that receives the solutions (NULL: not copied out). */
+int rb_server_submit_solve(rb_server* server, int32_t tree_id, int nrhs, int field, const double* params,
+                           const double* f, const double* g, double* u, double arrival, int64_t* request);
+/* Waits for a request (timeout_s < 0: without limit).  Returns its status (RB_OK or RB_ERR_*, with
+ * the message in rb_server_last_error) and forgets it, or 1 if it is still pending at the timeout. */
+int rb_server_wait(rb_server* server, int64_t request, double timeout_s);
+/* Counters and latency percentiles of the requests completed since the last reset (reset != 0
+ * clears them after reading). */
+int rb_server_get_stats(rb_server* server, rb_server_stats* stats, int reset);
 
 /* Leaf Robin-to-Robin maps for callers that cannot allocate device memory.  No counterpart in
  * the reference (whose leaf RtR is node%RtR after RTR_solve, robin_tree_module.f90:728-799; the
@@ -264,7 +344,7 @@ int rb_tree_launch_counts(const rb_tree* tree, int64_t* factor_launches, int64_t
  *            faces x1 x2 y1 y2 -- what rb_tree_get_rtr(tree, L, i) returns for a factored tree
  *  stream    cudaStream_t to run on (NULL = the default stream); the call returns after the
  *            stream's work is done
- * Limit: nleaves * (b*a^2 + nb*(nb + a*b)) * 16 + 256 bytes of scratch must fit 32 MiB (102 leaves
+ * Limit: nleaves * (b*a^2 + nb*(nb + a*b)) * 16 + 256 bytes of scratch must fit 32 MiB (85 leaves
  * of 16x16); larger batches are refused with RB_ERR_INVALID and a message giving the limit.
  * The first call on a device looks up the array's address (cudaGetSymbolAddress) with that device
  * current; make that first call before starting any stream capture.  All calls share the array

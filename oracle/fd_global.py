@@ -203,3 +203,115 @@ def backward_error(L, domain, h_tgt, kb, bndry_params, kvals, U, F, G):
                 (Rabs + (abs(zeta) + abs(nu)) * A0abs[:nb]).max())
     bmax = max(np.abs(F).max(), np.abs(G).max() if G.size else 0.0)
     return float(np.abs(res).max() / (normA * np.abs(U).max() + bmax))
+
+
+def _lattice(root, leaves):
+    """Leaf positions (ix, iy) on the regular leaf lattice and the inverse table."""
+    w = leaves[0].box[1] - leaves[0].box[0]
+    lo = root.box[0]
+    ix = np.array([int(round((lf.box[0, 0] - lo[0]) / w[0])) for lf in leaves])
+    iy = np.array([int(round((lf.box[0, 1] - lo[1]) / w[1])) for lf in leaves])
+    nx, ny = ix.max() + 1, iy.max() + 1
+    at = -np.ones((nx, ny), dtype=np.int64)
+    at[ix, iy] = np.arange(len(leaves))
+    return ix, iy, nx, ny, at
+
+
+class SparseFD:
+    """The same global system as ``GlobalFD``, assembled with array operations so that it can be
+    built at the full benchmark sizes (1024^2: 1.3 M unknowns), from the potential samples the
+    B200 path receives.
+
+    kvals: (nleaves, a*b) potential at the leaves' interior cell centres (leaf DFS order,
+    x fastest).  Rows and unknowns: every leaf's u vector in get_solution order.  ``solve``
+    factors the matrix once with SuperLU and solves for (F, G) pairs in the B200 path's input
+    layout (F: (nleaves, a*b) sources, G: (root_nb,) boundary data in the root's face order)."""
+
+    def __init__(self, L, domain, h_tgt, kb, bndry_params, kvals):
+        root, levels = H.build_tree(L, np.asarray(domain, dtype=np.float64), 2)
+        leaves = levels[-1]
+        h, grid = H.get_h(h_tgt, leaves[0].box, 2)
+        a, b = grid[0], grid[1]
+        nb = 2 * (a + b)
+        n = nb + a * b
+        nl = len(leaves)
+        self.a, self.b, self.nb, self.n, self.nl = a, b, nb, n, nl
+        bp = np.asarray(bndry_params, dtype=np.complex128)
+        nu = (-bp[0, 0] * bp[1, 1] + bp[0, 1] * bp[1, 0]) / (2 * bp[0, 0] * bp[0, 1])
+        zeta = (bp[0, 0] * bp[1, 1] + bp[0, 1] * bp[1, 0]) / (2 * bp[0, 0] * bp[0, 1])
+        A0 = sp.coo_matrix(H.fd_matrix(a, b, h, np.zeros(a * b, dtype=np.complex128), kb))
+        R = sp.coo_matrix(H.outgoing_rows(np.eye(n, dtype=np.complex128), a, b, h, kb))
+        kvals = np.asarray(kvals, dtype=np.complex128).reshape(nl, a * b)
+        base = (np.arange(nl, dtype=np.int64) * n)[:, None]
+        rows, cols, vals = [], [], []
+
+        def put(li_base, lj_base, r, c, v):
+            rows.append((li_base + r[None, :]).ravel())
+            cols.append((lj_base + c[None, :]).ravel())
+            vals.append(np.broadcast_to(v[None, :], (li_base.shape[0], v.size)).ravel())
+
+        keep = A0.row >= nb                                  # interior PDE rows
+        put(base, base, A0.row[keep], A0.col[keep], A0.data[keep])
+        diag = (base + np.arange(nb, n)[None, :]).ravel()
+        rows.append(diag); cols.append(diag); vals.append(kvals.ravel())
+        ix, iy, nx, ny, at = _lattice(root, leaves)
+        pf = H.get_pt_face((a, b))
+        off = H.face_offsets(pf)
+        rootpf = [ny * b, ny * b, nx * a, nx * a]
+        rootoff = H.face_offsets(rootpf)
+        self.g_rows = np.zeros(sum(rootpf), dtype=np.int64)   # root boundary point -> global row
+        for f in range(1, 5):
+            lo_r, hi_r = off[f - 1], off[f - 1] + pf[f - 1]
+            fo = {1: 2, 2: 1, 3: 4, 4: 3}[f]
+            jx, jy = {1: (ix - 1, iy), 2: (ix + 1, iy), 3: (ix, iy - 1), 4: (ix, iy + 1)}[f]
+            inside = (jx >= 0) & (jx < nx) & (jy >= 0) & (jy < ny)
+            li = np.nonzero(inside)[0]
+            lj = at[jx[li], jy[li]]
+            sel = (A0.row >= lo_r) & (A0.row < hi_r)
+            selR = (R.row >= lo_r) & (R.row < hi_r)
+            if li.size:
+                bi = base[li]
+                # transmission row of an interface point: h_own - zeta g_own - nu g_neighbour = 0
+                put(bi, bi, R.row[selR], R.col[selR], R.data[selR])
+                put(bi, bi, A0.row[sel], A0.col[sel], -zeta * A0.data[sel])
+                # the neighbour's row for the same point sits on the opposite face, same position
+                selo = (A0.row >= off[fo - 1]) & (A0.row < off[fo - 1] + pf[fo - 1])
+                rown = A0.row[selo] - off[fo - 1] + lo_r
+                put(bi, base[lj], rown, A0.col[selo], -nu * A0.data[selo])
+            lb = np.nonzero(~inside)[0]
+            if lb.size:
+                put(base[lb], base[lb], A0.row[sel], A0.col[sel], A0.data[sel])
+                pos = iy[lb] if f in (1, 2) else ix[lb]
+                idx = rootoff[f - 1] + pos[:, None] * pf[f - 1] + np.arange(pf[f - 1])[None, :]
+                self.g_rows[idx.ravel()] = (base[lb] + np.arange(lo_r, hi_r)[None, :]).ravel()
+        N = nl * n
+        self.A = sp.csc_matrix((np.concatenate(vals), (np.concatenate(rows), np.concatenate(cols))), shape=(N, N))
+        self._lu = None
+
+    def rhs(self, F, G):
+        out = np.zeros(self.nl * self.n, dtype=np.complex128)
+        out.reshape(self.nl, self.n)[:, self.nb:] = np.asarray(F, dtype=np.complex128).reshape(self.nl, -1)
+        out[self.g_rows] = np.asarray(G, dtype=np.complex128).reshape(-1)
+        return out
+
+    def factor(self):
+        if self._lu is None:
+            self._lu = spla.splu(self.A, permc_spec="COLAMD")
+        return self._lu
+
+    def solve(self, F, G):
+        """FP64 solution (nleaves, n) of the system for one right-hand side."""
+        return self.factor().solve(self.rhs(F, G)).reshape(self.nl, self.n)
+
+    def residual(self, U, F, G):
+        """max|A u - b| / max|b|."""
+        b = self.rhs(F, G)
+        r = self.A @ np.asarray(U, dtype=np.complex128).reshape(-1) - b
+        return float(np.max(np.abs(r)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def forward_error(U, U_ref):
+    """max|u - u_ref| / max|u_ref| over all leaves: the normwise max error every result states."""
+    U = np.asarray(U)
+    U_ref = np.asarray(U_ref)
+    return float(np.max(np.abs(U - U_ref)) / np.max(np.abs(U_ref)))

@@ -49,6 +49,9 @@ EXPORTS = [
     "rb_tree_set_timing", "rb_tree_stage_times", "rb_tree_clear_stage_times", "rb_tree_level_shape", "rb_tree_get_rtr", "rb_tree_launch_counts",
     "rb_leaf_rtr_noalloc",
     "rb_tree_sample_device", "rb_check_solution", "rb_check_solution_device", "rb_tree_save", "rb_tree_load",
+    "rb_tree_set_refinement", "rb_tree_refine_info",
+    "rb_server_create", "rb_server_destroy", "rb_server_last_error", "rb_server_now", "rb_server_add_tree",
+    "rb_server_tree_info", "rb_server_submit_factor", "rb_server_submit_solve", "rb_server_wait", "rb_server_get_stats",
 ]
 
 
@@ -84,6 +87,25 @@ class rb_info(C.Structure):
     ]
 
 
+class rb_server_opts(C.Structure):
+    _fields_ = [
+        ("device_budget", C.c_int64),
+        ("max_batch_rhs", C.c_int32),
+        ("precision", C.c_int32),
+        ("tol", C.c_double),
+    ]
+
+
+class rb_server_stats(C.Structure):
+    _fields_ = [
+        ("solves", C.c_int64), ("rhs", C.c_int64), ("factors", C.c_int64), ("batches", C.c_int64),
+        ("failed", C.c_int64),
+        ("p50_ms", C.c_double), ("p99_ms", C.c_double), ("mean_ms", C.c_double), ("max_ms", C.c_double),
+        ("factor_p50_ms", C.c_double), ("factor_max_ms", C.c_double),
+        ("reserved_bytes", C.c_int64),
+    ]
+
+
 def _load():
     if not LIB_PATH.exists():
         raise ImportError(f"{LIB_PATH} is missing: build it with `python -m robinsolver_b200.build`")
@@ -116,6 +138,23 @@ def _load():
         "rb_check_solution_device": (C.c_int, [P, C.c_int, P, C.c_int, C.c_int, D]),
         "rb_tree_save": (C.c_int, [P, C.c_char_p]),
         "rb_tree_load": (C.c_int, [C.c_char_p, C.POINTER(P)]),
+        "rb_tree_set_refinement": (C.c_int, [P, C.c_double, C.c_int]),
+        "rb_tree_refine_info": (C.c_int, [P, C.POINTER(C.c_int32), D, D, D]),
+        "rb_server_create": (C.c_int, [C.POINTER(rb_server_opts), C.POINTER(P)]),
+        "rb_server_destroy": (C.c_int, [P]),
+        "rb_server_last_error": (C.c_char_p, [P]),
+        "rb_server_now": (C.c_double, [P]),
+        "rb_server_add_tree": (C.c_int, [P, C.POINTER(rb_geom), C.POINTER(C.c_int32)]),
+        "rb_server_tree_info": (C.c_int, [P, C.c_int32, C.POINTER(rb_info)]),
+        "rb_server_submit_factor": (C.c_int, [P, C.c_int32, D, C.c_int, D, C.c_double, C.POINTER(C.c_int64)]),
+        "rb_server_submit_solve": (C.c_int, [P, C.c_int32, C.c_int, C.c_int, D, P, P, P, C.c_double,
+                                             C.POINTER(C.c_int64)]),
+        "rb_server_wait": (C.c_int, [P, C.c_int64, C.c_double]),
+        "rb_server_get_stats": (C.c_int, [P, C.POINTER(rb_server_stats), C.c_int]),
+        # test hook of the GEMM engines (rb_testing.cpp), not part of the drop-in boundary
+        "rb_test_zgemm": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_longlong, C.c_longlong, P,
+                                    C.c_longlong, C.c_longlong, P, C.c_longlong, C.c_longlong, C.c_double,
+                                    C.c_double, C.c_double, C.c_double, C.c_int]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

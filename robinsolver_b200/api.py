@@ -105,6 +105,27 @@ class leaf_solution:
 PRECISIONS = {"fp64": _lib.RB_PREC_FP64, "mixed": _lib.RB_PREC_MIXED}
 
 
+def make_geom(L, ell_op, opts, bndry_params, flags=0, budget=0) -> _lib.rb_geom:
+    """The C-ABI's rb_geom for robin_tree%factor(L, op, opts) with robin_tree%bndry_params."""
+    g = _lib.rb_geom()
+    g.d = int(ell_op.d)
+    g.L = int(L)
+    dom = np.asarray(ell_op.domain, dtype=np.float64)
+    for j in range(3):
+        g.domain[2 * j] = dom[0, j]
+        g.domain[2 * j + 1] = dom[1, j]
+    g.h_tgt = float(opts.h_tgt)
+    g.kb = float(opts.kb)
+    bp = np.asarray(bndry_params, dtype=np.complex128)
+    for q, (i, j) in enumerate([(0, 0), (1, 0), (0, 1), (1, 1)]):
+        g.bndry_params[2 * q] = bp[i, j].real
+        g.bndry_params[2 * q + 1] = bp[i, j].imag
+    g.ordering = int(opts.ordering)
+    g.flags = int(flags)
+    g.device_budget = int(budget)
+    return g
+
+
 class robin_tree:
     """robin_tree (robin_tree_module.f90:55-77) backed by a device-resident factorization."""
 
@@ -146,26 +167,12 @@ class robin_tree:
         if self.bndry_params is None:
             raise RobinSolverError(_lib.RB_ERR_BNDRY_PARAMS, "robin_tree%bndry_params is not set")
         self.close()
-        g = _lib.rb_geom()
-        g.d = int(ell_op.d)
-        g.L = int(L)
-        dom = np.asarray(ell_op.domain, dtype=np.float64)
-        for j in range(3):
-            g.domain[2 * j] = dom[0, j]
-            g.domain[2 * j + 1] = dom[1, j]
-        g.h_tgt = float(opts.h_tgt)
-        g.kb = float(opts.kb)
-        bp = np.asarray(self.bndry_params, dtype=np.complex128)
-        for q, (i, j) in enumerate([(0, 0), (1, 0), (0, 1), (1, 1)]):
-            g.bndry_params[2 * q] = bp[i, j].real
-            g.bndry_params[2 * q + 1] = bp[i, j].imag
-        g.ordering = int(opts.ordering)
-        g.flags = (_lib.RB_FLAG_VERBOSE if opts.debug.txt_output else 0) | \
-                  (_lib.RB_FLAG_SKIP_ROOT_RTR if self._skip_root else 0) | \
-                  (_lib.RB_FLAG_MERGE_DS if self._merge_ds else 0) | \
-                  (_lib.RB_FLAG_ASYNC_FACTOR if self._async else 0) | \
-                  (0 if self._graphs else _lib.RB_FLAG_NO_GRAPHS)
-        g.device_budget = self._budget
+        flags = (_lib.RB_FLAG_VERBOSE if opts.debug.txt_output else 0) | \
+                (_lib.RB_FLAG_SKIP_ROOT_RTR if self._skip_root else 0) | \
+                (_lib.RB_FLAG_MERGE_DS if self._merge_ds else 0) | \
+                (_lib.RB_FLAG_ASYNC_FACTOR if self._async else 0) | \
+                (0 if self._graphs else _lib.RB_FLAG_NO_GRAPHS)
+        g = make_geom(L, ell_op, opts, self.bndry_params, flags, self._budget)
         h = _lib.C.c_void_p()
         _check(lib.rb_tree_create(_lib.C.byref(g), _lib.C.byref(h)))
         self._h = h
@@ -246,8 +253,27 @@ class robin_tree:
                     G[r, bounds[fc]:bounds[fc + 1]] = gf(Xg[bounds[fc]:bounds[fc + 1]])
         return F, G
 
-    def solve(self, rhs):
-        """robin_tree%solve(rhs); ``rhs`` may be a list for a batched solve."""
+    def set_refinement(self, tol: float = 1e-10, max_iter: int = 8):
+        """Tolerance of the iterative refinement of solves against a mixed-precision factor
+        (rb_tree_set_refinement); FP64 factors solve directly."""
+        _check(lib.rb_tree_set_refinement(self._h, float(tol), int(max_iter)), self._h)
+
+    def refine_info(self):
+        """(corrections, contraction, estimated relative error, relative residual) of the last
+        mixed-precision solve."""
+        it = _lib.C.c_int32()
+        rho = _lib.C.c_double()
+        est = _lib.C.c_double()
+        res = _lib.C.c_double()
+        _check(lib.rb_tree_refine_info(self._h, _lib.C.byref(it), _lib.C.byref(rho), _lib.C.byref(est),
+                                       _lib.C.byref(res)), self._h)
+        return it.value, rho.value, est.value, res.value
+
+    def solve(self, rhs, tol: float | None = None):
+        """robin_tree%solve(rhs); ``rhs`` may be a list for a batched solve.  ``tol``: relative
+        error the refinement of a mixed-precision factor reaches (default 1e-10)."""
+        if tol is not None:
+            self.set_refinement(tol)
         if not self.factored:
             raise RobinSolverError(_lib.RB_ERR_NOT_FACTORED, "Error: Robin Tree must be factored first.")
         rhs_list = rhs if isinstance(rhs, (list, tuple)) else [rhs]
@@ -364,3 +390,111 @@ def check_solution(T: robin_tree, true_sol, irhs: int = 0, norm: str = "M", rel:
     code = {"1": 1, "2": 2}.get(str(norm), 0)
     _check(lib.rb_check_solution(T.handle, int(irhs), _lib.dptr(ue), code, 1 if rel else 0, _lib.dptr(err)), T.handle)
     return err
+
+
+class robin_server:
+    """Resident factorized trees behind a continuously batched request loop (rb_server_*; no
+    counterpart in the reference, which solves one right-hand side per call).
+
+    Solve requests queued for a tree while its previous sweep runs are merged into one batched
+    sweep; trees run concurrently; a tree's first factorization is admitted against the device
+    memory budget.  Host arrays handed to ``submit_solve`` are kept referenced here until the
+    request is collected with ``wait``."""
+
+    def __init__(self, device_budget: int = 0, max_batch_rhs: int = 64, precision: str = "fp64",
+                 tol: float = 1e-10):
+        o = _lib.rb_server_opts()
+        o.device_budget = int(device_budget)
+        o.max_batch_rhs = int(max_batch_rhs)
+        o.precision = PRECISIONS[precision]
+        o.tol = float(tol)
+        h = _lib.C.c_void_p()
+        _check(lib.rb_server_create(_lib.C.byref(o), _lib.C.byref(h)))
+        self._h = h
+        self._keep = {}
+
+    def _err(self, code):
+        if code != _lib.RB_OK:
+            msg = lib.rb_server_last_error(self._h)
+            raise RobinSolverError(code, msg.decode() if msg else "")
+
+    def close(self):
+        if self._h is not None:
+            lib.rb_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def now(self) -> float:
+        return lib.rb_server_now(self._h)
+
+    def add_tree(self, L, ell_op, opts, bndry_params) -> int:
+        g = make_geom(L, ell_op, opts, bndry_params)
+        tid = _lib.C.c_int32()
+        self._err(lib.rb_server_add_tree(self._h, _lib.C.byref(g), _lib.C.byref(tid)))
+        return tid.value
+
+    def tree_info(self, tid: int) -> _lib.rb_info:
+        inf = _lib.rb_info()
+        self._err(lib.rb_server_tree_info(self._h, int(tid), _lib.C.byref(inf)))
+        return inf
+
+    def submit_factor(self, tid: int, k=None, bumps=None, arrival: float = -1.0) -> int:
+        """k: potential samples at RB_POINTS_POTENTIAL, or bumps = (kb, delta, w, [(cx, cy, a), ...])
+        for the bump potential sampled on the device."""
+        req = _lib.C.c_int64()
+        if k is not None:
+            kv = np.ascontiguousarray(k, dtype=np.complex128)
+            self._err(lib.rb_server_submit_factor(self._h, int(tid), _lib.dptr(kv), 0, None, float(arrival),
+                                                  _lib.C.byref(req)))
+        else:
+            kb, delta, w, cs = bumps
+            par = np.ascontiguousarray(np.concatenate([[kb, delta, w], np.asarray(cs, dtype=np.float64).ravel()]))
+            self._err(lib.rb_server_submit_factor(self._h, int(tid), None, len(cs), _lib.dptr(par), float(arrival),
+                                                  _lib.C.byref(req)))
+        return req.value
+
+    def submit_solve(self, tid: int, nrhs: int, field: int = -1, params=None, f=None, g=None, u=None,
+                     arrival: float = -1.0) -> int:
+        """field = RB_FIELD_POINT_SOURCE / RB_FIELD_PLANE_WAVE with 3 params per right-hand side,
+        or host arrays f (nrhs, n_interior) and g (nrhs, root_nb) (None = zero).  u: complex128
+        array of nrhs * nleaves * leaf_n elements receiving the solutions (None: not copied)."""
+        req = _lib.C.c_int64()
+        keep = []
+        par = None
+        if params is not None:
+            par = np.ascontiguousarray(np.asarray(params, dtype=np.float64).ravel())
+            keep.append(par)
+        fp = gp = up = None
+        for arr in (f, g, u):
+            if arr is not None:
+                if not (isinstance(arr, np.ndarray) and arr.dtype == np.complex128 and arr.flags.c_contiguous):
+                    raise RobinSolverError(_lib.RB_ERR_INVALID, "host arrays must be C-contiguous complex128")
+                keep.append(arr)
+        fp = f.ctypes.data if f is not None else None
+        gp = g.ctypes.data if g is not None else None
+        up = u.ctypes.data if u is not None else None
+        self._err(lib.rb_server_submit_solve(self._h, int(tid), int(nrhs), int(field),
+                                             _lib.dptr(par) if par is not None else None, fp, gp, up,
+                                             float(arrival), _lib.C.byref(req)))
+        self._keep[req.value] = keep
+        return req.value
+
+    def wait(self, req: int, timeout: float = -1.0) -> bool:
+        """True once the request completed (raises on its error), False at the timeout."""
+        rc = lib.rb_server_wait(self._h, int(req), float(timeout))
+        if rc == 1:
+            return False
+        self._keep.pop(req, None)
+        self._err(rc)
+        return True
+
+    def stats(self, reset: bool = False) -> dict:
+        st = _lib.rb_server_stats()
+        self._err(lib.rb_server_get_stats(self._h, _lib.C.byref(st), 1 if reset else 0))
+        return {name: getattr(st, name) for name, _ in st._fields_}

@@ -85,15 +85,10 @@ __global__ void __launch_bounds__(32 * WM * WN, MINB) zgemm_dmma_kernel(const Ge
 template <int BM, int BN, int WM, int WN, int MINB>
 static cudaError_t launch_dmma(const GemmBatch& b, cudaStream_t s) {
     using Cfg = DmmaCfg<BM, BN, WM, WN>;
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(zgemm_dmma_kernel<BM, BN, WM, WN, MINB>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM_BYTES);
+    static DeviceAttrCache attr;
+    {
+        cudaError_t e = ensure_smem_attr(zgemm_dmma_kernel<BM, BN, WM, WN, MINB>, Cfg::SMEM_BYTES, attr, true);
         if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(zgemm_dmma_kernel<BM, BN, WM, WN, MINB>,
-                                 cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
-        if (e != cudaSuccess) return e;
-        attr = true;
     }
     const int tiles = ((b.max_m + BM - 1) / BM) * ((b.max_n + BN - 1) / BN);
     for (int off = 0; off < b.count; off += 65535) {
@@ -165,13 +160,10 @@ template <int BM, int BN, int WM, int WN, int MINB>
 static cudaError_t launch_dmma_split(const GemmBatch& b, cudaStream_t s) {
     using Cfg = DmmaCfg<BM, BN, WM, WN>;
     auto kern = zgemm_dmma_split_kernel<BM, BN, WM, WN, MINB>;
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM_BYTES);
+    static DeviceAttrCache attr;
+    {
+        cudaError_t e = ensure_smem_attr(kern, Cfg::SMEM_BYTES, attr, true);
         if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
-        if (e != cudaSuccess) return e;
-        attr = true;
     }
     if (b.count > 65535 || b.ksplit > 65535) return cudaErrorInvalidValue;
     const int tiles = ((b.max_m + BM - 1) / BM) * ((b.max_n + BN - 1) / BN);
@@ -202,13 +194,10 @@ template <int BM, int BN, int WM, int WN, int BK, int STAGES, int MINB>
 static cudaError_t launch_dmma_kc(const GemmBatch& b, cudaStream_t s) {
     using Cfg = DmmaKcCfg<BM, BN, WM, WN, BK, STAGES>;
     auto kern = zgemm_dmma_kc_kernel<BM, BN, WM, WN, BK, STAGES, MINB>;
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Cfg::SMEM_BYTES);
+    static DeviceAttrCache attr;
+    {
+        cudaError_t e = ensure_smem_attr(kern, Cfg::SMEM_BYTES, attr, true);
         if (e != cudaSuccess) return e;
-        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
-        if (e != cudaSuccess) return e;
-        attr = true;
     }
     const int tiles = ((b.max_m + BM - 1) / BM) * ((b.max_n + BN - 1) / BN);
     for (int off = 0; off < b.count; off += 65535) {
@@ -234,13 +223,11 @@ template <int BM, int BN, int TM, int TN, int BK, int STAGES, int MINB>
 static cudaError_t launch_cfg(const GemmBatch& b, cudaStream_t s) {
     constexpr int NT = (BM / TM) * (BN / TN);
     constexpr size_t SMEM = DfmaCfg<BM, BN, BK, STAGES>::SMEM_BYTES;
-    static bool attr = false;
-    if (!attr && SMEM > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(zgemm_desc_kernel<BM, BN, TM, TN, BK, STAGES, MINB>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    static DeviceAttrCache attr;
+    if (SMEM > 48 * 1024) {
+        cudaError_t e = ensure_smem_attr(zgemm_desc_kernel<BM, BN, TM, TN, BK, STAGES, MINB>, SMEM, attr);
         if (e != cudaSuccess) return e;
     }
-    attr = true;
     const int tiles = ((b.max_m + BM - 1) / BM) * ((b.max_n + BN - 1) / BN);
     for (int off = 0; off < b.count; off += 65535) {
         const int cnt = (b.count - off) < 65535 ? (b.count - off) : 65535;
@@ -255,13 +242,11 @@ template <int BM, int BN, int TM, int TN, int BK, int STAGES, int MINB>
 static cudaError_t launch_split(const GemmBatch& b, cudaStream_t s) {
     constexpr int NT = (BM / TM) * (BN / TN);
     constexpr size_t SMEM = DfmaCfg<BM, BN, BK, STAGES>::SMEM_BYTES;
-    static bool attr = false;
-    if (!attr && SMEM > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(zgemm_split_kernel<BM, BN, TM, TN, BK, STAGES, MINB>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM);
+    static DeviceAttrCache attr;
+    if (SMEM > 48 * 1024) {
+        cudaError_t e = ensure_smem_attr(zgemm_split_kernel<BM, BN, TM, TN, BK, STAGES, MINB>, SMEM, attr);
         if (e != cudaSuccess) return e;
     }
-    attr = true;
     if (b.count > 65535 || b.ksplit > 65535) return cudaErrorInvalidValue;
     const int tiles = ((b.max_m + BM - 1) / BM) * ((b.max_n + BN - 1) / BN);
     zgemm_split_kernel<BM, BN, TM, TN, BK, STAGES, MINB><<<dim3(tiles, b.count, b.ksplit), NT, SMEM, s>>>(

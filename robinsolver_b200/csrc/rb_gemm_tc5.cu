@@ -1,0 +1,446 @@
+// rb_gemm_tc5.cu -- descriptor-batched complex GEMM on the 5th-generation tensor cores
+// (tcgen05.mma kind::tf32, FP32 accumulators in tensor memory), for the mixed-precision factor
+// and solve of the lower merge levels.
+//
+// Split TF32 ("TF32x3"): every FP64 operand element x is held as two TF32 numbers,
+// hi = tf32(x) and lo = tf32(x - hi), so x = hi + lo to about 22 significant bits, and a real
+// product a*b is taken as ah*bh + ah*bl + al*bh (the lo*lo term is below that precision).  A
+// complex product is four real ones (re*re - im*im, re*im + im*re); the minus sign is the MMA's
+// own A-negate bit, so no negated copy of an operand is stored.  Twelve tcgen05.mma per k-step
+// of 8 accumulate into two FP32 accumulators in tensor memory, Cr and Ci (128 lanes x BN
+// columns each).  The result carries ~1e-6 relative error: the solve recovers FP64 accuracy by
+// iterative refinement against the FP64 residual (rb_refine.cu).
+//
+// CTA = one 128 x BN output tile of one problem (blockIdx.y), 9 warps:
+//   warps 0-7  producers: FP64 operand loads through the problem's ZViews (face gathers, row
+//              maps, skipped bands, exactly as the FP64 kernels), split to TF32 hi/lo in
+//              registers and stored to shared memory in the UMMA K-major no-swizzle layout; the
+//              loads of k-block kb+1 are in flight while block kb is converted and stored.
+//              Then the epilogue: tcgen05.ld of the accumulators (warp w reads lanes
+//              32 (w % 4) .. +31, half w / 4 of the columns), alpha/beta, scatter through the
+//              output maps.
+//   warp 8     allocates 2*BN tensor-memory columns; one lane issues the MMAs of each stage once
+//              its producers have arrived, and releases the stage with tcgen05.commit.
+// Every mbarrier wait is bounded (RB_TC5_WAIT_NS on the global timer).  A wait that runs out sets
+// RB_TC5_TIMEOUT in the status word, the CTA stops issuing work, waits (bounded) for the MMAs it
+// issued, frees its tensor memory and returns.
+#include <cstdint>
+
+#include "rb_kernels.h"
+
+namespace rb {
+
+namespace {
+
+constexpr int TC5_BM = 128;          // output rows per tile = UMMA M (one lane per row)
+constexpr int TC5_KB = 16;           // complex k per stage: 4 chunks of 4 TF32 = two UMMA k-steps
+constexpr int TC5_STAGES = 3;
+constexpr int TC5_PRODUCERS = 256;   // warps 0-7
+constexpr int TC5_THREADS = TC5_PRODUCERS + 32;
+constexpr unsigned long long RB_TC5_WAIT_NS = 1000000000ull;   // 1 s per wait
+
+template <int BN>
+struct Tc5Cfg {
+    static constexpr int A_PART = TC5_BM * TC5_KB * 4;   // bytes of one TF32 part of the A tile
+    static constexpr int B_PART = BN * TC5_KB * 4;
+    static constexpr int STAGE = 4 * A_PART + 4 * B_PART; // re/im x hi/lo of A and of B
+    // + 1024 for the alignment of the stages, + a guard of 16 row groups x one K chunk of A so
+    // that no operand descriptor of the last stage can point past the allocation
+    static constexpr int SMEM = TC5_STAGES * STAGE + 1024 + 16 * TC5_BM * 16;
+    static constexpr int TMEM_COLS = 2 * BN;               // Cr, Ci
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile(
+        "{\n\t.reg .b64 st;\n\t"
+        "mbarrier.arrive.release.cta.shared::cta.b64 st, [%0];\n\t}" ::"r"(bar)
+        : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.acquire.cta.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// waits for the phase with the given parity to complete; false after RB_TC5_WAIT_NS or when
+// another warp has already given up (*abort)
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort) {
+    if (mbar_try(bar, parity)) return true;
+    const unsigned long long t0 = global_ns();
+    for (unsigned it = 0;; ++it) {
+        if (mbar_try(bar, parity)) return true;
+        if ((it & 63) == 63) {
+            if (*abort) return false;
+            if (global_ns() - t0 > RB_TC5_WAIT_NS) return false;
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t tf32_rna(float x) {
+    uint32_t r;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+    return r;
+}
+
+// x -> (hi, lo): hi = tf32(x), lo = tf32(x - hi) with the difference taken in FP64
+__device__ __forceinline__ void split_tf32(double x, uint32_t& hi, uint32_t& lo) {
+    hi = tf32_rna(static_cast<float>(x));
+    lo = tf32_rna(static_cast<float>(x - static_cast<double>(__uint_as_float(hi))));
+}
+
+// UMMA shared-memory descriptor, K-major, no swizzle: core matrices of 8 rows x 16 bytes, rows
+// 16 bytes apart; sbo = bytes between 8-row groups, lbo = bytes between the two 16-byte K chunks
+// of one k-step.  Version 1 (sm_100), base offset 0, layout type 0 (SWIZZLE_NONE).
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFFu) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFFu) << 32;
+    d |= (uint64_t)1 << 46;
+    return d;
+}
+
+// instruction descriptor of kind::tf32: D FP32, A and B TF32, both K-major, M = 128, N = n
+__host__ __device__ constexpr uint32_t tc5_idesc(int n, bool neg_a) {
+    return (1u << 4) | (2u << 7) | (2u << 10) | ((neg_a ? 1u : 0u) << 13) | ((uint32_t)(n >> 3) << 17) |
+           ((uint32_t)(TC5_BM >> 4) << 24);
+}
+
+__device__ __forceinline__ void umma_tf32(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, "
+        "%14, %15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Per-thread share of one k-block: A units are (tile row, K chunk of 4), B units (column, chunk).
+template <int BN>
+struct Tc5Units {
+    static constexpr int A_UNITS = TC5_BM * (TC5_KB / 4) / TC5_PRODUCERS;           // 2
+    static constexpr int B_TOTAL = BN * (TC5_KB / 4);
+    static constexpr int B_UNITS = (B_TOTAL + TC5_PRODUCERS - 1) / TC5_PRODUCERS;  // 1 (BN <= 64), 2
+};
+
+template <int BN>
+struct Tc5Regs {
+    z a[Tc5Units<BN>::A_UNITS][4];
+    z b[Tc5Units<BN>::B_UNITS][4];
+};
+
+}  // namespace
+
+template <int BN>
+__global__ void __launch_bounds__(TC5_THREADS, 1) zgemm_tc5_kernel(const GemmDesc* __restrict__ descs, int* status) {
+    using Cfg = Tc5Cfg<BN>;
+    using U = Tc5Units<BN>;
+    extern __shared__ __align__(1024) unsigned char tc5_smem[];
+    __shared__ GemmDesc sd;
+    __shared__ int a_rows[TC5_BM];          // row offsets of the tile's rows in A (-1: outside m)
+    __shared__ long long b_cols[BN];        // column offsets of the tile's columns in B (-1: outside n)
+    __shared__ __align__(8) unsigned long long bars[2 * TC5_STAGES + 1];
+    __shared__ uint32_t tmem_slot;
+    __shared__ volatile int abort_flag;
+
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    {
+        const unsigned long long* src = reinterpret_cast<const unsigned long long*>(descs + blockIdx.y);
+        unsigned long long* dst = reinterpret_cast<unsigned long long*>(&sd);
+        for (int w = tid; w < (int)(sizeof(GemmDesc) / 8); w += TC5_THREADS) dst[w] = src[w];
+    }
+    __syncthreads();
+    const int m = sd.m, n = sd.n, K = sd.k;
+    const int tiles_m = (m + TC5_BM - 1) / TC5_BM;
+    const int tiles_n = (n + BN - 1) / BN;
+    if ((int)blockIdx.x >= tiles_m * tiles_n || K <= 0) return;      // uniform over the CTA
+    const int m0 = (blockIdx.x % tiles_m) * TC5_BM;
+    const int n0 = (blockIdx.x / tiles_m) * BN;
+
+    unsigned char* stage_base = reinterpret_cast<unsigned char*>(
+        (reinterpret_cast<uintptr_t>(tc5_smem) + 1023) & ~uintptr_t(1023));
+    const uint32_t full0 = smem_u32(&bars[0]);
+    const uint32_t empty0 = smem_u32(&bars[TC5_STAGES]);
+    const uint32_t done_bar = smem_u32(&bars[2 * TC5_STAGES]);
+
+    for (int i = tid; i < TC5_BM; i += TC5_THREADS) {
+        const int gi = m0 + i;
+        a_rows[i] = gi < m ? vrow(sd.A, gi) : -1;
+    }
+    for (int j = tid; j < BN; j += TC5_THREADS) {
+        const int gj = n0 + j;
+        b_cols[j] = gj < n ? (long long)vcol(sd.B, gj) * sd.B.ld : -1;
+    }
+    if (tid == 0) {
+        abort_flag = 0;
+        for (int s = 0; s < TC5_STAGES; ++s) {
+            mbar_init(full0 + 8 * s, TC5_PRODUCERS);
+            mbar_init(empty0 + 8 * s, 1);
+        }
+        mbar_init(done_bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    if (warp == 8) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
+                     "r"((uint32_t)Cfg::TMEM_COLS));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+    const int nkb = (K + TC5_KB - 1) / TC5_KB;
+
+    if (warp == 8) {
+        // ---------------- MMA issuer: one lane, the warp kept converged ----------------------
+        const uint32_t id_pos = tc5_idesc(BN, false), id_neg = tc5_idesc(BN, true);
+        const uint32_t c_re = tmem, c_im = tmem + BN;
+        bool ok = true;
+        for (int kb = 0; kb < nkb && ok; ++kb) {
+            const int s = kb % TC5_STAGES;
+            const uint32_t par = (uint32_t)((kb / TC5_STAGES) & 1);
+            ok = __all_sync(0xffffffffu, mbar_wait(full0 + 8 * s, par, &abort_flag));
+            if (!ok) break;
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            if (lane == 0) {
+                const uint32_t st = smem_u32(stage_base + (size_t)s * Cfg::STAGE);
+                const uint32_t a_rh = st, a_rl = st + Cfg::A_PART, a_ih = st + 2 * Cfg::A_PART,
+                               a_il = st + 3 * Cfg::A_PART;
+                const uint32_t bb = st + 4 * Cfg::A_PART;
+                const uint32_t b_rh = bb, b_rl = bb + Cfg::B_PART, b_ih = bb + 2 * Cfg::B_PART,
+                               b_il = bb + 3 * Cfg::B_PART;
+                // K chunk c of A sits at + c * 128 * 16 bytes, of B at + c * BN * 16
+                constexpr uint32_t LBO_A = TC5_BM * 16, LBO_B = BN * 16, SBO = 128;
+#pragma unroll
+                for (int q = 0; q < TC5_KB / 8; ++q) {
+                    const uint32_t oa = q * 2 * LBO_A, ob = q * 2 * LBO_B;
+                    const uint64_t Arh = umma_desc(a_rh + oa, LBO_A, SBO), Arl = umma_desc(a_rl + oa, LBO_A, SBO);
+                    const uint64_t Aih = umma_desc(a_ih + oa, LBO_A, SBO), Ail = umma_desc(a_il + oa, LBO_A, SBO);
+                    const uint64_t Brh = umma_desc(b_rh + ob, LBO_B, SBO), Brl = umma_desc(b_rl + ob, LBO_B, SBO);
+                    const uint64_t Bih = umma_desc(b_ih + ob, LBO_B, SBO), Bil = umma_desc(b_il + ob, LBO_B, SBO);
+                    const uint32_t acc = (kb > 0 || q > 0) ? 1u : 0u;
+                    // Cr = Ar Br - Ai Bi, small terms first
+                    umma_tf32(c_re, Arl, Brh, id_pos, acc);
+                    umma_tf32(c_re, Arh, Brl, id_pos, 1u);
+                    umma_tf32(c_re, Ail, Bih, id_neg, 1u);
+                    umma_tf32(c_re, Aih, Bil, id_neg, 1u);
+                    umma_tf32(c_re, Arh, Brh, id_pos, 1u);
+                    umma_tf32(c_re, Aih, Bih, id_neg, 1u);
+                    // Ci = Ar Bi + Ai Br
+                    umma_tf32(c_im, Arl, Bih, id_pos, acc);
+                    umma_tf32(c_im, Arh, Bil, id_pos, 1u);
+                    umma_tf32(c_im, Ail, Brh, id_pos, 1u);
+                    umma_tf32(c_im, Aih, Brl, id_pos, 1u);
+                    umma_tf32(c_im, Arh, Bih, id_pos, 1u);
+                    umma_tf32(c_im, Aih, Brh, id_pos, 1u);
+                }
+                umma_commit(empty0 + 8 * s);          // the stage is free once these MMAs are done
+            }
+            __syncwarp();
+        }
+        if (!ok) {
+            abort_flag = 1;
+            if (lane == 0) atomicOr(status, RB_TC5_TIMEOUT);
+        }
+        // the accumulators are complete (or, after a timeout, every issued MMA has finished) when
+        // this arrives: commit tracks all prior MMAs of this thread
+        if (lane == 0) umma_commit(done_bar);
+        __syncwarp();
+    } else {
+        // ---------------- producers --------------------------------------------------------------
+        const z* __restrict__ Ap = sd.A.p;
+        const z* __restrict__ Bp = sd.B.p;
+        const long long lda = sd.A.ld;
+        Tc5Regs<BN> cur;
+        auto load = [&](int kb, Tc5Regs<BN>& r) {
+            const int k0 = kb * TC5_KB;
+#pragma unroll
+            for (int u = 0; u < U::A_UNITS; ++u) {
+                const int unit = tid + u * TC5_PRODUCERS;       // (row, chunk): row fastest
+                const int row = unit % TC5_BM, c = unit / TC5_BM;
+                const int ro = a_rows[row];
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int k = k0 + 4 * c + e;
+                    r.a[u][e] = (ro >= 0 && k < K) ? __ldg(Ap + ro + (long long)vcol(sd.A, k) * lda) : zmk(0.0, 0.0);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U::B_UNITS; ++u) {
+                const int unit = tid + u * TC5_PRODUCERS;       // (column, chunk): chunk fastest
+                const int j = unit / 4, c = unit % 4;
+                const long long co = (unit < U::B_TOTAL) ? b_cols[j] : -1;
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const int k = k0 + 4 * c + e;
+                    r.b[u][e] = (co >= 0 && k < K) ? __ldg(Bp + vrow(sd.B, k) + co) : zmk(0.0, 0.0);
+                }
+            }
+        };
+        auto store = [&](int s, const Tc5Regs<BN>& r) {
+            unsigned char* st = stage_base + (size_t)s * Cfg::STAGE;
+#pragma unroll
+            for (int u = 0; u < U::A_UNITS; ++u) {
+                const int unit = tid + u * TC5_PRODUCERS;
+                const int row = unit % TC5_BM, c = unit / TC5_BM;
+                uint4 rh, rl, ih, il;
+                split_tf32(r.a[u][0].x, rh.x, rl.x); split_tf32(r.a[u][0].y, ih.x, il.x);
+                split_tf32(r.a[u][1].x, rh.y, rl.y); split_tf32(r.a[u][1].y, ih.y, il.y);
+                split_tf32(r.a[u][2].x, rh.z, rl.z); split_tf32(r.a[u][2].y, ih.z, il.z);
+                split_tf32(r.a[u][3].x, rh.w, rl.w); split_tf32(r.a[u][3].y, ih.w, il.w);
+                const size_t off = (size_t)c * TC5_BM * 16 + (size_t)row * 16;
+                *reinterpret_cast<uint4*>(st + off) = rh;
+                *reinterpret_cast<uint4*>(st + Cfg::A_PART + off) = rl;
+                *reinterpret_cast<uint4*>(st + 2 * Cfg::A_PART + off) = ih;
+                *reinterpret_cast<uint4*>(st + 3 * Cfg::A_PART + off) = il;
+            }
+            unsigned char* sb = st + 4 * Cfg::A_PART;
+#pragma unroll
+            for (int u = 0; u < U::B_UNITS; ++u) {
+                const int unit = tid + u * TC5_PRODUCERS;
+                if (unit >= U::B_TOTAL) continue;
+                const int j = unit / 4, c = unit % 4;
+                uint4 rh, rl, ih, il;
+                split_tf32(r.b[u][0].x, rh.x, rl.x); split_tf32(r.b[u][0].y, ih.x, il.x);
+                split_tf32(r.b[u][1].x, rh.y, rl.y); split_tf32(r.b[u][1].y, ih.y, il.y);
+                split_tf32(r.b[u][2].x, rh.z, rl.z); split_tf32(r.b[u][2].y, ih.z, il.z);
+                split_tf32(r.b[u][3].x, rh.w, rl.w); split_tf32(r.b[u][3].y, ih.w, il.w);
+                const size_t off = (size_t)c * BN * 16 + (size_t)j * 16;
+                *reinterpret_cast<uint4*>(sb + off) = rh;
+                *reinterpret_cast<uint4*>(sb + Cfg::B_PART + off) = rl;
+                *reinterpret_cast<uint4*>(sb + 2 * Cfg::B_PART + off) = ih;
+                *reinterpret_cast<uint4*>(sb + 3 * Cfg::B_PART + off) = il;
+            }
+        };
+        load(0, cur);
+        bool ok = true;
+        for (int kb = 0; kb < nkb; ++kb) {
+            const int s = kb % TC5_STAGES;
+            Tc5Regs<BN> nxt;
+            if (kb + 1 < nkb) load(kb + 1, nxt);       // in flight during the wait and the stores
+            if (kb >= TC5_STAGES) {
+                // the MMAs of k-block kb - STAGES read this stage
+                ok = mbar_wait(empty0 + 8 * s, (uint32_t)(((kb / TC5_STAGES) - 1) & 1), &abort_flag);
+                if (!ok) break;
+            }
+            store(s, cur);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // generic -> async proxy
+            mbar_arrive(full0 + 8 * s);
+            if (kb + 1 < nkb) cur = nxt;
+        }
+        if (!ok) {
+            abort_flag = 1;
+            atomicOr(status, RB_TC5_TIMEOUT);
+        }
+        // ---------------- epilogue ------------------------------------------------------------------
+        // warp-uniform: the accumulator reads below are warp-collective
+        const bool done = __all_sync(0xffffffffu, mbar_wait(done_bar, 0u, &abort_flag) && !abort_flag);
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        if (!done) {
+            if (lane == 0 && !abort_flag) atomicOr(status, RB_TC5_TIMEOUT);
+        } else {
+            const int quarter = warp & 3, half = warp >> 2;
+            const int row = quarter * 32 + lane;
+            const int gi = m0 + row;
+            const bool live = gi < m;
+            long long dro = 0, cro = 0;
+            bool use_c = false;
+            if (live) {
+                dro = vrow(sd.D, gi);
+                use_c = sd.C.p && !(gi >= sd.nobeta_r0 && gi < sd.nobeta_r1);
+                if (use_c) cro = vrow(sd.C, gi);
+            }
+            const z alpha = sd.alpha, beta = sd.beta;
+            constexpr int HALF = BN / 2;
+            constexpr int CH = HALF < 16 ? HALF : 16;
+#pragma unroll 1
+            for (int c0 = half * HALF; c0 < (half + 1) * HALF; c0 += CH) {
+                float vr[16], vi[16];
+                const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+                tmem_ld16(tmem + lane_base + (uint32_t)c0, vr);
+                tmem_ld16(tmem + lane_base + (uint32_t)(BN + c0), vi);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (!live) continue;
+#pragma unroll
+                for (int e = 0; e < CH; ++e) {
+                    const int gj = n0 + c0 + e;
+                    if (gj >= n) break;
+                    z v = zmul(alpha, zmk((double)vr[e], (double)vi[e]));
+                    if (use_c) zfma(v, beta, sd.C.p[cro + (long long)vcol(sd.C, gj) * sd.C.ld]);
+                    sd.D.p[dro + (long long)vcol(sd.D, gj) * sd.D.ld] = v;
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 8) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)Cfg::TMEM_COLS));
+    }
+}
+
+template <int BN>
+static cudaError_t launch_tc5(const GemmBatch& b, int* status, cudaStream_t s) {
+    using Cfg = Tc5Cfg<BN>;
+    static DeviceAttrCache attr;
+    cudaError_t e = ensure_smem_attr(zgemm_tc5_kernel<BN>, Cfg::SMEM, attr, true);
+    if (e != cudaSuccess) return e;
+    const int tiles = ((b.max_m + TC5_BM - 1) / TC5_BM) * ((b.max_n + BN - 1) / BN);
+    for (int off = 0; off < b.count; off += 65535) {
+        const int cnt = (b.count - off) < 65535 ? (b.count - off) : 65535;
+        zgemm_tc5_kernel<BN><<<dim3(tiles, cnt), TC5_THREADS, Cfg::SMEM, s>>>(b.d_desc + off, status);
+        note_launch();
+    }
+    return cudaGetLastError();
+}
+
+int tc5_tile_n(const GemmBatch& b) {
+    // n columns per tile: the widest UMMA N that the problems fill, 64 for the merges, 32 for
+    // narrow solves
+    return b.max_n <= 32 ? 32 : 64;
+}
+
+cudaError_t launch_gemm_tc5(const GemmBatch& b, int* status, cudaStream_t s) {
+    if (b.count == 0 || b.max_m == 0 || b.max_n == 0) return cudaSuccess;
+    if (!status) return cudaErrorInvalidValue;
+    return tc5_tile_n(b) == 32 ? launch_tc5<32>(b, status, s) : launch_tc5<64>(b, status, s);
+}
+
+}  // namespace rb

@@ -578,12 +578,10 @@ static cudaError_t gj_blocked(const GJDesc* d, int count, int m, int* st, cudaSt
     if (threads > MAXT) return cudaErrorInvalidValue;
     constexpr int CW = 8;
     const size_t sh = (size_t)m * CW * sizeof(z);
-    static bool attr = false;
-    if (!attr) {
-        cudaError_t e = cudaFuncSetAttribute(gj_apply_kernel<CW, NB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)(1024 * CW * sizeof(z)));
+    static DeviceAttrCache attr;
+    {
+        cudaError_t e = ensure_smem_attr(gj_apply_kernel<CW, NB>, 1024 * CW * sizeof(z), attr);
         if (e != cudaSuccess) return e;
-        attr = true;
     }
     for (int k0 = 0; k0 < m; k0 += NB) {
         const int nbk = (m - k0) < NB ? (m - k0) : NB;
@@ -615,13 +613,9 @@ static cudaError_t gj_resident(const GJDesc* d, int count, int m, void* flags, i
     if ((e = cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, dev)) != cudaSuccess) return e;
     if (!coop) return cudaSuccess;
     constexpr int SMEM_MAX = 227 * 1024;
-    static bool attr = false;
-    if (!attr) {
-        e = cudaFuncSetAttribute(gj_resident_kernel<NB, MAXT, RPT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 SMEM_MAX - (int)sizeof(ResShared<NB>));
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
+    static DeviceAttrCache attr;
+    e = ensure_smem_attr(gj_resident_kernel<NB, MAXT, RPT>, SMEM_MAX - sizeof(ResShared<NB>), attr);
+    if (e != cudaSuccess) return e;
     for (int ppc = 1; ppc <= npanels; ++ppc) {
         const int P = (npanels + ppc - 1) / ppc;
         const size_t sh = ((size_t)m + 2 * NB) * ppc * NB * sizeof(z);
@@ -662,12 +656,10 @@ cudaError_t gj_invert_batch(const GJDesc* d_desc, int count, int m, void* work, 
     if (count <= 0 || m <= 0) return cudaSuccess;
     if (m < GJ_BLOCKED_MIN) {
         const size_t sh = (size_t)m * m * sizeof(z);
-        static bool attr = false;
-        if (!attr) {
-            cudaError_t e = cudaFuncSetAttribute(gj_small_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                 (int)(GJ_SMALL_MAX * GJ_SMALL_MAX * sizeof(z)));
+        static DeviceAttrCache attr;
+        {
+            cudaError_t e = ensure_smem_attr(gj_small_kernel, GJ_SMALL_MAX * GJ_SMALL_MAX * sizeof(z), attr);
             if (e != cudaSuccess) return e;
-            attr = true;
         }
         gj_small_kernel<<<count, 256, sh, s>>>(d_desc, m, d_status);
         note_launch();

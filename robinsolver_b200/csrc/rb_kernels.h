@@ -1,9 +1,39 @@
 // rb_kernels.h -- internal launch interface of the CUDA kernels (not part of the C-ABI).
 #pragma once
 #include <cuda_runtime.h>
+#include <algorithm>
+#include <atomic>
+#include <mutex>
 #include "rb_common.cuh"
 
 namespace rb {
+
+// ---- per-device kernel attributes -----------------------------------------------------------------
+// A kernel's dynamic shared-memory limit (and carveout preference) is a setting of the current
+// device, not of the process.  Each launch site keeps one cache: the largest limit it has set on
+// each device, so that a handle on a second device (or a second host thread) sets it there too.
+struct DeviceAttrCache {
+    std::mutex mu;
+    std::atomic<size_t> set[128] = {};
+};
+template <class K>
+inline cudaError_t ensure_smem_attr(K kern, size_t bytes, DeviceAttrCache& c, bool max_carveout = false) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    const bool cached = dev >= 0 && dev < 128;
+    if (cached && c.set[dev].load(std::memory_order_acquire) >= bytes) return cudaSuccess;
+    std::lock_guard<std::mutex> lk(c.mu);
+    const size_t want = cached ? std::max(bytes, c.set[dev].load(std::memory_order_relaxed)) : bytes;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)want);
+    if (e != cudaSuccess) return e;
+    if (max_carveout) {
+        e = cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, (int)cudaSharedmemCarveoutMaxShared);
+        if (e != cudaSuccess) return e;
+    }
+    if (cached) c.set[dev].store(want, std::memory_order_release);
+    return cudaSuccess;
+}
 
 // ---- launch accounting --------------------------------------------------------------------------
 void note_launch();
@@ -11,8 +41,18 @@ long long launch_count();
 // message returned by rb_last_error(NULL) on this thread
 void set_thread_error(const char* msg);
 
+// ---- device status word ----------------------------------------------------------------------------
+// Bits a kernel ORs into a handle's status word (read after a factor or solve).
+constexpr int RB_STATUS_ZERO_PIVOT = 1;     // a leaf block or interface inverse met a zero pivot
+constexpr int RB_STATUS_GJ_TIMEOUT = 2;     // a resident Gauss-Jordan CTA gave up waiting for a panel
+constexpr int RB_TC5_TIMEOUT = 4;           // a tensor-core GEMM CTA gave up waiting on an mbarrier
+
 // ---- batched GEMM ---------------------------------------------------------------------------------
 cudaError_t launch_gemm_batch(const GemmBatch& b, cudaStream_t s);
+// The same batch on the tcgen05 tensor cores in split TF32 (rb_gemm_tc5.cu): ~1e-6 relative error,
+// for the mixed-precision levels.  status: device word for RB_TC5_TIMEOUT.
+cudaError_t launch_gemm_tc5(const GemmBatch& b, int* status, cudaStream_t s);
+int tc5_tile_n(const GemmBatch& b);
 // Chooses split-K for a fixed-order batch (sets ksplit, kchunk, pstride) and returns the
 // workspace it needs in complex elements (0: no split); the caller sets b.work.
 long long gemm_plan_split(GemmBatch& b);
@@ -75,6 +115,26 @@ cudaError_t sample_plane_waves(const double* pts, int nb, int ra, int rb, const 
                                const double* d_par, z* g, cudaStream_t s);
 cudaError_t check_solution(const z* u, const z* ue, int nleaves, int n, int norm, int rel, double* err,
                            cudaStream_t s);
+
+// ---- iterative refinement of the mixed-precision solve (rb_refine.cu) ------------------------------------
+struct RefineGeom {
+    int a, b;          // leaf grid
+    int nleaves;
+    int root_nb;       // boundary points of the whole domain
+    double kb;         // solve_opts%kb (FD boundary rows)
+    z zeta, nu;        // transmission coefficients of the merge (bndry_params)
+};
+// r <- r - A d for the global FD system, in place: interior rows in f [rhs][leaf][ab], domain
+// boundary rows in groot [rhs][root_nb], interface rows in ri [rhs][leaf][nb] (zero before when
+// first).  bclass[leaf*nb + r]: root position (>= 0) or -1 - (neighbour's leaf*nb + row).
+// rnorm[rhs] accumulates max |r| (|re| + |im|) when non-null.
+cudaError_t fd_residual(const RefineGeom& g, int nrhs, const z* d, z* f, z* groot, z* ri, const z* kv,
+                        const double* hh, const int* bclass, bool first, double* rnorm, cudaStream_t s);
+// hbuf of level l's children -= ri at the interface points listed in rows (nnodes*2*m leaf rows)
+cudaError_t iface_inject(int nnodes, int m, int nbc, int o1, int o2, int nrhs, int leaf_rows, const int* rows,
+                         const z* ri, z* hbuf, cudaStream_t s);
+// x += dx; per right-hand side max |x| into xnorm and max |dx| into dnorm (accumulated)
+cudaError_t refine_update(z* x, const z* dx, long long per, int nrhs, double* xnorm, double* dnorm, cudaStream_t s);
 
 // ---- sweep helpers --------------------------------------------------------------------------------------
 // children's g on their non-interface faces from the parent's g (backward sweep):

@@ -761,11 +761,10 @@ cudaError_t leaf_block_factor(const LeafGeom& g, int nleaves, const double* h, c
                               int* status, cudaStream_t s) {
     if (g.a == 16 && g.nb <= 32 * LTC_CH && leaf_tc_enabled()) {     // one warp per leaf, tensor cores
         const size_t sh = 4 * (256 + (size_t)LTC_CH * LTC_LDR * 32) * sizeof(z);
-        static bool attr = false;
-        if (!attr) {
-            cudaError_t e = cudaFuncSetAttribute(leaf_tc_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+        static DeviceAttrCache attr;
+        {
+            cudaError_t e = ensure_smem_attr(leaf_tc_factor_kernel, sh, attr);
             if (e != cudaSuccess) return e;
-            attr = true;
         }
         leaf_tc_factor_kernel<<<(nleaves + 3) / 4, 128, sh, s>>>(g, nleaves, h, k, sinv, Y, status);
         note_launch();
@@ -778,7 +777,8 @@ cudaError_t leaf_block_factor(const LeafGeom& g, int nleaves, const double* h, c
     }
     const size_t sh = leaf_block_factor_smem(g);
     if (sh > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(leaf_block_factor_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+        static DeviceAttrCache attr;
+        cudaError_t e = ensure_smem_attr(leaf_block_factor_kernel, sh, attr);
         if (e != cudaSuccess) return e;
     }
     leaf_block_factor_kernel<<<nleaves, 256, sh, s>>>(g, h, k, sinv, Y, status);
@@ -1021,11 +1021,10 @@ cudaError_t leaf_block_solve(const LeafGeom& g, int nleaves, int nrhs, const dou
                              const z* sinv, z* sol, cudaStream_t s) {
     if (g.a == 16 && leaf_solve_engine_hw()) {
         const size_t sh = ((size_t)2 * 256 + 2 * 16 * LHW_KC + (size_t)g.nb * LHW_KC) * sizeof(z);
-        static size_t set = 0;
-        if (sh > set) {
-            cudaError_t e = cudaFuncSetAttribute(leaf_hw_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+        static DeviceAttrCache attr;
+        {
+            cudaError_t e = ensure_smem_attr(leaf_hw_solve_kernel, sh, attr);
             if (e != cudaSuccess) return e;
-            set = sh;
         }
         leaf_hw_solve_kernel<<<nleaves, 256, sh, s>>>(g, nleaves, nrhs, h, f, gb, sinv, sol);
         note_launch();
@@ -1033,7 +1032,8 @@ cudaError_t leaf_block_solve(const LeafGeom& g, int nleaves, int nrhs, const dou
     }
     const size_t sh = ((size_t)g.a * g.a + 2 * (size_t)g.a * LEAF_KC) * sizeof(z);
     if (sh > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(leaf_block_solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh);
+        static DeviceAttrCache attr;
+        cudaError_t e = ensure_smem_attr(leaf_block_solve_kernel, sh, attr);
         if (e != cudaSuccess) return e;
     }
     leaf_block_solve_kernel<<<nleaves, 256, sh, s>>>(g, nleaves, nrhs, h, f, gb, sinv, sol);

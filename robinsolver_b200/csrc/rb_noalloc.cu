@@ -44,11 +44,29 @@ extern "C" int rb_leaf_rtr_noalloc(int a, int b, double kb, const double* d_h, c
                                    double* d_rtr, void* stream) {
     if (a < 3 || b < 3 || nleaves < 1 || !d_h || !d_k || !d_rtr)
         return noalloc_fail(RB_ERR_INVALID, "rb_leaf_rtr_noalloc: grid must be at least 3x3, nleaves >= 1, pointers non-null");
-    if (a * a > 1024 || 2 * (a + b) > 512)
+    // sizes in 64-bit arithmetic: a grid this large cannot fit the scratch array anyway
+    if ((int64_t)a * a > 1024 || 2 * ((int64_t)a + b) > 512)
         return noalloc_fail(RB_ERR_INVALID, "rb_leaf_rtr_noalloc: leaf grid too large for the leaf kernel");
     LeafGeom g{a, b, 2 * (a + b), 2 * (a + b) + a * b, kb};
     const size_t per_leaf = ((size_t)b * a * a + (size_t)g.nb * g.n) * sizeof(z);
     const size_t need = 256 + (size_t)nleaves * per_leaf;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128)
+        return noalloc_fail(RB_ERR_CUDA, "rb_leaf_rtr_noalloc: no current CUDA device");
+    if (a != 16) {
+        // leaves other than 16 wide run the one-CTA-per-leaf kernel, whose shared memory grows
+        // with a and nb: refuse a grid it cannot hold on this device
+        int optin = 0;
+        if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess)
+            return noalloc_fail(RB_ERR_CUDA, "rb_leaf_rtr_noalloc: cannot query the device's shared memory");
+        if (leaf_block_factor_smem(g) > (size_t)optin) {
+            char msg[200];
+            std::snprintf(msg, sizeof(msg),
+                          "rb_leaf_rtr_noalloc: a %dx%d leaf needs %zu bytes of shared memory, the device allows %d",
+                          a, b, leaf_block_factor_smem(g), optin);
+            return noalloc_fail(RB_ERR_INVALID, msg);
+        }
+    }
     if (need > RB_NOALLOC_SCRATCH_BYTES) {
         char msg[256];
         std::snprintf(msg, sizeof(msg),
@@ -57,9 +75,6 @@ extern "C" int rb_leaf_rtr_noalloc(int a, int b, double kb, const double* d_h, c
                       nleaves, a, b, need, RB_NOALLOC_SCRATCH_BYTES, (RB_NOALLOC_SCRATCH_BYTES - 256) / per_leaf);
         return noalloc_fail(RB_ERR_INVALID, msg);
     }
-    int dev = 0;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 128)
-        return noalloc_fail(RB_ERR_CUDA, "rb_leaf_rtr_noalloc: no current CUDA device");
     void* base = nullptr;
     {
         std::lock_guard<std::mutex> lk(g_noalloc_mutex);

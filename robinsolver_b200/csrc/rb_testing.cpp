@@ -1,0 +1,67 @@
+// rb_testing.cpp -- test hooks of the GEMM engines, outside the drop-in C-ABI.
+//
+// rb_test_zgemm runs `count` complex GEMMs D_i = alpha A_i B_i + beta D_i (column-major, device
+// pointers, plain strided views) on one engine, so that the tests can hold each engine against a
+// host product directly:
+//   engine 0: the FP64 launcher the FP64 path uses (tensor-core DMMA / DFMA tiles)
+//   engine 1: the tcgen05 split-TF32 kernel of the mixed-precision levels
+// It allocates its descriptor array itself and synchronises; it returns 0, a negative RB_ERR_*
+// code for bad arguments or CUDA failures, or the device status word's bits (> 0) when a kernel
+// reported one.
+#include <string>
+#include <vector>
+
+#include "robin_b200.h"
+#include "rb_kernels.h"
+
+using namespace rb;
+
+extern "C" int rb_test_zgemm(int engine, int m, int n, int k, const double* dA, long long lda, long long strideA,
+                             const double* dB, long long ldb, long long strideB, double* dC, long long ldc,
+                             long long strideC, double ar, double ai, double br, double bi, int count) {
+    if (m <= 0 || n <= 0 || k <= 0 || count <= 0 || !dA || !dB || !dC || lda < m || ldb < k || ldc < m)
+        return RB_ERR_INVALID;
+    std::vector<GemmDesc> h(count);
+    const z* A = reinterpret_cast<const z*>(dA);
+    const z* B = reinterpret_cast<const z*>(dB);
+    z* C = reinterpret_cast<z*>(dC);
+    const bool use_beta = br != 0.0 || bi != 0.0;
+    for (int i = 0; i < count; ++i) {
+        GemmDesc& g = h[i];
+        g = GemmDesc{};
+        g.A = zview(A + i * strideA, lda);
+        g.B = zview(B + i * strideB, ldb);
+        g.C = use_beta ? zview(C + i * strideC, ldc) : zview(nullptr, 1);
+        g.D = zout(C + i * strideC, ldc);
+        g.alpha = zmk(ar, ai);
+        g.beta = zmk(br, bi);
+        g.m = m; g.n = n; g.k = k;
+        g.nobeta_r0 = g.nobeta_r1 = 0;
+    }
+    GemmBatch b;
+    b.count = count;
+    b.max_m = m; b.max_n = n; b.max_k = k;
+    b.kcontig = true;
+    int* d_status = nullptr;
+    if (cudaMalloc(&b.d_desc, sizeof(GemmDesc) * count) != cudaSuccess) return RB_ERR_CUDA;
+    if (cudaMalloc(&d_status, sizeof(int)) != cudaSuccess) {
+        cudaFree(b.d_desc);
+        return RB_ERR_CUDA;
+    }
+    int rc = RB_OK;
+    cudaError_t e = cudaMemcpy(b.d_desc, h.data(), sizeof(GemmDesc) * count, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(d_status, 0, sizeof(int));
+    if (e == cudaSuccess) e = engine == 1 ? launch_gemm_tc5(b, d_status, 0) : launch_gemm_batch(b, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    int st = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&st, d_status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+        set_thread_error((std::string("rb_test_zgemm: ") + cudaGetErrorString(e)).c_str());
+        rc = RB_ERR_CUDA;
+    } else {
+        rc = st;
+    }
+    cudaFree(b.d_desc);
+    cudaFree(d_status);
+    return rc;
+}

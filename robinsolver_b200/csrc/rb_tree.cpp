@@ -36,6 +36,7 @@
 #include <cstring>
 #include <string>
 #include <functional>
+#include <map>
 #include <vector>
 
 #include "robin_b200.h"
@@ -159,6 +160,29 @@ struct rb_tree {
     int ev_used = 0;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     int64_t factor_launches = 0, solve_launches = 0;
+
+    // RB_PREC_MIXED: the GEMMs of the merge levels l >= 2 whose interface is at least one
+    // tensor-core tile tall (m >= 128) run on the tcgen05 split-TF32 kernel (~1e-6 relative);
+    // the top two levels, the interface inverses, the leaves and the FD residual stay FP64, and
+    // the solve refines every right-hand side against the FP64 residual to refine_tol
+    int prec = RB_PREC_FP64;          // precision of the current factorization
+    int gx_factor_prec = -1;          // precision the captured factor graph was recorded with
+    double refine_tol = 1e-10;
+    int refine_maxit = 8;
+    int refine_iters = 0;             // corrections the last solve applied
+    double refine_rho = 0.0;          // largest contraction factor seen
+    double refine_est = 0.0;          // estimated relative error after the last correction
+    double refine_res = 0.0;          // max |r| / max |x| of the last residual
+    std::vector<int> h_bclass;        // leaf boundary row -> root position or -1 - neighbour row
+    std::vector<std::vector<int>> h_ifrows;   // per level: interface points -> leaf boundary rows
+    int* d_bclass = nullptr;
+    std::vector<int*> d_ifrows;
+    int refine_cap = 0;
+    z* dsol = nullptr;                // the correction of the current refinement step
+    z* d_ri = nullptr;                // interface rows of the residual [rhs][leaf][nb]
+    double* d_norms = nullptr;        // [0, k) max|r|, [k, 2k) max|x|, [2k, 3k) max|dx|
+    double* h_norms = nullptr;
+    std::vector<DevBuf> refine_bufs;
 
     // CUDA graphs: the factor and solve launch sequences are fixed per tree (and per RHS count),
     // so after one direct run each is captured once and replayed
@@ -569,6 +593,18 @@ static int ensure_factor_storage(rb_tree* t) {
 // a GEMM batch, timed under the name of the engine it runs on
 #define RB_GEMM(batch, stream) RB_TIMED(gemm_stage_name(batch), (batch).flops, launch_gemm_batch(batch, stream))
 
+// merge level l of a mixed-precision factorization runs its GEMMs on the tcgen05 split-TF32
+// kernel: below the top two levels, and only where the interface fills the 128-row MMA tile
+static bool mixed_level(const rb_tree* t, int l) {
+    return t->prec == RB_PREC_MIXED && l >= 2 && l < t->P.L && t->P.lv[l].m >= 128;
+}
+static cudaError_t launch_gemm_level(rb_tree* t, const GemmBatch& b, int l, cudaStream_t s) {
+    return mixed_level(t, l) ? launch_gemm_tc5(b, t->d_status, s) : launch_gemm_batch(b, s);
+}
+#define RB_GEMM_L(batch, level, stream)                                                          \
+    RB_TIMED(mixed_level(t, level) ? "zgemm_tc5" : gemm_stage_name(batch), (batch).flops,         \
+             launch_gemm_level(t, batch, level, stream))
+
 static double gj_flops(int m, int count) { return 8.0 * (double)m * m * m * count; }
 // arithmetic of one structured leaf factor: b block inverses (8 a^3 each) and two block sweeps
 // of S^T Z = C^T with nb right-hand sides (8 a^2 nb per block and sweep)
@@ -611,16 +647,16 @@ static int run_factor(rb_tree* t, const z* dk, const std::vector<cudaEvent_t>* r
             if (fork) {
                 RB_CK(cudaEventRecord(t->ev_fork[l], s));
                 RB_CK(cudaStreamWaitEvent(t->stream2, t->ev_fork[l], 0));
-                RB_LAUNCH(launch_gemm_batch(t->fM1[l], t->stream2));
+                RB_LAUNCH(launch_gemm_level(t, t->fM1[l], l, t->stream2));
                 RB_CK(cudaEventRecord(t->ev_join[l], t->stream2));
             }
             RB_TIMED("merge_form", 0.0, merge_form_k(p.nnodes, p.m, t->nu, t->kinv[l], s));
-            RB_GEMM(t->fK[l], s);
+            RB_GEMM_L(t->fK[l], l, s);
             RB_TIMED("gj_invert", gj_flops(p.m, p.nnodes),
                      gj_invert_batch(t->gj_k[l].d_desc, p.nnodes, p.m, t->gj_work, t->d_status, s));
             if (rec) RB_CK(cudaEventRecord((*rec)[l], s));      // inv(K), A1, A2 of level l are ready
             if (fork) RB_CK(cudaStreamWaitEvent(s, t->ev_join[l], 0));
-            else RB_GEMM(t->fM1[l], s);
+            else RB_GEMM_L(t->fM1[l], l, s);
             if (l == 0 && before_root_tail && (rc = (*before_root_tail)())) return rc;
         } else {
             RB_TIMED("merge_form", 0.0, merge_form_d(cs, p.nnodes, p.m, p.o2, t->zeta, t->dinv[l], s));
@@ -631,19 +667,19 @@ static int run_factor(rb_tree* t, const z* dk, const std::vector<cudaEvent_t>* r
             if (fork) {
                 RB_CK(cudaEventRecord(t->ev_fork[l], s));
                 RB_CK(cudaStreamWaitEvent(t->stream2, t->ev_fork[l], 0));
-                RB_LAUNCH(launch_gemm_batch(t->fM1[l], t->stream2));
+                RB_LAUNCH(launch_gemm_level(t, t->fM1[l], l, t->stream2));
                 RB_CK(cudaEventRecord(t->ev_join[l], t->stream2));
             }
             RB_TIMED("merge_form", 0.0, merge_form_s(cs, p.nnodes, p.m, p.o1, t->zeta, t->nu, t->dinv[l], t->sinv[l], s));
             RB_TIMED("gj_invert", gj_flops(p.m, p.nnodes), gj_invert_batch(t->gj_s[l].d_desc, p.nnodes, p.m, t->gj_work, t->d_status, s));
             if (rec) RB_CK(cudaEventRecord((*rec)[l], s));      // inv(D), inv(S) of level l are ready
             if (fork) RB_CK(cudaStreamWaitEvent(s, t->ev_join[l], 0));
-            else RB_GEMM(t->fM1[l], s);
+            else RB_GEMM_L(t->fM1[l], l, s);
             if (l == 0 && before_root_tail && (rc = (*before_root_tail)())) return rc;
         }
-        RB_GEMM(t->fM2[l], s);
-        RB_GEMM(t->fM3[l], s);
-        RB_GEMM(t->fM4[l], s);
+        RB_GEMM_L(t->fM2[l], l, s);
+        RB_GEMM_L(t->fM3[l], l, s);
+        RB_GEMM_L(t->fM4[l], l, s);
         if ((rc = timer_end(t))) return rc;
     }
     return RB_OK;
@@ -807,26 +843,39 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
 // The solve on stream s.  wait (optional): the factor's progress events (run_factor's rec); the
 // leaf forward GEMM waits for the leaves and forward level l for level l of a factor that runs
 // on another stream; the backward sweep reads only levels the forward sweep waited for.
-static int run_solve(rb_tree* t, int k, cudaStream_t s, const std::vector<cudaEvent_t>* wait = nullptr) {
+// out: where the leaf solutions go (t->sol when null).  inject: subtract the interface rows of
+// the residual (t->d_ri) from the children's outgoing data before each level's merge (the
+// correction sweeps of the mixed-precision refinement).
+static int run_solve(rb_tree* t, int k, cudaStream_t s, const std::vector<cudaEvent_t>* wait = nullptr,
+                     z* out = nullptr, bool inject = false) {
     const Plan& P = t->P;
     const int L = P.L, nl = P.nleaves();
     LeafGeom lg{P.leaf_a(), P.leaf_b(), P.leaf_nb(), P.leaf_n(), P.kb};
     int rc;
+    auto inject_level = [&](int l) -> int {
+        if (!inject) return RB_OK;
+        const PlanLevel& p = P.lv[l];
+        RB_TIMED("sweep_aux", 0.0, iface_inject(p.nnodes, p.m, p.nbc, p.o1, p.o2, k, nl * P.leaf_nb(), t->d_ifrows[l],
+                                                t->d_ri, t->hbuf[l + 1], s));
+        return RB_OK;
+    };
     if ((rc = timer_begin(t, "forward"))) return rc;
     if (wait) RB_CK(cudaStreamWaitEvent(s, (*wait)[L], 0));
     RB_GEMM(t->sL0, s);
     for (int l = L - 1; l >= 1; --l) {
         if (wait) RB_CK(cudaStreamWaitEvent(s, (*wait)[l], 0));
-        RB_GEMM(t->sF12[l], s);
-        RB_GEMM(t->sF3[l], s);
-        RB_GEMM(t->sF4[l], s);
-        RB_GEMM(t->sF5[l], s);
+        if ((rc = inject_level(l))) return rc;
+        RB_GEMM_L(t->sF12[l], l, s);
+        RB_GEMM_L(t->sF3[l], l, s);
+        RB_GEMM_L(t->sF4[l], l, s);
+        RB_GEMM_L(t->sF5[l], l, s);
     }
     // the root: x = h + T_iN g_N needs level 1's maps (and the K form's first product, A2), not
     // the root's inverse, so it runs as soon as the root's A2 is formed
     if (L > 0) {
         const PlanLevel& p = P.lv[0];
         if (wait) RB_CK(cudaStreamWaitEvent(s, t->ev_root_forms, 0));
+        if ((rc = inject_level(0))) return rc;
         RB_TIMED("sweep_aux", 0.0, sweep_scatter_down(p.nnodes, k, p.nb, p.nbc, p.m, p.o1, p.o2, p.n1, p.n2,
                                                       t->d_pmap1[0], t->d_pmap2[0], t->gbuf[0], t->gbuf[1], s));
         RB_GEMM(t->sR1, s);
@@ -842,12 +891,180 @@ static int run_solve(rb_tree* t, int k, cudaStream_t s, const std::vector<cudaEv
         const PlanLevel& p = P.lv[l];
         RB_TIMED("sweep_aux", 0.0, sweep_scatter_down(p.nnodes, k, p.nb, p.nbc, p.m, p.o1, p.o2, p.n1, p.n2, t->d_pmap1[l],
                                      t->d_pmap2[l], t->gbuf[l], t->gbuf[l + 1], s));
-        RB_GEMM(t->sBY[l], s);
+        RB_GEMM_L(t->sBY[l], l, s);
     }
     if ((rc = timer_end(t))) return rc;
     if ((rc = timer_begin(t, "leaf_recover"))) return rc;
-    RB_TIMED("leaf_solve", 0.0, leaf_block_solve(lg, nl, k, t->d_h, t->d_f, t->gbuf[L], t->leaf_sinv, t->sol, s));
+    RB_TIMED("leaf_solve", 0.0, leaf_block_solve(lg, nl, k, t->d_h, t->d_f, t->gbuf[L], t->leaf_sinv,
+                                                 out ? out : t->sol, s));
     if ((rc = timer_end(t))) return rc;
+    return RB_OK;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Mixed-precision refinement: tables of the global FD system's boundary rows and the loop.
+
+// bclass[leaf*nb + r]: the root boundary position of a point on the domain boundary, or
+// -1 - (leaf'*nb + r') of the neighbouring leaf's row for the same interface point; ifrows[l]:
+// for every node of level l and child k, the leaf boundary rows of the child's interface points
+// in the child's face order.  Both follow the merges' face orderings (pmap1, pmap2) from the
+// leaves up, so the interface rows land where each merge reads its children's outgoing data.
+static std::string build_refine_tables(const Plan& P, std::vector<int>& bclass, std::vector<std::vector<int>>& ifrows) {
+    const int L = P.L;
+    const PlanLevel& lf = P.lv[L];
+    const int nl = lf.nnodes, nb = lf.nb;
+    std::vector<int> cur((size_t)nl * nb);
+    for (size_t e = 0; e < cur.size(); ++e) cur[e] = (int)e;
+    ifrows.assign(L, {});
+    for (int l = L - 1; l >= 0; --l) {
+        const PlanLevel& p = P.lv[l];
+        const PlanLevel& c = P.lv[l + 1];
+        std::vector<int> par((size_t)p.nnodes * p.nb, -1);
+        std::vector<int>& ir = ifrows[l];
+        ir.assign((size_t)p.nnodes * 2 * p.m, -1);
+        for (int i = 0; i < p.nnodes; ++i)
+            for (int k = 0; k < 2; ++k) {
+                const int child = 2 * i + k, o = k ? p.o2 : p.o1;
+                const std::vector<int>& pm = k ? p.pmap2 : p.pmap1;
+                for (int q = 0; q < (int)pm.size(); ++q) {
+                    const int phys = q < o ? q : q + p.m;
+                    par[(size_t)i * p.nb + pm[q]] = cur[(size_t)child * c.nb + phys];
+                }
+                for (int q = 0; q < p.m; ++q) ir[((size_t)i * 2 + k) * p.m + q] = cur[(size_t)child * c.nb + o + q];
+            }
+        cur.swap(par);
+    }
+    bclass.assign((size_t)nl * nb, INT_MIN);
+    for (int q = 0; q < (int)cur.size(); ++q) {
+        if (cur[q] < 0) return "refinement tables: root boundary point without a leaf row";
+        bclass[cur[q]] = q;
+    }
+    // interface points: the neighbour across each inner face, found by exact box coordinates
+    // (every box edge is produced by the same bisection arithmetic on both sides)
+    std::map<std::pair<double, double>, int> by_lo, by_hix, by_hiy;
+    for (int i = 0; i < nl; ++i) {
+        const double* lo = &lf.lo[3 * i];
+        const double* hi = &lf.hi[3 * i];
+        by_lo[{lo[0], lo[1]}] = i;
+        by_hix[{hi[0], lo[1]}] = i;
+        by_hiy[{lo[0], hi[1]}] = i;
+    }
+    for (int i = 0; i < nl; ++i) {
+        const double* lo = &lf.lo[3 * i];
+        const double* hi = &lf.hi[3 * i];
+        for (int f = 0; f < 4; ++f) {
+            if (lf.isb[4 * i + f]) continue;
+            std::map<std::pair<double, double>, int>::const_iterator it;
+            int fo;
+            if (f == 0) { it = by_hix.find({lo[0], lo[1]}); fo = 1; if (it == by_hix.end()) return "refinement tables: no x1 neighbour"; }
+            else if (f == 1) { it = by_lo.find({hi[0], lo[1]}); fo = 0; if (it == by_lo.end()) return "refinement tables: no x2 neighbour"; }
+            else if (f == 2) { it = by_hiy.find({lo[0], lo[1]}); fo = 3; if (it == by_hiy.end()) return "refinement tables: no y1 neighbour"; }
+            else { it = by_lo.find({lo[0], hi[1]}); fo = 2; if (it == by_lo.end()) return "refinement tables: no y2 neighbour"; }
+            const int j = it->second;
+            for (int q = 0; q < lf.pf[f]; ++q)
+                bclass[(size_t)i * nb + lf.off[f] + q] = -1 - (j * nb + lf.off[fo] + q);
+        }
+    }
+    for (int v : bclass)
+        if (v == INT_MIN) return "refinement tables: a leaf boundary row is neither on the domain boundary nor on an interface";
+    return "";
+}
+
+static int ensure_refine_storage(rb_tree* t, int k) {
+    const Plan& P = t->P;
+    int rc;
+    if (!t->d_bclass) {
+        const std::string msg = build_refine_tables(P, t->h_bclass, t->h_ifrows);
+        if (!msg.empty()) return fail(t, RB_ERR_GEOMETRY, msg);
+        if ((rc = alloc_n(t, t->bufs, t->h_bclass.size(), &t->d_bclass))) return rc;
+        RB_CK(cudaMemcpy(t->d_bclass, t->h_bclass.data(), t->h_bclass.size() * sizeof(int), cudaMemcpyHostToDevice));
+        t->d_ifrows.assign(P.L, nullptr);
+        for (int l = 0; l < P.L; ++l) {
+            if ((rc = alloc_n(t, t->bufs, t->h_ifrows[l].size(), &t->d_ifrows[l]))) return rc;
+            RB_CK(cudaMemcpy(t->d_ifrows[l], t->h_ifrows[l].data(), t->h_ifrows[l].size() * sizeof(int),
+                             cudaMemcpyHostToDevice));
+        }
+    }
+    if (k > t->refine_cap) {
+        free_list(t, t->refine_bufs);
+        t->refine_cap = 0;
+        const size_t per = (size_t)P.nleaves() * P.leaf_n();
+        if ((rc = alloc_n(t, t->refine_bufs, per * k, &t->dsol))) return rc;
+        if ((rc = alloc_n(t, t->refine_bufs, (size_t)P.nleaves() * P.leaf_nb() * k, &t->d_ri))) return rc;
+        if ((rc = alloc_n(t, t->refine_bufs, (size_t)3 * k + 1, &t->d_norms))) return rc;
+        if (t->h_norms) cudaFreeHost(t->h_norms);
+        t->h_norms = nullptr;
+        RB_CK(cudaMallocHost(&t->h_norms, ((size_t)3 * k + 1) * sizeof(double)));
+        t->refine_cap = k;
+    }
+    return RB_OK;
+}
+
+// The mixed-precision solve of the k right-hand sides in t->d_f / t->gbuf[0]: a first sweep,
+// then corrections d = M^-1 r with r = b - A x in FP64 until every right-hand side's estimated
+// relative error is below refine_tol.  The error of x after adding d is about rho |d|, rho the
+// contraction of the iteration (|d| / |x| for the first correction, |d| / |d_previous| after),
+// so the loop stops when rho |d| <= tol |x| / 10.  The residual overwrites d_f and gbuf[0].
+static int refine_solve(rb_tree* t, int k, cudaStream_t s) {
+    const Plan& P = t->P;
+    int rc;
+    if ((rc = ensure_refine_storage(t, k))) return rc;
+    const size_t per = (size_t)P.nleaves() * P.leaf_n();
+    RefineGeom rg{P.leaf_a(), P.leaf_b(), P.nleaves(), P.lv[0].nb, P.kb, t->zeta, t->nu};
+    if ((rc = run_solve(t, k, s, nullptr, t->sol, false))) return rc;
+    std::vector<double> dprev(k, 0.0), xn(k, 0.0);
+    t->refine_iters = 0;
+    t->refine_rho = 0.0;
+    t->refine_est = 0.0;
+    t->refine_res = 0.0;
+    bool converged = false;
+    for (int it = 0; it < t->refine_maxit; ++it) {
+        RB_CK(cudaMemsetAsync(t->d_norms, 0, ((size_t)3 * k + 1) * sizeof(double), s));
+        RB_TIMED("fd_residual", 0.0, fd_residual(rg, k, it == 0 ? t->sol : t->dsol, t->d_f, t->gbuf[0], t->d_ri, t->d_k,
+                                                 t->d_h, t->d_bclass, it == 0, t->d_norms, s));
+        if ((rc = run_solve(t, k, s, nullptr, t->dsol, true))) return rc;
+        RB_TIMED("refine_update", 0.0, refine_update(t->sol, t->dsol, (long long)per, k, t->d_norms + k,
+                                                     t->d_norms + 2 * k, s));
+        RB_CK(cudaMemcpyAsync(t->d_norms + 3 * k, t->d_status, sizeof(int), cudaMemcpyDeviceToDevice, s));
+        RB_CK(cudaMemcpyAsync(t->h_norms, t->d_norms, ((size_t)3 * k + 1) * sizeof(double), cudaMemcpyDeviceToHost, s));
+        RB_CK(cudaStreamSynchronize(s));
+        int st = 0;
+        std::memcpy(&st, t->h_norms + 3 * k, sizeof(int));
+        if (st & (RB_STATUS_GJ_TIMEOUT | RB_TC5_TIMEOUT))
+            return fail(t, RB_ERR_CUDA, "a device wait timed out during the solve");
+        t->refine_iters = it + 1;
+        double worst = 0.0, rho_max = 0.0, res = 0.0;
+        bool diverging = false;
+        for (int r = 0; r < k; ++r) {
+            const double rn = t->h_norms[r], x = t->h_norms[k + r], d = t->h_norms[2 * k + r];
+            const double ref = it == 0 ? x : dprev[r];
+            const double rho = ref > 0.0 ? d / ref : 0.0;
+            const double rel = x > 0.0 ? d / x : 0.0;
+            dprev[r] = d;
+            xn[r] = x;
+            res = std::max(res, x > 0.0 ? rn / x : 0.0);
+            // a correction far below the tolerance: converged, whatever the ratio of two
+            // rounding-level corrections says
+            if (rel <= 1e-3 * t->refine_tol) continue;
+            if (!(rho < 0.5)) diverging = true;
+            rho_max = std::max(rho_max, rho);
+            worst = std::max(worst, rho * rel);
+        }
+        t->refine_rho = std::max(t->refine_rho, rho_max);
+        t->refine_est = worst;
+        t->refine_res = res;
+        if (!std::isfinite(worst) || diverging)
+            return fail(t, RB_ERR_NUMERIC, "iterative refinement of the mixed-precision solve does not converge "
+                                           "(contraction " + std::to_string(rho_max) + ")");
+        if (worst <= 0.1 * t->refine_tol) {
+            converged = true;
+            break;
+        }
+    }
+    if (!converged)
+        return fail(t, RB_ERR_NUMERIC, "iterative refinement reached " + std::to_string(t->refine_maxit) +
+                                           " corrections without meeting the tolerance (estimated error " +
+                                           std::to_string(t->refine_est) + ")");
     return RB_OK;
 }
 
@@ -929,7 +1146,9 @@ int rb_tree_destroy(rb_tree* t) {
     drop_graph(t->gx_factor);
     drop_graph(t->gx_solve);
     free_list(t, t->solve_bufs);
+    free_list(t, t->refine_bufs);
     free_list(t, t->bufs);
+    if (t->h_norms) cudaFreeHost(t->h_norms);
     for (auto& e : t->ev)
         if (e) cudaEventDestroy(e);
     for (auto& e : t->ev_pool) cudaEventDestroy(e);
@@ -1073,6 +1292,8 @@ static int settle_factor(rb_tree* t) {
     if (*t->h_status) {
         t->factored = false;
         t->nrhs = 0;
+        if (*t->h_status & (RB_STATUS_GJ_TIMEOUT | RB_TC5_TIMEOUT))
+            return fail(t, RB_ERR_CUDA, "a device wait timed out during the factorization");
         return fail(t, RB_ERR_NUMERIC, "zero pivot met while inverting a leaf or interface matrix");
     }
     if (t->verbose) std::printf("RTR computation completed.\nFactorization completed.\n");
@@ -1097,8 +1318,8 @@ static int settle_solution(rb_tree* t) {
 static int factor_common(rb_tree* t, const double* k, int precision, bool host, int sync) {
     if (!t) return RB_ERR_INVALID;
     if (!k) return fail(t, RB_ERR_INVALID, "rb_tree_factor: null potential samples");
-    if (precision != RB_PREC_FP64)
-        return fail(t, RB_ERR_UNSUPPORTED, "precision mode " + std::to_string(precision) + " is not implemented");
+    if (precision != RB_PREC_FP64 && precision != RB_PREC_MIXED)
+        return fail(t, RB_ERR_INVALID, "precision mode " + std::to_string(precision) + " is not defined");
     int rc = ensure_factor_storage(t);
     if (rc) return rc;
     // a previous factor nobody waited for: report it, unless this call asks not to wait at all;
@@ -1110,6 +1331,12 @@ static int factor_common(rb_tree* t, const double* k, int precision, bool host, 
     const size_t nint = (size_t)P.nleaves() * P.leaf_a() * P.leaf_b();
     t->factored = false;
     t->nrhs = 0;
+    if (precision != t->prec) {
+        // the mixed factor launches other kernels on some levels: capture its own graph
+        t->prec = precision;
+        drop_graph(t->gx_factor);
+        t->factor_runs = 0;
+    }
     if (t->timing == 1) {
         timers_collect(t);
         t->stage_ms.clear();
@@ -1157,6 +1384,27 @@ static int solve_common(rb_tree* t, int nrhs, const double* f, const double* g, 
     const cudaMemcpyKind kind = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
     t->nrhs = 0;
     t->solve_overlapped = false;
+    if (t->prec == RB_PREC_MIXED) {
+        // mixed precision: a host-steered refinement loop after the factor (no overlap with it)
+        if (t->factor_deferred && (rc = launch_factor(t, nullptr))) return rc;
+        if ((rc = settle_factor(t))) return rc;
+        RB_CK(cudaStreamWaitEvent(t->stream, t->ev[3], 0));      // the last read-back is done
+        RB_CK(cudaMemcpyAsync(t->d_f, f, nrhs * nint * sizeof(z), kind, t->stream));
+        RB_CK(cudaMemcpyAsync(t->gbuf[0], g, nrhs * nroot * sizeof(z), kind, t->stream));
+        RB_CK(cudaEventRecord(t->ev[2], t->stream));
+        const long long l0 = launch_count();
+        if ((rc = refine_solve(t, nrhs, t->stream))) return rc;
+        t->solve_launches = launch_count() - l0;
+        RB_CK(cudaEventRecord(t->ev[3], t->stream));
+        RB_CK(cudaStreamSynchronize(t->stream));
+        float ms = 0.f;
+        RB_CK(cudaEventElapsedTime(&ms, t->ev[2], t->ev[3]));
+        t->s_time = ms * 1e-3;
+        timers_collect(t);
+        if (t->verbose) std::printf("Elliptic solve completed.\n");
+        t->nrhs = nrhs;
+        return RB_OK;
+    }
     if (t->factor_deferred && t->timing == 0) {
         // factor and solve together: the factor on the main stream, the solve on the copy stream
         // right after its inputs, each solve level waiting for that level of the factor; the main
@@ -1340,6 +1588,24 @@ int rb_tree_get_rtr(const rb_tree* tc, int level, int node, double* out) {
     return RB_OK;
 }
 
+int rb_tree_set_refinement(rb_tree* t, double tol, int max_iter) {
+    if (!t) return RB_ERR_INVALID;
+    if (!(tol > 0.0) || !(tol < 1.0) || max_iter < 1 || max_iter > 100)
+        return fail(t, RB_ERR_INVALID, "rb_tree_set_refinement: tol must be in (0, 1) and max_iter in 1..100");
+    t->refine_tol = tol;
+    t->refine_maxit = max_iter;
+    return RB_OK;
+}
+
+int rb_tree_refine_info(const rb_tree* t, int32_t* iters, double* contraction, double* est_err, double* residual) {
+    if (!t) return RB_ERR_INVALID;
+    if (iters) *iters = t->refine_iters;
+    if (contraction) *contraction = t->refine_rho;
+    if (est_err) *est_err = t->refine_est;
+    if (residual) *residual = t->refine_res;
+    return RB_OK;
+}
+
 int rb_tree_launch_counts(const rb_tree* t, int64_t* fl, int64_t* sl) {
     if (!t) return RB_ERR_INVALID;
     if (fl) *fl = t->factor_launches;
@@ -1348,6 +1614,33 @@ int rb_tree_launch_counts(const rb_tree* t, int64_t* fl, int64_t* sl) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------------
+// Accessors for the serving loop (rb_server.cpp), which drives handles through the C-ABI.
+
+namespace rb {
+// device address of the solutions of the last solve, [rhs][leaf][leaf_n]
+const z* tree_solutions(const rb_tree* t) { return t->sol; }
+int tree_device(const rb_tree* t) { return t->device; }
+// bytes a factorization plus the buffers of one solve of nrhs right-hand sides take on the device
+// (persistent factor storage as rb_tree_create's budget check counts it, the solve's per-level
+// vectors, its split-K workspace bound and, for a mixed-precision factor, the refinement buffers)
+double tree_bytes_estimate(const rb_tree* t, int nrhs, int precision) {
+    const Plan& Q = t->P;
+    const double ab = (double)Q.leaf_a() * Q.leaf_b();
+    double need = (double)Q.nleaves() * (ab * Q.leaf_a() + (double)Q.leaf_nb() * Q.leaf_n() + ab) * 16.0;
+    double per_rhs = (double)Q.nleaves() * (ab + Q.leaf_n()) * 16.0;
+    for (int l = 0; l < Q.L; ++l) {
+        need += (double)Q.lv[l].nnodes *
+                ((double)Q.lv[l].nb * Q.lv[l].nb + (t->kform ? 3.0 : 2.0) * Q.lv[l].m * Q.lv[l].m +
+                 2.0 * Q.lv[l].m * (Q.lv[l].n1 + Q.lv[l].n2)) * 16.0;
+        per_rhs += 2.0 * Q.lv[l].nnodes * Q.lv[l].nb * 16.0;
+    }
+    per_rhs *= 1.5;                                   // split-K workspace and the root's x1, x2
+    if (precision == RB_PREC_MIXED) per_rhs += (double)Q.nleaves() * (Q.leaf_n() + Q.leaf_nb()) * 16.0;
+    return need * 1.02 + per_rhs * nrhs + (64 << 20);
+}
+}  // namespace rb
 
 // ---------------------------------------------------------------------------------------------------
 // Device-side sampling, check_solution, save / load.

@@ -36,11 +36,15 @@ CONFIGS = {
 
 @dataclass
 class Potential:
+    """k(x) = kb^p (1 + 0.3 sum_j a_j bump_j(x)) + i delta kb^p.  p = 1 is the formula used
+    literally as ``ell_op%k`` (fd_module.f90:145 adds k itself, not its square); p = 2 is the
+    oscillatory stress variant whose coefficient is a squared wavenumber, kb^2 (1 + ...)."""
     kb: float
     delta: float
     centres: np.ndarray
     amps: np.ndarray
     width: float = 0.08
+    power: int = 1
 
     def __call__(self, X):
         X = np.asarray(X, dtype=np.float64)
@@ -49,7 +53,8 @@ class Potential:
         for c, a in zip(self.centres, self.amps):
             r2 = (X[:, 0] - c[0]) ** 2 + (X[:, 1] - c[1]) ** 2
             s += a * np.exp(-r2 / w2)
-        return self.kb * (1.0 + 0.3 * s) + 1j * (self.delta * self.kb)
+        scale = self.kb ** self.power
+        return scale * (1.0 + 0.3 * s) + 1j * (self.delta * scale)
 
 
 @dataclass
@@ -122,9 +127,10 @@ class Workload:
 
 
 def make_workload(config_id: int, instance: int = 0, nrhs: int | None = None, N=None, L=None,
-                  kb=None, nbumps=None, delta=None, kinds=None) -> Workload:
+                  kb=None, nbumps=None, delta=None, kinds=None, kpower: int = 1) -> Workload:
     """Seeded workload; seed = 1000 * config_id + instance.  Keyword overrides allow
-    smaller variants with the same generator."""
+    smaller variants with the same generator; ``kpower=2`` gives the squared-wavenumber
+    potential kb^2 (1 + ...) with the same draws."""
     c = dict(CONFIGS[config_id])
     for k_, v in dict(N=N, L=L, kb=kb, nbumps=nbumps, delta=delta, nrhs=nrhs, kinds=kinds).items():
         if v is not None:
@@ -133,7 +139,7 @@ def make_workload(config_id: int, instance: int = 0, nrhs: int | None = None, N=
     centres = rng.uniform(0.2, 0.8, size=(c["nbumps"], 2))
     amps = rng.uniform(-1.0, 1.0, size=c["nbumps"])
     dom = np.array([[0.0, 0.0, 0.0], [1.0, 1.0, 1.0]])
-    pot = Potential(kb=c["kb"], delta=c["delta"], centres=centres, amps=amps)
+    pot = Potential(kb=c["kb"], delta=c["delta"], centres=centres, amps=amps, power=kpower)
     wl = Workload(N=c["N"], L=c["L"], kb=c["kb"], domain=dom, potential=pot)
     for r in range(c["nrhs"]):
         kind = c["kinds"]

@@ -15,7 +15,7 @@ ROOT = Path(__file__).resolve().parents[1]
 def test_library_exports_every_declared_symbol():
     from robinsolver_b200 import _lib
     hdr = (ROOT / "include" / "robin_b200.h").read_text()
-    declared = set(re.findall(r"^\s*(?:int|void\*|const char\*)\s+(rb_\w+)\s*\(", hdr, re.M))
+    declared = set(re.findall(r"^\s*(?:int|double|void\*|const char\*)\s+(rb_\w+)\s*\(", hdr, re.M))
     assert declared == set(_lib.EXPORTS)
     for name in declared:
         assert hasattr(_lib.lib, name), name

@@ -5,7 +5,10 @@ Config 2 (512^2, L=10, kb=100): the FD system's conditioning puts the floor of a
 evaluation near 1e-11 -- the oracle itself, run with 1 and with 8 BLAS threads, differs by
 1.2e-11 on these right-hand sides -- so the bar there is 3e-11.  Full size (1024^2, L=12) is
 checked by the normwise backward error of the global FD system (oracle/fd_global.py), which
-the oracle's own solutions meet at ~2e-16; the bar is 1e-14.
+the oracle's own solutions meet at ~2e-16 (bar 1e-14), and by the max-norm forward error
+against an FP64 CPU solve of the same FD system (SuperLU on the assembled global matrix,
+bar 1e-10 relative).  The squared-wavenumber potential k = kb^2 (1 + ...) is held to the
+config-1 bar of 1e-11 against the oracle, including coarse leaves with |k| h^2 >= 4.
 """
 import numpy as np
 import pytest
@@ -182,4 +185,46 @@ def test_full_size_backward_error():
         e = G.backward_error(wl.L, wl.domain, wl.h_tgt, wl.opts_kb, wl.bndry_params, kv, U,
                              F[r].reshape(inf.nleaves, -1), Gs[r])
         assert e < 1e-14, (r, e)
+    T.close()
+
+
+@pytest.mark.parametrize("kb", [20.0, 128.0, 160.0, 200.0])
+def test_squared_potential_matches_oracle(kb):
+    """k = kb^2 (1 + 0.3 sum a_j bump_j) + i delta kb^2 on config 1's 64^2, L=4 tree.  kb = 20 is
+    the stress variant of config 1; from kb = 128 on, |k| h^2 >= 4 on the 16x16 leaves (h = 1/64),
+    so the interior blocks of the leaf's block-tridiagonal Schur complement are no longer
+    diagonally dominant and only the pivoting inside each block keeps the block LU stable.  The
+    oracle factors the dense leaf matrix with partial pivoting (zgetrf) and agrees with an
+    assembled SuperLU solve to 2e-13 on all four."""
+    wl = W.make_workload(1, kb=kb, kpower=2)
+    wl2 = W.make_workload(1, instance=1, kinds="plane", kb=kb, kpower=2)
+    rhs = wl.rhs + wl2.rhs
+    O, U = oracle_run(wl, rhs)
+    T = _factored(wl)
+    Ug = _solve(T, rhs)
+    for r in range(len(rhs)):
+        assert rel_err(Ug[r], U[r]) < 1e-11, (kb, r, rel_err(Ug[r], U[r]))
+    for l in (wl.L, 2, 0):
+        assert rel_err(T.get_rtr(l, 0), O.levels[l][0].rtr) < 1e-11, l
+    T.close()
+
+
+@pytest.mark.slow
+@pytest.mark.parametrize("kpower", [1, 2])
+def test_full_size_forward_error(kpower):
+    """1024^2, L=12, kb=200 (the headline configuration; kpower=2 is its squared-wavenumber
+    stress variant): the max-norm error of the returned solution against an FP64 CPU solve of
+    the same global FD system (SuperLU, oracle/fd_global.SparseFD), for two plane waves."""
+    wl = W.make_workload(4, nrhs=2, kpower=kpower)
+    T, op, opts = gpu_tree(wl)
+    T.factor(wl.L, op, opts)
+    F, Gs = T.sample_rhs(gpu_rhs(wl.rhs))
+    T.solve_samples(F, Gs)
+    inf = T.info()
+    kv = wl.potential(_samples(T)).reshape(inf.nleaves, -1)
+    S = G.SparseFD(wl.L, wl.domain, wl.h_tgt, wl.opts_kb, wl.bndry_params, kv)
+    for r in range(len(wl.rhs)):
+        Uc = S.solve(F[r], Gs[r])
+        e = G.forward_error(T.solution_array(r), Uc)
+        assert e < 1e-10, (kpower, r, e)
     T.close()
