@@ -1,27 +1,41 @@
 #!/usr/bin/env python
-"""Benchmark: factor + batched solve of the 1024^2 2D Helmholtz HPS problem on B200.
+"""Benchmark: factor + batched solve of the 1024^2 2D Helmholtz HPS problem on B200, mixed precision
+against FP64.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision mixed|fp64]
+    python bench.py --serve [--requests R]
 
 One step = the reference's hot path on one batch: robin_tree%factor of the 1024^2, L=12 tree
 (16x16 leaves, kb=200, seeded 100-bump potential with 0.002i*kb damping) followed by one batched
 solve of its 32 seeded plane-wave right-hand sides and get_solution.  ``value`` is right-hand
 sides per second with the factorization inside every step, so it moves with both factor time
-and solve throughput; factor_ms, solve_ms and per-step p50/p99 are reported beside it.
+and solve throughput.  The headline arm is the mixed-precision path (RB_PREC_MIXED: split-TF32
+tcgen05 GEMMs on the merge levels 2-6, FP64 elsewhere, every solve refined to 1e-10 against the
+FP64 residual); the plain FP64 path is timed on the same inputs in the same run and reported
+beside it (``fp64``, ``mixed_vs_fp64``).
 
 * value:  device-resident inputs (rb_tree_factor_device / rb_tree_solve_device /
           rb_get_solution_device), CUDA events on the library's stream, max over ranks.
 * e2e:    the same steps through the host C-ABI calls a user makes (rb_tree_factor,
           rb_tree_solve, rb_get_solution per RHS) from pinned host buffers: H2D of the
           potential and right-hand sides and D2H of every solution inside the timed region.
+* accuracy: mixed against FP64 GPU on every right-hand side; both against an FP64 CPU solve of
+          the same global FD system (SuperLU, run in a spawned process beside the GPU work) for
+          the first and last right-hand side; the normwise backward error of the e2e solutions.
 * roofline: per-launch CUDA events over a second pass of the same steps give the dominant
-          kernel's algorithmic flops / time; the denominator is the complex128 cuBLAS GEMM
-          rate measured in this run (MEASURED_PEAKS.json has no FP64 entry).
-* cpu_baseline / --impl reference: the reference's LAPACK/BLAS call sequence (oracle port,
-          scipy OpenBLAS, all host threads) timed on a sample of the same workload -- 16 leaves,
-          one node per merge level (children with random Robin-to-Robin maps of the true sizes),
-          leaf and node solves of one right-hand side -- and scaled by the node counts to the full
-          step (the reference solves one right-hand side per call).
+          kernel family's algorithmic flops / time, against the peak of the pipe it runs on: the
+          complex128 cuBLAS GEMM measured in this run (FP64 kernels; MEASURED_PEAKS.json has no
+          FP64 entry) or MEASURED_PEAKS.json's bf16 rate / 2 (TF32) / 3 (split products) for the
+          tcgen05 kernel.
+* cpu_baseline / --impl reference: the reference's LAPACK/BLAS call sequence (oracle port, scipy
+          OpenBLAS, all host threads) MEASURED on the whole workload: the full factor (every leaf
+          and merge) and a few single-RHS solves (the reference solves one right-hand side per
+          call); RHS/s = nrhs / (factor + nrhs x mean solve).  The reference arm cuts that one
+          pass into K consecutive measured steps.
+* --serve: the serving loop (rb_server_*): 8 resident trees of BASELINE's serving set, a
+          Poisson stream of device-sampled point-source / plane-wave solve requests (1-64 RHS)
+          with 20 refactors, at 0.5x and 0.9x of the measured saturated rate; p50/p99 latency
+          from arrival to solution in host memory, mixed and FP64 servers.
 Multi-GPU: replicas only (every rank factors and solves its own copy of the problem); the only
 collective is the max-reduction of the timings.
 """
@@ -43,11 +57,11 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "Factor time + solves/s on 1024² 2D Helmholtz, mixed vs FP64 GPU @1e-10; p99 ms"
 
-# DRAM bytes (read + write) per launch of a stage's kernel in one step of the 1024^2 / L=12
-# workload, from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum, one pass):
-# profiles/zgemm_dmma_kc_1024sq_L12_fp64.md.  ncu cannot run inside this script, so the figure
-# is carried here and reported for the bench's own workload only.
-DRAM_BYTES_PER_LAUNCH = {4: {"zgemm_tc": 1.912e8}}
+# DRAM bytes (read + write) per launch of the dominant kernel families in one step of the 1024^2,
+# L=12 workload, from one ncu capture of this script (dram__bytes_read.sum + dram__bytes_write.sum;
+# the profiles/ directory keeps the capture's summary and command).  ncu cannot run inside this
+# script, so the figures are carried here; they are reported for the 1024^2 workload only.
+DRAM_BYTES_PER_LAUNCH = {}
 
 
 def parse():
@@ -59,8 +73,14 @@ def parse():
     ap.add_argument("--nrhs", type=int, default=None, help="right-hand sides per step (default: the config's)")
     ap.add_argument("--config", type=int, default=4, choices=[1, 2, 4],
                     help="workload: 4 = 1024^2 L=12 (the headline), 2 = 512^2 L=10, 1 = 64^2 L=4 (profiling/tests)")
+    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
+                    help="the headline arm (value, e2e, roofline); the other precision is timed beside it")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-forward-error", action="store_true")
+    ap.add_argument("--serve", action="store_true",
+                    help="serving bench: 8 resident trees, Poisson solve stream at 0.5x and 0.9x of saturation")
+    ap.add_argument("--requests", type=int, default=4000, help="solve requests per offered load (--serve)")
     return ap.parse_args()
 
 
@@ -71,106 +91,177 @@ WORKLOAD_TEXT = {
 }
 
 
-def config_dict(cfg, nrhs):
+def config_dict(cfg, nrhs, precision):
     from robinsolver_b200 import workloads as W
     c = W.CONFIGS[cfg]
+    solve = "RHS batched solve" if precision == "fp64" else \
+        "RHS batched solve refined to 1e-10 against the FP64 residual"
     return {
-        "workload": f"{WORKLOAD_TEXT[cfg]}, impedance boundary; per step: factor + {nrhs} "
-                    f"{'plane-wave' if cfg == 4 else 'point-source/plane-wave'} RHS batched solve + get_solution",
-        "grid": c["N"], "L": c["L"], "leaf": "16x16", "nrhs": nrhs, "precision": "fp64",
+        "workload": f"{WORKLOAD_TEXT[cfg]}, impedance boundary; per step: factor ({precision}) + {nrhs} "
+                    f"{'plane-wave' if cfg == 4 else 'point-source/plane-wave'} {solve} + get_solution",
+        "grid": c["N"], "L": c["L"], "leaf": "16x16", "nrhs": nrhs, "precision": precision,
         "l2": "no flush: per-step working set and inputs larger than L2 (126 MB)" if cfg != 1
               else "small case: fits in L2",
     }
 
 
 # ------------------------------------------------------------------------------------------------
-# CPU baseline: the reference's LAPACK/BLAS call sequence on a sample of the workload
+# CPU baseline: the reference's LAPACK/BLAS call sequence, run on the whole workload
 # ------------------------------------------------------------------------------------------------
 
-def cpu_reference_step_seconds(wl, nrhs, threads):
-    """Seconds the reference's LAPACK/BLAS calls would take for one full step (factor + nrhs
-    single-RHS solves), from timed samples scaled by node counts."""
-    from threadpoolctl import threadpool_limits
-
+def _oracle_tree(wl):
     from oracle import hps_ref as H
+    T = H.RobinTree()
+    T.bndry_params = wl.bndry_params
+    T.nlvls = wl.L
+    T.ell_op = H.EllipticOperator(2, wl.domain, wl.potential)
+    T.opts = H.SolveOpts(h_tgt=wl.h_tgt, kb=wl.opts_kb)
+    T.root, T.levels = H.build_tree(wl.L, np.asarray(wl.domain, dtype=np.float64), 2)
+    T.keep_leaf = True
+    return T
 
-    rng = np.random.default_rng(4242)
+
+def reference_items(wl, nsolves):
+    """The reference's call sequence on the whole workload as a list of work items: every leaf
+    and merge of robin_tree%factor in compute_RTR's post order, then nsolves robin_tree%solve
+    calls of one right-hand side each (the reference solves one per call).  Returns the oracle
+    tree and the items; run_item executes one."""
+    T = _oracle_tree(wl)
+    order = []
+
+    def post(n):
+        if n.isleaf:
+            order.append(("leaf", n))
+        else:
+            post(n.child1)
+            post(n.child2)
+            order.append(("merge", n))
+    post(T.root)
+    order += [("solve", r) for r in range(nsolves)]
+    return T, order
+
+
+def run_item(T, wl, item):
+    from oracle import hps_ref as H
+    kind, x = item
+    if kind == "leaf":
+        T._leaf(x)
+    elif kind == "merge":
+        T._merge(x)
+        if x is T.root:
+            T.factored = True
+    else:
+        r = wl.rhs[x % len(wl.rhs)]
+        T.solve([H.EllipticRHS(2, r.f, r.g)])
+
+
+def timed_items(T, wl, items):
+    """(LAPACK/BLAS seconds, wall seconds) of a run of items.  The Python index loops of the
+    restatement are compiled loops in the reference, so the LAPACK/BLAS time is its CPU cost."""
+    from oracle import hps_ref as H
+    prof = [0.0, 0]
+    H.PROFILE = prof
+    t0 = time.perf_counter()
+    try:
+        for it in items:
+            run_item(T, wl, it)
+    finally:
+        H.PROFILE = None
+    return prof[0], time.perf_counter() - t0
+
+
+def cpu_full_pass(wl, nrhs, nsolves, chunks=1, on_chunk=None):
+    """The full factor plus nsolves single-RHS solves, measured (not extrapolated), in `chunks`
+    consecutive slices of the item list.  Returns per-chunk (lapack_s, wall_s) and the factor and
+    mean solve times."""
+    T, items = reference_items(wl, nsolves)
+    nf = len(items) - nsolves
+    per = [(0.0, 0.0)] * chunks
+    fac = sol = 0.0
+    walls = 0.0
+    bounds = np.linspace(0, len(items), chunks + 1).astype(int)
+    for c in range(chunks):
+        lo, hi = bounds[c], bounds[c + 1]
+        lap_f = lap_s = 0.0
+        wall = 0.0
+        # split the chunk at the factor/solve boundary to attribute the time
+        for a, b in ((lo, min(hi, nf)), (max(lo, nf), hi)):
+            if b > a:
+                lp, wl_s = timed_items(T, wl, items[a:b])
+                wall += wl_s
+                if a < nf:
+                    lap_f += lp
+                else:
+                    lap_s += lp
+        fac += lap_f
+        sol += lap_s
+        walls += wall
+        per[c] = (lap_f + lap_s, wall)
+        if on_chunk:
+            on_chunk(c)
+    return per, fac, sol / max(nsolves, 1), walls
+
+
+def cpu_sample_threads(wl, threads):
+    """LAPACK/BLAS seconds of a fixed sample (16 leaves, the deepest merge whose interface has
+    256 points with children given random maps of the true sizes, one leaf solve) at a given
+    thread count: the CPU's own thread scaling on this workload's kernels."""
+    from threadpoolctl import threadpool_limits
+    from oracle import hps_ref as H
     with threadpool_limits(limits=threads):
-        root, levels = H.build_tree(wl.L, wl.domain, 2)
-        T = H.RobinTree()
-        T.bndry_params = wl.bndry_params
-        T.opts = H.SolveOpts(h_tgt=wl.h_tgt, kb=wl.opts_kb)
-        T.ell_op = H.EllipticOperator(2, wl.domain, wl.potential)
-        T.levels = levels
-        T.keep_leaf = True
+        T = _oracle_tree(wl)
+        leaves = T.levels[-1][:16]
+        lap, _ = timed_items(T, wl, [("leaf", n) for n in leaves])
+        rng = np.random.default_rng(7)
+        for l in range(wl.L - 1, -1, -1):
+            node = T.levels[l][0]
+            kids = (node.child1, node.child2)
+            grids = [tuple(int(round(w * wl.N)) for w in (c.box[1] - c.box[0])[:2]) for c in kids]
+            cut = int(np.argmax(np.abs((node.box[1] - node.box[0]) - (kids[0].box[1] - kids[0].box[0]))[:2]))
+            if grids[0][1 - cut] >= 256:
+                break
+        for c, (ga, gb) in zip(kids, grids):
+            c.ptbox = [ga, gb, -1]
+            nbc = 2 * (ga + gb)
+            c.rtr = np.asfortranarray((rng.standard_normal((nbc, nbc)) + 1j * rng.standard_normal((nbc, nbc)))
+                                      / np.sqrt(2.0 * nbc))
         prof = [0.0, 0]
         H.PROFILE = prof
         try:
-            # leaves: FD_solve's zgetrf + zgetrs(64 RHS) on real leaves
-            nsamp = 16
-            idx = rng.choice(len(levels[-1]), nsamp, replace=False)
-            for i in idx:
-                T._leaf(levels[-1][i])
-            leaf_factor = prof[0] / nsamp
-            # leaf solves: fd_leaf_solve + fd_leaf_update = two zgetrs with one RHS
-            prof[0] = 0.0
-            for i in idx:
-                lf = levels[-1][i]
-                b = np.zeros((lf.lu.shape[0], 1), dtype=np.complex128, order="F")
-                H._getrs((lf.lu, lf.piv), b)
-                H._getrs((lf.lu, lf.piv), b)
-            leaf_solve = prof[0] / nsamp
-            a, bb = levels[-1][idx[0]].ptbox[:2]
-            total_factor = len(levels[-1]) * leaf_factor
-            total_solve = len(levels[-1]) * leaf_solve
-            # one node per merge level, children with random RtR maps of the true sizes
-            child_grid = (a, bb)
-            grids = {wl.L: child_grid}
-            for l in range(wl.L - 1, -1, -1):
-                node = levels[l][0]
-                c1, c2 = node.child1, node.child2
-                for c in (c1, c2):
-                    c.ptbox = [grids[l + 1][0], grids[l + 1][1], -1]
-                    nbc = 2 * (c.ptbox[0] + c.ptbox[1])
-                    c.rtr = np.asfortranarray((rng.standard_normal((nbc, nbc)) + 1j * rng.standard_normal((nbc, nbc)))
-                                              / np.sqrt(2.0 * nbc))
-                prof[0] = 0.0
-                T._merge(node)
-                total_factor += len(levels[l]) * prof[0]
-                grids[l] = tuple(node.ptbox[:2])
-                # node solve work of one RHS: apply_invm in both sweeps + the T_ji g_i / T_in g_n products
-                m = H.get_pt_face(c1.ptbox)[c1.iface - 1]
-                x = rng.standard_normal((m, 1)) + 0j
-                prof[0] = 0.0
-                H.apply_invm(None, None, x, x, 0.0, node.D, node.S, node.nu)
-                H.apply_invm(x, x, x, x, 1.0, node.D, node.S, node.nu)
-                for c in (c1, c2):
-                    nbc = c.rtr.shape[0]
-                    H._gemm(1.0, np.asfortranarray(c.rtr[:, :m]), x)
-                    H._gemm(1.0, np.asfortranarray(c.rtr[:m, :]), rng.standard_normal((nbc, 1)) + 0j)
-                total_solve += len(levels[l]) * prof[0]
-                c1.rtr = c2.rtr = None
-                node.rtr = None
+            T._merge(node)
+            lf = leaves[0]
+            b = np.zeros((lf.lu.shape[0], 1), dtype=np.complex128, order="F")
+            H._getrs((lf.lu, lf.piv), b)
         finally:
             H.PROFILE = None
-    return total_factor + nrhs * total_solve, total_factor, total_solve
+    return lap + prof[0]
 
 
-def cpu_baseline_block(wl, nrhs, reps):
+def cpu_model():
+    try:
+        out = subprocess.run(["lscpu"], capture_output=True, text=True, timeout=10).stdout
+        for line in out.splitlines():
+            if line.startswith("Model name"):
+                return line.split(":", 1)[1].strip()
+    except Exception:
+        pass
+    return "unknown"
+
+
+def cpu_baseline_block(wl, nrhs, nsolves=2):
     threads = os.cpu_count() or 1
-    vals = []
-    for _ in range(reps):
-        t0 = time.perf_counter()
-        step, fac, sol = cpu_reference_step_seconds(wl, nrhs, threads)
-        vals.append((step, fac, sol, time.perf_counter() - t0))
-    step, fac, sol, wall = sorted(vals)[len(vals) // 2]
+    per, fac, sol, wall = cpu_full_pass(wl, nrhs, nsolves)
+    step = fac + nrhs * sol
+    t1 = cpu_sample_threads(wl, 1)
+    tn = cpu_sample_threads(wl, threads)
     return {
         "value": nrhs / step, "unit": "RHS/s", "cores": threads, "kind": "port",
-        "factor_s": fac, "solve_s_per_rhs": sol,
-        "sample": f"LAPACK/BLAS time of the reference's call sequence (scipy OpenBLAS, {threads} threads) on "
-                  f"16 leaves, one node per merge level (random child RtR maps of the true sizes) and one-RHS "
-                  f"leaf/node solves, scaled by node counts to a full factor + {nrhs} single-RHS solves; "
-                  f"median of {reps} samples of ~{wall:.1f} s wall each",
+        "cpu": cpu_model(), "factor_s": fac, "solve_s_per_rhs": sol, "wall_s": wall,
+        "thread_scaling": {"sample_s_1_thread": t1, f"sample_s_{threads}_threads": tn, "speedup": t1 / tn},
+        "sample": f"measured on the whole workload: the full factor (every leaf and merge of the reference's "
+                  f"call sequence) and {nsolves} single-RHS solves, LAPACK/BLAS time (scipy OpenBLAS, {threads} "
+                  f"threads; the restatement's Python loops are compiled in the reference and not counted, "
+                  f"{wall:.0f} s wall); RHS/s = {nrhs} / (factor + {nrhs} x mean solve)",
     }
 
 
@@ -182,29 +273,28 @@ def reference_arm(args):
     nrhs = args.nrhs or W.CONFIGS[args.config]["nrhs"]
     wl = W.make_workload(args.config, nrhs=nrhs)
     threads = os.cpu_count() or 1
+    # warm-up: the factor of config 1's small tree, W times
+    small = W.make_workload(1)
     for _ in range(args.warmup):
-        cpu_reference_step_seconds(wl, nrhs, threads)
-    steps = []
-    t_wall = 0.0
-    for _ in range(args.steps):
-        t0 = time.perf_counter()
-        step, fac, sol = cpu_reference_step_seconds(wl, nrhs, threads)
-        t_wall += time.perf_counter() - t0
-        steps.append((step, fac, sol))
-    tot = sum(s[0] for s in steps)
-    value = nrhs * len(steps) / tot
-    ms = 1e3 * tot / len(steps)
+        T, items = reference_items(small, 1)
+        timed_items(T, small, items)
+    # timed: ONE pass over the whole workload -- full factor + 4 single-RHS solves -- cut into
+    # `steps` consecutive slices; every slice is measured
+    nsolves = 4
+    per, fac, sol, wall = cpu_full_pass(wl, nrhs, nsolves, chunks=args.steps)
+    tot = sum(p[0] for p in per)
+    value = nrhs / (fac + nrhs * sol)
     out = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "RHS/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * tot / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "complex128", "data": "synthetic (seeded)",
-        "config": config_dict(args.config, nrhs),
-        "factor_ms": 1e3 * np.mean([s[1] for s in steps]),
-        "solve_ms_per_rhs": 1e3 * np.mean([s[2] for s in steps]),
-        "cpu_baseline": {"value": value, "unit": "RHS/s", "cores": threads, "kind": "port",
-                         "sample": "each step: LAPACK/BLAS time of the reference's call sequence on 16 leaves, one "
-                                   "node per merge level and one-RHS solves, scaled by node counts to the full "
-                                   f"step ({t_wall / max(len(steps), 1):.1f} s wall per step)"},
+        "config": config_dict(args.config, nrhs, "fp64"),
+        "factor_ms": 1e3 * fac, "solve_ms_per_rhs": 1e3 * sol, "wall_s": wall,
+        "cpu_baseline": {"value": value, "unit": "RHS/s", "cores": threads, "kind": "port", "cpu": cpu_model(),
+                         "sample": f"one pass over the whole workload (full factor: every leaf and merge; then "
+                                   f"{nsolves} single-RHS solves), cut into {args.steps} consecutive measured "
+                                   f"steps; LAPACK/BLAS time of the reference's call sequence (scipy OpenBLAS, "
+                                   f"{threads} threads); RHS/s = {nrhs} / (factor + {nrhs} x mean solve)"},
         "e2e": {"value": value, "unit": "RHS/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(out), flush=True)
@@ -287,13 +377,148 @@ def zgemm_peak_tflops(torch, dev):
     return 8.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
+def _superlu_reference(wl, kv, F, G, rows):
+    """FP64 CPU solutions of the global FD system (SuperLU) for the listed right-hand sides; runs
+    in a spawned process beside the GPU measurement (one host core)."""
+    from oracle import fd_global as FG
+    S = FG.SparseFD(wl.L, wl.domain, wl.h_tgt, wl.opts_kb, wl.bndry_params, kv)
+    return [S.solve(F[r], G[r]) for r in rows]
+
+
+def _start_superlu(wl_args, kv, F, G, rows):
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    pool = ctx.Pool(1)
+    return pool, pool.apply_async(_superlu_from_args, (wl_args, kv, F[rows], G[rows]))
+
+
+def _superlu_from_args(wl_args, kv, F, G):
+    sys.path.insert(0, str(ROOT))
+    from robinsolver_b200 import workloads as W
+    wl = W.make_workload(*wl_args[0], **wl_args[1])
+    return _superlu_reference(wl, kv, F, G, range(F.shape[0]))
+
+
+class Arm:
+    """One tree of the bench workload at one precision, driven through the C-ABI."""
+
+    def __init__(self, rb, _lib, wl, precision, kv, d_k, d_f, d_g, nrhs):
+        self.lib = _lib.lib
+        self._lib = _lib
+        self.precision = precision
+        self.prec = _lib.RB_PREC_MIXED if precision == "mixed" else _lib.RB_PREC_FP64
+        # RB_FLAG_ASYNC_FACTOR: the host factor call returns once enqueued, so that the e2e step's
+        # right-hand-side upload overlaps the factor (the device-path calls are asynchronous anyway)
+        self.T = rb.robin_tree(async_factor=True)
+        self.T.bndry_params = wl.bndry_params
+        op = rb.elliptic_operator(d=2, domain=wl.domain, k=wl.potential)
+        opts = rb.solve_opts(h_tgt=wl.h_tgt, kb=wl.opts_kb)
+        self.inf = self.T.plan(wl.L, op, opts)
+        self.h = self.T.handle
+        self.kv, self.d_k, self.d_f, self.d_g, self.nrhs = kv, d_k, d_f, d_g, nrhs
+        import torch
+        self.d_u = torch.empty((nrhs, self.inf.nleaves, self.inf.leaf_n), dtype=torch.complex128, device=d_k.device)
+
+    def ck(self, code):
+        if code != 0:
+            raise RuntimeError(self._lib.last_error(self.h))
+
+    def step(self):
+        lib = self.lib
+        self.ck(lib.rb_tree_factor_device(self.h, self.d_k.data_ptr(), self.prec, 0))
+        self.ck(lib.rb_tree_solve_device(self.h, self.nrhs, self.d_f.data_ptr(), self.d_g.data_ptr(), 0))
+        self.ck(lib.rb_get_solution_device(self.h, self.d_u.data_ptr(), 0))
+
+    def stream(self, torch, dev):
+        return torch.cuda.ExternalStream(self.lib.rb_tree_stream(self.h), device=dev)
+
+    def timed(self, torch, dev, steps, warmup):
+        """Per-step ms and total ms of `steps` steps after `warmup`, CUDA events on the library's
+        stream."""
+        self.T.factor_samples(self.kv, self.precision)   # first calls allocate and build descriptors
+        F = self.d_f.cpu().numpy()
+        G = self.d_g.cpu().numpy()
+        self.T.solve_samples(F, G)
+        for _ in range(warmup):
+            self.step()
+        torch.cuda.synchronize()
+        st = self.stream(torch, dev)
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        with torch.cuda.stream(st):
+            ev[0].record(st)
+            for i in range(steps):
+                self.step()
+                ev[i + 1].record(st)
+        torch.cuda.synchronize()
+        return [ev[i].elapsed_time(ev[i + 1]) for i in range(steps)], ev[0].elapsed_time(ev[-1])
+
+    def split(self, torch, dev):
+        """(factor ms, solve ms) of one step: the factor's own device time and the solve alone."""
+        self.T.factor_samples(self.kv, self.precision)
+        self.T._update_times()
+        factor_ms = self.T.f_time * 1e3
+        st = self.stream(torch, dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(st):
+            e0.record(st)
+            self.ck(self.lib.rb_tree_solve_device(self.h, self.nrhs, self.d_f.data_ptr(), self.d_g.data_ptr(), 0))
+            e1.record(st)
+        torch.cuda.synchronize()
+        return factor_ms, e0.elapsed_time(e1)
+
+
+def roofline_block(arm, torch, dev, steps, zpeak, bf16_peak):
+    """Per-launch events over `steps` more steps: the dominant kernel family, its algorithmic
+    rate and its fraction of the peak of the pipe it runs on."""
+    arm.T.set_timing(2)
+    arm.T.clear_stage_times()
+    for _ in range(steps):
+        arm.step()
+    torch.cuda.synchronize()
+    entries = arm.T.stage_times(with_flops=True)
+    arm.T.set_timing(0)
+    per = {}
+    for name, ms, flops in entries:
+        d = per.setdefault(name, [0, 0.0, 0.0])
+        d[0] += 1
+        d[1] += ms
+        d[2] += flops
+    tot = sum(v[1] for v in per.values())
+    shares = {k: round(v[1] / tot, 4) for k, v in per.items()}
+    dname, (dcnt, dms, dflops) = max(per.items(), key=lambda kv_: kv_[1][1])
+    achieved = dflops / (dms * 1e-3) / 1e12 if dflops > 0 else None
+    # split TF32 on tcgen05: the dense TF32 rate is half the measured bf16 rate, and every complex
+    # multiply-add is 4 real ones x 3 split products: algorithmic 8mnk is a third of the executed
+    # 24mnk real tensor flops
+    tc5_peak = bf16_peak / 2.0 / 3.0 if bf16_peak else None
+    fams = {}
+    for k, v in per.items():
+        if v[2] > 0:
+            pk = tc5_peak if k == "zgemm_tc5" else zpeak
+            fams[k] = {"launches": v[0], "ms": round(v[1], 3), "tflops": round(v[2] / (v[1] * 1e-3) / 1e12, 2),
+                       "frac": round(v[2] / (v[1] * 1e-3) / 1e12 / pk, 3) if pk else None}
+    if dname == "zgemm_tc5":
+        peak, pipe, src = tc5_peak, "tf32 (tcgen05, split x3)", \
+            "MEASURED_PEAKS.json bf16_tflops / 2 (dense TF32) / 3 (split products per complex term)"
+    else:
+        peak, pipe, src = zpeak, "fp64", "complex128 cuBLAS GEMM 4096^3 measured in this run (no FP64 entry in " \
+                                         "MEASURED_PEAKS.json)"
+    return {
+        "bound": "tensor", "pipe": pipe, "kernel": dname, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+        "frac": (achieved / peak) if (achieved and peak) else None,
+        "traffic": DRAM_BYTES_PER_LAUNCH.get(dname) if arm.T.nlvls == 12 else None, "launches": dcnt, "ms_total": dms,
+        "share_of_step": shares.get(dname), "peak_source": src,
+        "flop_count": "algorithmic 8mnk per complex GEMM, 8m^3 per Gauss-Jordan inverse",
+        "families": fams, "shares": shares,
+    }
+
+
 def our_arm(args):
     import torch
 
     import robinsolver_b200 as rb
     from robinsolver_b200 import _lib
     from robinsolver_b200 import workloads as W
-
     from robinsolver_b200.replicas import Replicas
 
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -302,103 +527,69 @@ def our_arm(args):
     # replicas only: each rank runs the whole workload on its GPU; no data-path collective
     rep = Replicas("nccl", device=dev, timeout_s=300)
     world, rank = rep.world, rep.rank
-    barrier = rep.barrier
-    max_over_ranks = rep.max
 
     nrhs = args.nrhs or W.CONFIGS[args.config]["nrhs"]
     wl = W.make_workload(args.config, nrhs=nrhs)
-    # RB_FLAG_ASYNC_FACTOR: the host factor call returns once enqueued, so that the e2e step's
-    # right-hand-side upload overlaps the factor (the device-path calls are asynchronous anyway)
-    T = rb.robin_tree(async_factor=True)
-    T.bndry_params = wl.bndry_params
-    op = rb.elliptic_operator(d=2, domain=wl.domain, k=wl.potential)
-    opts = rb.solve_opts(h_tgt=wl.h_tgt, kb=wl.opts_kb)
-    inf = T.plan(wl.L, op, opts)
-    kv = np.ascontiguousarray(wl.potential(T.sample_points(_lib.RB_POINTS_POTENTIAL)))
-    rhs = [rb.elliptic_rhs(d=2, f=r.f, g=[rb.bndry_rhs(g) for g in r.g]) for r in wl.rhs]
-    F, G = T.sample_rhs(rhs)
+    Tp = rb.robin_tree()
+    Tp.bndry_params = wl.bndry_params
+    inf = Tp.plan(wl.L, rb.elliptic_operator(d=2, domain=wl.domain, k=wl.potential),
+                  rb.solve_opts(h_tgt=wl.h_tgt, kb=wl.opts_kb))
+    kv = np.ascontiguousarray(wl.potential(Tp.sample_points(_lib.RB_POINTS_POTENTIAL)))
+    F, G = Tp.sample_rhs([rb.elliptic_rhs(d=2, f=r.f, g=[rb.bndry_rhs(g) for g in r.g]) for r in wl.rhs])
+    Tp.close()
     nleaf, nper = inf.nleaves, inf.leaf_n
-    # device-resident inputs/outputs for `value`
+
+    # the FP64 CPU solve of the same FD system for the forward errors, beside the GPU work
+    check_rows = [0, nrhs - 1] if nrhs > 1 else [0]
+    superlu = None
+    if rank == 0 and not args.no_forward_error:
+        superlu = _start_superlu(((args.config,), {"nrhs": nrhs}), kv.reshape(nleaf, -1), F, G, check_rows)
+
     d_k = torch.from_numpy(kv).to(dev)
     d_f = torch.from_numpy(F).to(dev)
     d_g = torch.from_numpy(G).to(dev)
-    d_u = torch.empty((nrhs, nleaf, nper), dtype=torch.complex128, device=dev)
-    lib = _lib.lib
-    h = T.handle
+    main = args.precision
+    other = "fp64" if main == "mixed" else "mixed"
+    arms = {p: Arm(rb, _lib, wl, p, kv, d_k, d_f, d_g, nrhs) for p in (main, other)}
 
-    def ck(code):
-        if code != 0:
-            raise RuntimeError(_lib.last_error(h))
-
-    def device_step():
-        ck(lib.rb_tree_factor_device(h, d_k.data_ptr(), _lib.RB_PREC_FP64, 0))
-        ck(lib.rb_tree_solve_device(h, nrhs, d_f.data_ptr(), d_g.data_ptr(), 0))
-        ck(lib.rb_get_solution_device(h, d_u.data_ptr(), 0))
-
-    # first call allocates and builds the launch descriptors
-    T.factor_samples(kv)
-    T.solve_samples(F, G)
-    stream = torch.cuda.ExternalStream(lib.rb_tree_stream(h), device=dev)
-    for _ in range(args.warmup):
-        device_step()
-    torch.cuda.synchronize()
-
-    # ---- timed region: value -----------------------------------------------------------------
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    # ---- timed regions: the headline precision, then the other one --------------------------------
+    res = {}
     clocks = ClockSampler(local)
-    barrier()
-    torch.cuda.synchronize()
-    clocks.start()
-    fl0 = sl0 = 0
-    launches = 0
-    with torch.cuda.stream(stream):
-        ev[0].record(stream)
-        for i in range(args.steps):
-            device_step()
-            ev[i + 1].record(stream)
-    torch.cuda.synchronize()
-    barrier()
-    clk = clocks.stop()
-    fl, sl = T.launch_counts()
-    launches = (fl + sl) * args.steps
-    step_ms = [ev[i].elapsed_time(ev[i + 1]) for i in range(args.steps)]
-    value, total_ms = rep.rate(nrhs * args.steps, ev[0].elapsed_time(ev[-1]))
+    for p in (main, other):
+        rep.barrier()
+        torch.cuda.synchronize()
+        if p == main:
+            clocks.start()
+        step_ms, tot_ms = arms[p].timed(torch, dev, args.steps, args.warmup)
+        rep.barrier()
+        if p == main:
+            clk = clocks.stop()
+        value, total_ms = rep.rate(nrhs * args.steps, tot_ms)
+        fl, sl = arms[p].T.launch_counts()
+        fms, sms = arms[p].split(torch, dev)
+        res[p] = {"value": value, "total_ms": total_ms, "step_ms": step_ms, "launches": (fl + sl) * args.steps,
+                  "factor_ms": fms, "solve_ms": sms}
 
-    # factor / solve split from the library's own events on the last step
-    T.factor_samples(kv)
-    T._update_times()                # waits for the (asynchronous) factor and takes its time
-    factor_ms = T.f_time * 1e3
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    with torch.cuda.stream(stream):
-        e0.record(stream)
-        ck(lib.rb_tree_solve_device(h, nrhs, d_f.data_ptr(), d_g.data_ptr(), 0))
-        e1.record(stream)
-    torch.cuda.synchronize()
-    solve_ms = e0.elapsed_time(e1)
+    # ---- accuracy: mixed vs FP64 GPU on every right-hand side, both vs the FP64 CPU solve ------------
+    U = {p: arms[p].d_u.cpu().numpy() for p in arms}
+    mix_vs_fp64 = [float(np.abs(U["mixed"][r] - U["fp64"][r]).max() / np.abs(U["fp64"][r]).max())
+                   for r in range(nrhs)]
+    it, rho, est, resid = arms["mixed"].T.refine_info()
 
-    # ---- roofline: per-launch events over the same steps ----------------------------------------
-    T.set_timing(2)
-    T.clear_stage_times()
-    for _ in range(args.steps):
-        device_step()
-    torch.cuda.synchronize()
-    entries = T.stage_times(with_flops=True)
-    T.set_timing(0)
-    per = {}
-    for name, ms, flops in entries:
-        d = per.setdefault(name, [0, 0.0, 0.0])
-        d[0] += 1
-        d[1] += ms
-        d[2] += flops
-    dom = max(per.items(), key=lambda kv_: kv_[1][1])
-    peak = zgemm_peak_tflops(torch, dev)
-    dname, (dcnt, dms, dflops) = dom
-    achieved = dflops / (dms * 1e-3) / 1e12 if dflops > 0 else None
-    shares = {k: round(v[1] / sum(x[1] for x in per.values()), 4) for k, v in per.items()}
+    # ---- roofline of the headline precision ---------------------------------------------------------
+    zpeak = zgemm_peak_tflops(torch, dev)
+    peaks = {}
+    try:
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+    except Exception:
+        pass
+    roof = roofline_block(arms[main], torch, dev, args.steps, zpeak, peaks.get("bf16_tflops"))
 
-    # ---- e2e through the host C-ABI ---------------------------------------------------------------
+    # ---- e2e through the host C-ABI ---------------------------------------------------------------------
     e2e = None
     if not args.no_e2e:
+        arm = arms[main]
+        lib, h = arm.lib, arm.h
         pk = torch.from_numpy(kv).pin_memory()
         pf = torch.from_numpy(F).pin_memory()
         pg = torch.from_numpy(G).pin_memory()
@@ -407,78 +598,237 @@ def our_arm(args):
         u_ptrs = [_lib.C.cast(pu[r].data_ptr(), _lib.C.POINTER(_lib.C.c_double)) for r in range(nrhs)]
 
         def host_step():
-            ck(lib.rb_tree_factor(h, pk_p, _lib.RB_PREC_FP64))
-            ck(lib.rb_tree_solve(h, nrhs, pf_p, pg_p))
+            arm.ck(lib.rb_tree_factor(h, pk_p, arm.prec))
+            arm.ck(lib.rb_tree_solve(h, nrhs, pf_p, pg_p))
             for r in range(nrhs):
-                ck(lib.rb_get_solution(h, r, u_ptrs[r], None))
+                arm.ck(lib.rb_get_solution(h, r, u_ptrs[r], None))
 
         for _ in range(max(1, args.warmup)):
             host_step()
-        barrier()
+        rep.barrier()
         torch.cuda.synchronize()
+        st = arm.stream(torch, dev)
         t0 = time.perf_counter()
         a0 = torch.cuda.Event(enable_timing=True)
         a1 = torch.cuda.Event(enable_timing=True)
-        a0.record(stream)
+        a0.record(st)
         for _ in range(args.steps):
             host_step()
-        a1.record(stream)
+        a1.record(st)
         torch.cuda.synchronize()
         wall = time.perf_counter() - t0
-        e2e_ms = max_over_ranks(max(a0.elapsed_time(a1), wall * 1e3))
+        e2e_ms = rep.max(max(a0.elapsed_time(a1), wall * 1e3))
         e2e = {"value": world * nrhs * args.steps / (e2e_ms * 1e-3), "unit": "RHS/s",
                "calls": "rb_tree_factor (RB_FLAG_ASYNC_FACTOR), rb_tree_solve, rb_get_solution per RHS; "
-                        "pinned host buffers",
+                        "pinned host buffers", "precision": main,
                "h2d_bytes_per_step": int(kv.nbytes + F.nbytes + G.nbytes),
                "d2h_bytes_per_step": int(pu.numel() * 16)}
-        # the solution the user read back: backward error of two right-hand sides
-        from oracle import fd_global as FG
-        bw = max(FG.backward_error(wl.L, wl.domain, wl.h_tgt, wl.opts_kb, wl.bndry_params, kv.reshape(nleaf, -1),
-                                   pu[r].numpy(), F[r].reshape(nleaf, -1), G[r]) for r in (0, nrhs - 1))
+        U_e2e = pu.numpy().copy()
     else:
-        bw = None
+        U_e2e = U[main]
+
+    # backward error of the solutions the user read back; forward errors against SuperLU
+    from oracle import fd_global as FG
+    bw = max(FG.backward_error(wl.L, wl.domain, wl.h_tgt, wl.opts_kb, wl.bndry_params, kv.reshape(nleaf, -1),
+                               U_e2e[r], F[r].reshape(nleaf, -1), G[r]) for r in check_rows)
+    fwd = None
+    if superlu is not None:
+        pool, job = superlu
+        ref = job.get(timeout=1800)
+        pool.close()
+        pool.join()
+        fwd = {p: max(FG.forward_error(U[p][r], ref[i]) for i, r in enumerate(check_rows)) for p in U}
+        fwd["rhs_checked"] = check_rows
+        fwd["reference"] = "SuperLU solve of the assembled global FD system (oracle/fd_global.SparseFD), FP64, CPU"
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_block(wl, nrhs, reps=3)
+        cpu = cpu_baseline_block(wl, nrhs)
 
     if rank == 0:
+        r0, r1 = res[main], res[other]
         out = {
-            "metric": METRIC, "value": value, "unit": "RHS/s", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "complex128",
+            "metric": METRIC, "value": r0["value"], "unit": "RHS/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": r0["total_ms"] / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "complex128" if main == "fp64" else
+            "complex128 storage; tf32x3 tensor-core GEMMs on levels 2-6, fp64 elsewhere",
             "data": "synthetic (seeded potential and plane waves, no dataset)",
-            "config": config_dict(args.config, nrhs),
-            "factor_ms": factor_ms, "solve_ms": solve_ms,
-            "solves_per_s_resident": nrhs / (solve_ms * 1e-3),
-            "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99)),
-            "backward_error": bw,
-            "roofline": {
-                "bound": "tensor", "pipe": "fp64", "kernel": dname, "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None,
-                "traffic": DRAM_BYTES_PER_LAUNCH.get(args.config, {}).get(dname),
-                "launches": dcnt, "ms_total": dms, "share_of_step": shares.get(dname),
-                "flop_count": "algorithmic 8mnk per complex GEMM (the tensor-core kernel issues three real "
-                              "MMAs per complex product, so achieved can exceed a four-product peak)",
-                # the MMA pipe's own work is 6mnk of the 8mnk counted: its busy fraction
-                "executed_frac": (0.75 * achieved / peak) if achieved else None,
-                "peak_source": "complex128 cuBLAS GEMM 4096^3 measured in this run (no FP64 entry in "
-                               "MEASURED_PEAKS.json)",
-                "shares": shares,
-            },
-            "cpu_baseline": cpu,
-            "e2e": e2e,
-            "gpu_launches": int(launches),
-            "clocks": clk,
+            "config": config_dict(args.config, nrhs, main),
+            "factor_ms": r0["factor_ms"], "solve_ms": r0["solve_ms"],
+            "solves_per_s_resident": nrhs / (r0["solve_ms"] * 1e-3),
+            "p50_ms": float(np.percentile(r0["step_ms"], 50)), "p99_ms": float(np.percentile(r0["step_ms"], 99)),
+            other: {"value": r1["value"], "ms_per_step": r1["total_ms"] / args.steps, "factor_ms": r1["factor_ms"],
+                    "solve_ms": r1["solve_ms"], "solves_per_s_resident": nrhs / (r1["solve_ms"] * 1e-3)},
+            "mixed_vs_fp64": {
+                "step_speedup": res["fp64"]["total_ms"] / res["mixed"]["total_ms"],
+                "factor_speedup": res["fp64"]["factor_ms"] / res["mixed"]["factor_ms"],
+                "solve_speedup": res["fp64"]["solve_ms"] / res["mixed"]["solve_ms"],
+                "max_rel_err_all_rhs": max(mix_vs_fp64), "refine_corrections": it, "contraction": rho,
+                "estimated_error": est, "residual": resid},
+            "backward_error": bw, "forward_error": fwd,
+            "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
+            "gpu_launches": int(r0["launches"]), "clocks": clk,
         }
         print(json.dumps(out), flush=True)
-    T.close()
+    for a in arms.values():
+        a.T.close()
     rep.close()
+    return 0
+
+
+# ------------------------------------------------------------------------------------------------
+# Serving: resident trees, a Poisson stream of solve requests and refactors (rb_server_*)
+# ------------------------------------------------------------------------------------------------
+
+SERVE_GRIDS = [(256, 6), (384, 8), (512, 8), (768, 10), (1024, 12)]
+
+
+def serve_trees(seed=5000, ntrees=8):
+    """8 trees with grids drawn from {256^2 (L6), 384^2 (L8), 512^2 (L8), 768^2 (L10), 1024^2 (L12)},
+    kb ~ U(50, 200) and seeded 40-bump potentials with 0.005i kb damping."""
+    from robinsolver_b200 import workloads as W
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(ntrees):
+        N, L = SERVE_GRIDS[int(rng.integers(len(SERVE_GRIDS)))]
+        kb = float(rng.uniform(50.0, 200.0))
+        out.append(W.make_workload(2, instance=100 + i, N=N, L=L, kb=kb, nbumps=40, delta=0.005, nrhs=0))
+    return out
+
+
+def _bump_params(wl, rng=None):
+    pot = wl.potential
+    if rng is None:
+        cs, amps = pot.centres, pot.amps
+    else:
+        cs = rng.uniform(0.2, 0.8, size=pot.centres.shape)
+        amps = rng.uniform(-1.0, 1.0, size=pot.amps.shape)
+    return (pot.kb, pot.delta, pot.width, [(c[0], c[1], a) for c, a in zip(cs, amps)])
+
+
+def serve_stream(srv, trees, tids, requests, rate_rhs, rng, nfactor, bufs, collect, max_rhs=64):
+    """Submits `requests` solve requests (1..max_rhs RHS, point sources or plane waves sampled on
+    the device) at Poisson arrivals of rate_rhs right-hand sides per second, with nfactor refactors
+    (new seeded potentials) spread through the stream; returns once every request completed.
+    Each tree has a few pinned output buffers: a request waits for a free one (its latency still
+    counts from its scheduled arrival)."""
+    import queue
+    from robinsolver_b200 import _lib
+    sizes = rng.integers(1, max_rhs + 1, size=requests)
+    mean_rhs = float(sizes.mean())
+    gaps = rng.exponential(mean_rhs / rate_rhs, size=requests)
+    which = rng.integers(len(trees), size=requests)
+    kinds = rng.integers(2, size=requests)
+    fac_at = set(np.linspace(0, requests - 1, nfactor + 2).astype(int)[1:-1].tolist()) if nfactor else set()
+    pending = [[] for _ in trees]          # per tree, in submission order: (request, buffer)
+
+    def release(i, block):
+        while pending[i]:
+            rr, b = pending[i][0]
+            if not srv.wait(rr, -1.0 if block else 0.0):
+                return
+            pending[i].pop(0)
+            if b is not None:
+                bufs[i].put(b)
+            if block:
+                return
+
+    t0 = srv.now()
+    arrival = t0
+    for q in range(requests):
+        arrival += gaps[q]
+        while srv.now() < arrival:
+            dt = arrival - srv.now()
+            if dt > 2e-4:
+                time.sleep(dt - 1e-4)
+        ti = int(which[q])
+        wl = trees[ti]
+        if q in fac_at:
+            pending[ti].append((srv.submit_factor(tids[ti], bumps=_bump_params(wl, rng), arrival=arrival), None))
+        nr = int(sizes[q])
+        if kinds[q] == 0:
+            par = np.stack([rng.uniform(0.1, 0.9, nr), rng.uniform(0.1, 0.9, nr), np.full(nr, 0.05)], axis=1)
+            field = _lib.RB_FIELD_POINT_SOURCE
+        else:
+            th = rng.uniform(0.0, 2 * np.pi, nr)
+            par = np.stack([np.full(nr, wl.kb), np.cos(th), np.sin(th)], axis=1)
+            field = _lib.RB_FIELD_PLANE_WAVE
+        while True:
+            try:
+                buf = bufs[ti].get_nowait()
+                break
+            except queue.Empty:
+                release(ti, True)
+        pending[ti].append((srv.submit_solve(tids[ti], nr, field=field, params=par, u=buf[:nr * collect[ti]],
+                                             arrival=arrival), buf))
+        for i in range(len(trees)):
+            release(i, False)
+    for i in range(len(trees)):
+        while pending[i]:
+            release(i, True)
+    return srv.now() - t0
+
+
+def serve_arm(args):
+    import queue
+
+    import torch
+
+    import robinsolver_b200 as rb
+    from robinsolver_b200 import _lib
+
+    torch.cuda.set_device(0)
+    trees = serve_trees()
+    out = {"metric": "serving: solve latency p50/p99 (arrival -> solution in host memory) and RHS/s, "
+                     "8 resident trees, Poisson stream", "unit": "ms", "requests": args.requests}
+    for prec in ("mixed", "fp64"):
+        srv = rb.robin_server(max_batch_rhs=64, precision=prec, tol=1e-10)
+        tids = []
+        for wl in trees:
+            tids.append(srv.add_tree(wl.L, rb.elliptic_operator(d=2, domain=wl.domain, k=wl.potential),
+                                     rb.solve_opts(h_tgt=wl.h_tgt, kb=wl.opts_kb), wl.bndry_params))
+        per = []
+        for t in tids:
+            inf = srv.tree_info(t)
+            per.append(inf.nleaves * inf.leaf_n)
+        reqs = [srv.submit_factor(t, bumps=_bump_params(wl)) for t, wl in zip(tids, trees)]
+        for r in reqs:
+            srv.wait(r)
+        # pinned output buffers: 3 per tree of 64 right-hand sides
+        bufs = []
+        for p in per:
+            qq = queue.Queue()
+            for _ in range(3):
+                qq.put(torch.empty(64 * p, dtype=torch.complex128).pin_memory().numpy())
+            bufs.append(qq)
+        srv.stats(reset=True)
+        rng = np.random.default_rng(777)
+        # saturation: a closed burst of requests submitted at once
+        dur = serve_stream(srv, trees, tids, max(50, args.requests // 10), 1e9, rng, 0, bufs, per)
+        st = srv.stats(reset=True)
+        sat = st["rhs"] / dur
+        res = {"saturated_rhs_per_s": sat, "saturation_burst": {k: st[k] for k in ("solves", "rhs", "batches")}}
+        for load in (0.5, 0.9):
+            rng = np.random.default_rng(int(load * 1000))
+            dur = serve_stream(srv, trees, tids, args.requests, load * sat, rng, 20, bufs, per)
+            st = srv.stats(reset=True)
+            res[f"load_{load}"] = {"offered_rhs_per_s": load * sat, "rhs_per_s": st["rhs"] / dur,
+                                   "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
+                                   "max_ms": st["max_ms"], "solves": st["solves"], "batches": st["batches"],
+                                   "factors": st["factors"], "factor_p50_ms": st["factor_p50_ms"],
+                                   "failed": st["failed"], "duration_s": dur}
+        res["reserved_gb"] = st["reserved_bytes"] / 1e9
+        out[prec] = res
+        srv.close()
+    out["trees"] = [f"{wl.N}^2 L={wl.L} kb={wl.kb:.1f}" for wl in trees]
+    print(json.dumps(out), flush=True)
     return 0
 
 
 def main():
     args = parse()
+    if args.serve:
+        return serve_arm(args)
     if args.impl == "reference":
         return reference_arm(args)
     return our_arm(args)

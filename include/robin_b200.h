@@ -266,6 +266,33 @@ int rb_tree_refine_info(const rb_tree* tree, int32_t* iters, double* contraction
 /* Number of this library's kernels launched by the last factor and the last solve. */
 int rb_tree_launch_counts(const rb_tree* tree, int64_t* factor_launches, int64_t* solve_launches);
 
+/* ---- forests: many trees factored in one level-synchronous schedule ---------------------------
+ *
+ * No counterpart in the reference, which factors one tree by a serial recursion (compute_RTR,
+ * robin_tree_module.f90:375-401).  A forest references existing trees (created with
+ * rb_tree_create, any sizes, single-inversion K-form merges; still owned by the caller) and factors
+ * them together: aligned by height above their leaves, every merge stage of a height runs as ONE
+ * launch over the concatenated descriptors of all trees (uneven interface lengths in one launch),
+ * with one Gauss-Jordan launch per distinct interface size; the schedule is captured into a CUDA
+ * graph and replayed.  A project autotuner (autotune != 0 on a factor call) times each applicable
+ * FP64 GEMM tile shape on every concatenated stage once, keeps the fastest, and caches the choices
+ * for the process by stage shape.  After rb_forest_factor every tree is factored (FP64) and is
+ * solved with rb_tree_solve as usual. */
+typedef struct rb_forest rb_forest;
+int rb_forest_create(rb_tree* const* trees, int ntrees, rb_forest** out);
+int rb_forest_destroy(rb_forest* forest);
+const char* rb_forest_last_error(const rb_forest* forest);
+/* d_k[i]: device array of tree i's potential samples (n_interior complex at RB_POINTS_POTENTIAL).
+ * Blocks until the factorizations are done; sets every tree's f_time to the forest's time. */
+int rb_forest_factor(rb_forest* forest, const double* const* d_k, int autotune);
+/* Device time of the last forest factor, the launches of its schedule, and the stages whose tile
+ * shape the autotuner fixed (any output pointer may be NULL). */
+int rb_forest_info(const rb_forest* forest, double* f_time, int64_t* launches, int32_t* tuned_stages);
+/* The autotuner's measurements: min(n, count) entries of (height, stage 0..4 = K, B1, Y1, Y2, parent
+ * map, engine id, ms per launch); returns the count.  rb_gemm_engine_name names an engine id. */
+int rb_forest_tuning(const rb_forest* forest, int32_t* height, int32_t* stage, int32_t* engine, double* ms, int n);
+const char* rb_gemm_engine_name(int engine);
+
 /* ---- serving: resident factorized trees and a continuously batched request loop ---------------
  *
  * No counterpart in the reference, which factors one tree and solves one right-hand side per call,

@@ -7,7 +7,7 @@ The API names load the shared library on first use (``robinsolver_b200.build`` a
 ``robinsolver_b200.workloads`` do not need it).
 """
 _API = ("RobinSolverError", "bndry_rhs", "check_solution", "debug_opts", "elliptic_operator", "elliptic_rhs",
-        "get_solution", "leaf_solution", "robin_server", "robin_tree", "scalar_callback", "solve_opts")
+        "get_solution", "leaf_solution", "robin_forest", "robin_server", "robin_tree", "scalar_callback", "solve_opts")
 
 __all__ = list(_API)
 

@@ -52,6 +52,8 @@ EXPORTS = [
     "rb_tree_set_refinement", "rb_tree_refine_info",
     "rb_server_create", "rb_server_destroy", "rb_server_last_error", "rb_server_now", "rb_server_add_tree",
     "rb_server_tree_info", "rb_server_submit_factor", "rb_server_submit_solve", "rb_server_wait", "rb_server_get_stats",
+    "rb_forest_create", "rb_forest_destroy", "rb_forest_last_error", "rb_forest_factor", "rb_forest_info",
+    "rb_forest_tuning", "rb_gemm_engine_name",
 ]
 
 
@@ -151,6 +153,14 @@ def _load():
                                              C.POINTER(C.c_int64)]),
         "rb_server_wait": (C.c_int, [P, C.c_int64, C.c_double]),
         "rb_server_get_stats": (C.c_int, [P, C.POINTER(rb_server_stats), C.c_int]),
+        "rb_forest_create": (C.c_int, [C.POINTER(P), C.c_int, C.POINTER(P)]),
+        "rb_forest_destroy": (C.c_int, [P]),
+        "rb_forest_last_error": (C.c_char_p, [P]),
+        "rb_forest_factor": (C.c_int, [P, C.POINTER(P), C.c_int]),
+        "rb_forest_info": (C.c_int, [P, D, C.POINTER(C.c_int64), C.POINTER(C.c_int32)]),
+        "rb_forest_tuning": (C.c_int, [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32), D,
+                                       C.c_int]),
+        "rb_gemm_engine_name": (C.c_char_p, [C.c_int]),
         # test hook of the GEMM engines (rb_testing.cpp), not part of the drop-in boundary
         "rb_test_zgemm": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_longlong, C.c_longlong, P,
                                     C.c_longlong, C.c_longlong, P, C.c_longlong, C.c_longlong, C.c_double,

@@ -498,3 +498,56 @@ class robin_server:
         st = _lib.rb_server_stats()
         self._err(lib.rb_server_get_stats(self._h, _lib.C.byref(st), 1 if reset else 0))
         return {name: getattr(st, name) for name, _ in st._fields_}
+
+
+class robin_forest:
+    """Several robin_tree handles factored together in one level-synchronous schedule with
+    autotuned GEMM tile shapes (rb_forest_*; no counterpart in the reference).  The trees must be
+    planned (``robin_tree.plan``); after ``factor`` each is factored and solves as usual."""
+
+    def __init__(self, trees):
+        self.trees = list(trees)
+        arr = (_lib.C.c_void_p * len(self.trees))(*[t.handle for t in self.trees])
+        h = _lib.C.c_void_p()
+        _check(lib.rb_forest_create(arr, len(self.trees), _lib.C.byref(h)))
+        self._h = h
+
+    def _err(self, code):
+        if code != _lib.RB_OK:
+            msg = lib.rb_forest_last_error(self._h)
+            raise RobinSolverError(code, msg.decode() if msg else "")
+
+    def factor(self, d_k_ptrs, autotune: bool = True):
+        """d_k_ptrs: device addresses of each tree's potential samples (e.g. tensor.data_ptr())."""
+        arr = (_lib.C.c_void_p * len(self.trees))(*[int(p) for p in d_k_ptrs])
+        self._err(lib.rb_forest_factor(self._h, arr, 1 if autotune else 0))
+        for t in self.trees:
+            t.factored = True
+            t._info = t.info()
+
+    def info(self):
+        f = _lib.C.c_double()
+        n = _lib.C.c_int64()
+        tu = _lib.C.c_int32()
+        self._err(lib.rb_forest_info(self._h, _lib.C.byref(f), _lib.C.byref(n), _lib.C.byref(tu)))
+        return {"f_time": f.value, "launches": n.value, "tuned_stages": tu.value}
+
+    def tuning(self):
+        n = lib.rb_forest_tuning(self._h, None, None, None, None, 0)
+        h = (_lib.C.c_int32 * max(n, 1))()
+        st = (_lib.C.c_int32 * max(n, 1))()
+        en = (_lib.C.c_int32 * max(n, 1))()
+        ms = (_lib.C.c_double * max(n, 1))()
+        lib.rb_forest_tuning(self._h, h, st, en, ms, n)
+        return [(h[i], st[i], lib.rb_gemm_engine_name(en[i]).decode(), ms[i]) for i in range(n)]
+
+    def close(self):
+        if self._h is not None:
+            lib.rb_forest_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

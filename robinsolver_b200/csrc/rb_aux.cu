@@ -2,6 +2,8 @@
 //
 // The merge helpers form the interface matrices D and S of compute_RTR; the sweep helpers move
 // boundary data between a node and its children.
+#include <algorithm>
+
 #include "rb_kernels.h"
 
 namespace rb {
@@ -60,6 +62,34 @@ __global__ void merge_form_k_kernel(int m, z nu2, z* __restrict__ dst) {
 cudaError_t merge_form_k(int nnodes, int m, z nu, z* dst, cudaStream_t s) {
     dim3 grid((m * m + 255) / 256, nnodes);
     merge_form_k_kernel<<<grid, 256, 0, s>>>(m, zmul(nu, nu), dst);
+    note_launch();
+    return cudaGetLastError();
+}
+
+// One node of a batched K-form merge (several trees, several levels): A2 = zeta I - T2_ii,
+// A1 = zeta I - T1_ii, K = nu^2 I, each m x m.
+__global__ void merge_form_kform_kernel(const MergeFormDesc* __restrict__ descs) {
+    const MergeFormDesc d = descs[blockIdx.y];
+    const int m = d.m;
+    for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < m * m; idx += gridDim.x * blockDim.x) {
+        const int r = idx % m, q = idx / m;
+        z a2 = zneg(d.t2[(d.o2 + r) + (long long)(d.o2 + q) * d.ld]);
+        z a1 = zneg(d.t1[(d.o1 + r) + (long long)(d.o1 + q) * d.ld]);
+        if (r == q) {
+            a2 = zadd(a2, d.zeta);
+            a1 = zadd(a1, d.zeta);
+        }
+        d.a2[idx] = a2;
+        d.a1[idx] = a1;
+        d.k[idx] = r == q ? d.nu2 : zmk(0.0, 0.0);
+    }
+}
+
+cudaError_t merge_form_kform_batch(const MergeFormDesc* d_descs, int count, int max_m, cudaStream_t s) {
+    if (count <= 0) return cudaSuccess;
+    if (count > 65535) return cudaErrorInvalidValue;
+    const int bx = std::min((max_m * max_m + 255) / 256, 64);
+    merge_form_kform_kernel<<<dim3(bx, count), 256, 0, s>>>(d_descs);
     note_launch();
     return cudaGetLastError();
 }

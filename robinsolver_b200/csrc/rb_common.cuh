@@ -112,6 +112,13 @@ struct GemmBatch {
     // every problem's k runs contiguously through both operands (gemm_k_contiguous), so operand
     // copies may advance by a fixed stride per k-tile
     bool kcontig = false;
+    // split-K of the same batch on the tcgen05 kernel (128-row tiles): t5_ksplit ranges of
+    // t5_kchunk, raw sums in `work` (t5_pstride elements per range and problem, ld max_m)
+    int t5_ksplit = 1;
+    int t5_kchunk = 0;
+    long long t5_pstride = 0;
+    // FP64 engine (tile shape) chosen by an autotuner; -1: the launcher's own rule
+    int engine = -1;
 };
 
 // A(i, k) sits at A.p[row(i) + k * A.ld] and B(k, j) at B.p[k + col(j) * B.ld] for every k < K:

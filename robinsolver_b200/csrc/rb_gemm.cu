@@ -263,6 +263,7 @@ static cudaError_t launch_split(const GemmBatch& b, cudaStream_t s) {
 enum class GemmShape { Dfma16, Dfma32, Dmma32, Dmma64, DmmaKc64, DmmaFixed, Dfma128x64, Dfma64 };
 static GemmShape gemm_shape(const GemmBatch& b) {
     const int mm = b.max_m, nn = b.max_n;
+    if (b.engine >= 0 && !b.fixed_order) return static_cast<GemmShape>(b.engine);
     // fixed-order batches (the solve) on the tensor cores: one tile shape, split-K planned from
     // count, m and k only; an element's sum runs over k in MMA steps of 4 in order whatever n is
     if (use_dmma() && b.fixed_order) return GemmShape::DmmaFixed;
@@ -315,6 +316,43 @@ long long gemm_plan_split(GemmBatch& b) {
     }
     b.pstride = (long long)b.max_m * b.max_n;
     return (long long)b.count * b.ksplit * b.pstride;
+}
+
+cudaError_t launch_gemm_reduce(const GemmBatch& b, int ksplit, long long pstride, cudaStream_t s) {
+    const long long elems = (long long)b.max_m * b.max_n;
+    if (b.count > 65535) return cudaErrorInvalidValue;
+    zgemm_reduce_kernel<<<dim3((unsigned)((elems + 255) / 256), b.count), 256, 0, s>>>(b.d_desc, b.work, pstride,
+                                                                                     b.max_m, ksplit);
+    note_launch();
+    return cudaGetLastError();
+}
+
+int gemm_engine_candidates(const GemmBatch& b, int* out) {
+    int n = 0;
+    if (b.fixed_order) return 0;
+    out[n++] = (int)GemmShape::Dfma32;
+    out[n++] = (int)GemmShape::Dfma64;
+    if (use_dmma()) {
+        out[n++] = (int)GemmShape::Dmma32;
+        out[n++] = (int)GemmShape::Dmma64;
+        if (b.kcontig) out[n++] = (int)GemmShape::DmmaKc64;
+    }
+    if (b.max_m >= 128) out[n++] = (int)GemmShape::Dfma128x64;
+    return n;
+}
+
+const char* gemm_engine_name(int e) {
+    switch (static_cast<GemmShape>(e)) {
+        case GemmShape::Dfma16: return "dfma16";
+        case GemmShape::Dfma32: return "dfma32";
+        case GemmShape::Dmma32: return "dmma32";
+        case GemmShape::Dmma64: return "dmma64";
+        case GemmShape::DmmaKc64: return "dmma_kc64";
+        case GemmShape::DmmaFixed: return "dmma_fixed";
+        case GemmShape::Dfma128x64: return "dfma128x64";
+        case GemmShape::Dfma64: return "dfma64";
+    }
+    return "?";
 }
 
 const char* gemm_stage_name(const GemmBatch& b) {

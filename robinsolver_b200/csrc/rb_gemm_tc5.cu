@@ -24,6 +24,7 @@
 // Every mbarrier wait is bounded (RB_TC5_WAIT_NS on the global timer).  A wait that runs out sets
 // RB_TC5_TIMEOUT in the status word, the CTA stops issuing work, waits (bounded) for the MMAs it
 // issued, frees its tensor memory and returns.
+#include <algorithm>
 #include <cstdint>
 
 #include "rb_kernels.h"
@@ -167,8 +168,12 @@ struct Tc5Regs {
 
 }  // namespace
 
+// Split-K (part != nullptr): blockIdx.z takes k in [z * kchunk, (z + 1) * kchunk) and writes its raw
+// sums to part + (problem * ksplit + z) * pstride + i + j * ldp; the reduction kernel finishes.
 template <int BN>
-__global__ void __launch_bounds__(TC5_THREADS, 1) zgemm_tc5_kernel(const GemmDesc* __restrict__ descs, int* status) {
+__global__ void __launch_bounds__(TC5_THREADS, 1) zgemm_tc5_kernel(const GemmDesc* __restrict__ descs, int* status,
+                                                                  int kchunk, z* part, long long pstride, int ldp,
+                                                                  int ksplit) {
     using Cfg = Tc5Cfg<BN>;
     using U = Tc5Units<BN>;
     extern __shared__ __align__(1024) unsigned char tc5_smem[];
@@ -186,10 +191,23 @@ __global__ void __launch_bounds__(TC5_THREADS, 1) zgemm_tc5_kernel(const GemmDes
         for (int w = tid; w < (int)(sizeof(GemmDesc) / 8); w += TC5_THREADS) dst[w] = src[w];
     }
     __syncthreads();
-    const int m = sd.m, n = sd.n, K = sd.k;
+    const int m = sd.m, n = sd.n;
+    const int kbeg = part ? (int)blockIdx.z * kchunk : 0;
+    const int K = part ? min(sd.k, kbeg + kchunk) : sd.k;             // this CTA's k runs over [kbeg, K)
     const int tiles_m = (m + TC5_BM - 1) / TC5_BM;
     const int tiles_n = (n + BN - 1) / BN;
-    if ((int)blockIdx.x >= tiles_m * tiles_n || K <= 0) return;      // uniform over the CTA
+    if ((int)blockIdx.x >= tiles_m * tiles_n || K <= kbeg) {
+        // nothing to sum: a split range past this problem's k still owes its share of zeros
+        if (part && (int)blockIdx.x < tiles_m * tiles_n) {
+            const int m0 = (blockIdx.x % tiles_m) * TC5_BM, n0 = (blockIdx.x / tiles_m) * BN;
+            z* pp = part + ((long long)blockIdx.y * ksplit + blockIdx.z) * pstride;
+            for (int e = threadIdx.x; e < TC5_BM * BN; e += TC5_THREADS) {
+                const int i = m0 + e % TC5_BM, j = n0 + e / TC5_BM;
+                if (i < m && j < n) pp[i + (long long)j * ldp] = zmk(0.0, 0.0);
+            }
+        }
+        return;      // uniform over the CTA
+    }
     const int m0 = (blockIdx.x % tiles_m) * TC5_BM;
     const int n0 = (blockIdx.x / tiles_m) * BN;
 
@@ -225,7 +243,7 @@ __global__ void __launch_bounds__(TC5_THREADS, 1) zgemm_tc5_kernel(const GemmDes
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_slot;
-    const int nkb = (K + TC5_KB - 1) / TC5_KB;
+    const int nkb = (K - kbeg + TC5_KB - 1) / TC5_KB;
 
     if (warp == 8) {
         // ---------------- MMA issuer: one lane, the warp kept converged ----------------------
@@ -289,7 +307,7 @@ __global__ void __launch_bounds__(TC5_THREADS, 1) zgemm_tc5_kernel(const GemmDes
         const long long lda = sd.A.ld;
         Tc5Regs<BN> cur;
         auto load = [&](int kb, Tc5Regs<BN>& r) {
-            const int k0 = kb * TC5_KB;
+            const int k0 = kbeg + kb * TC5_KB;
 #pragma unroll
             for (int u = 0; u < U::A_UNITS; ++u) {
                 const int unit = tid + u * TC5_PRODUCERS;       // (row, chunk): row fastest
@@ -387,6 +405,7 @@ __global__ void __launch_bounds__(TC5_THREADS, 1) zgemm_tc5_kernel(const GemmDes
                 if (use_c) cro = vrow(sd.C, gi);
             }
             const z alpha = sd.alpha, beta = sd.beta;
+            z* pp = part ? part + ((long long)blockIdx.y * ksplit + blockIdx.z) * pstride : nullptr;
             constexpr int HALF = BN / 2;
             constexpr int CH = HALF < 16 ? HALF : 16;
 #pragma unroll 1
@@ -401,6 +420,10 @@ __global__ void __launch_bounds__(TC5_THREADS, 1) zgemm_tc5_kernel(const GemmDes
                 for (int e = 0; e < CH; ++e) {
                     const int gj = n0 + c0 + e;
                     if (gj >= n) break;
+                    if (pp) {
+                        pp[gi + (long long)gj * ldp] = zmk((double)vr[e], (double)vi[e]);
+                        continue;
+                    }
                     z v = zmul(alpha, zmk((double)vr[e], (double)vi[e]));
                     if (use_c) zfma(v, beta, sd.C.p[cro + (long long)vcol(sd.C, gj) * sd.C.ld]);
                     sd.D.p[dro + (long long)vcol(sd.D, gj) * sd.D.ld] = v;
@@ -423,12 +446,43 @@ static cudaError_t launch_tc5(const GemmBatch& b, int* status, cudaStream_t s) {
     cudaError_t e = ensure_smem_attr(zgemm_tc5_kernel<BN>, Cfg::SMEM, attr, true);
     if (e != cudaSuccess) return e;
     const int tiles = ((b.max_m + TC5_BM - 1) / TC5_BM) * ((b.max_n + BN - 1) / BN);
+    if (b.t5_ksplit > 1 && b.work) {
+        if (b.count > 65535 || b.t5_ksplit > 65535) return cudaErrorInvalidValue;
+        zgemm_tc5_kernel<BN><<<dim3(tiles, b.count, b.t5_ksplit), TC5_THREADS, Cfg::SMEM, s>>>(
+            b.d_desc, status, b.t5_kchunk, b.work, b.t5_pstride, b.max_m, b.t5_ksplit);
+        note_launch();
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        return launch_gemm_reduce(b, b.t5_ksplit, b.t5_pstride, s);
+    }
     for (int off = 0; off < b.count; off += 65535) {
         const int cnt = (b.count - off) < 65535 ? (b.count - off) : 65535;
-        zgemm_tc5_kernel<BN><<<dim3(tiles, cnt), TC5_THREADS, Cfg::SMEM, s>>>(b.d_desc + off, status);
+        zgemm_tc5_kernel<BN><<<dim3(tiles, cnt), TC5_THREADS, Cfg::SMEM, s>>>(b.d_desc + off, status, 0, nullptr, 0,
+                                                                             0, 1);
         note_launch();
     }
     return cudaGetLastError();
+}
+
+long long gemm_plan_split_tc5(GemmBatch& b) {
+    b.t5_ksplit = 1;
+    b.t5_kchunk = 0;
+    b.t5_pstride = 0;
+    if (b.count == 0 || b.max_k < 128) return 0;
+    // about two waves of one CTA per SM from the 128-row tiles alone (n-independent), each range
+    // at least 64 deep
+    const long long ctas = (long long)b.count * ((b.max_m + TC5_BM - 1) / TC5_BM);
+    long long sp = (2 * 148 + ctas - 1) / ctas;
+    sp = std::min<long long>(sp, 32);
+    sp = std::min<long long>(sp, b.max_k / 64);
+    if (sp < 2) return 0;
+    const int kc = (int)(((b.max_k + sp - 1) / sp + TC5_KB - 1) / TC5_KB * TC5_KB);
+    const int ks = (b.max_k + kc - 1) / kc;
+    if (ks < 2) return 0;
+    b.t5_kchunk = kc;
+    b.t5_ksplit = ks;
+    b.t5_pstride = (long long)b.max_m * b.max_n;
+    return (long long)b.count * ks * b.t5_pstride;
 }
 
 int tc5_tile_n(const GemmBatch& b) {

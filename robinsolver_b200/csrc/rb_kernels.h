@@ -53,6 +53,17 @@ cudaError_t launch_gemm_batch(const GemmBatch& b, cudaStream_t s);
 // for the mixed-precision levels.  status: device word for RB_TC5_TIMEOUT.
 cudaError_t launch_gemm_tc5(const GemmBatch& b, int* status, cudaStream_t s);
 int tc5_tile_n(const GemmBatch& b);
+// Engines (tile shapes) of the FP64 launcher that can run a non-fixed-order batch, for the
+// autotuner: writes up to 8 engine ids to out (a batch's `engine` field takes one) and returns
+// the count.  gemm_engine_name gives each a stage-timer name.
+int gemm_engine_candidates(const GemmBatch& b, int* out);
+const char* gemm_engine_name(int engine);
+// Chooses split-K of a batch on the tcgen05 kernel (sets t5_ksplit, t5_kchunk, t5_pstride; from
+// count, m and k only) and returns the workspace it needs in complex elements (0: no split).
+long long gemm_plan_split_tc5(GemmBatch& b);
+// Adds the split ranges' raw sums in range order and applies the problem's epilogue (alpha, beta,
+// C, output maps): the second pass of every split-K GEMM.
+cudaError_t launch_gemm_reduce(const GemmBatch& b, int ksplit, long long pstride, cudaStream_t s);
 // Chooses split-K for a fixed-order batch (sets ksplit, kchunk, pstride) and returns the
 // workspace it needs in complex elements (0: no split); the caller sets b.work.
 long long gemm_plan_split(GemmBatch& b);
@@ -105,6 +116,18 @@ cudaError_t merge_form_s(ChildStore c, int nnodes, int m, int o1, z zeta, z nu, 
                          cudaStream_t s);
 // K = nu^2 I for every node, into dst + node*m*m.
 cudaError_t merge_form_k(int nnodes, int m, z nu, z* dst, cudaStream_t s);
+// The three K-form merge inputs of one node of any tree and level (a forest's batched merge).
+struct MergeFormDesc {
+    const z* t1;       // child1's Robin-to-Robin matrix
+    const z* t2;       // child2's
+    long long ld;
+    int m, o1, o2, pad;
+    z zeta, nu2;
+    z* a2;             // zeta I - T2_ii
+    z* a1;             // zeta I - T1_ii
+    z* k;              // nu^2 I
+};
+cudaError_t merge_form_kform_batch(const MergeFormDesc* d_descs, int count, int max_m, cudaStream_t s);
 
 // ---- device-side sampling and check_solution (rb_sample.cu) -------------------------------------------
 // pts: n points (x, y, z) as rb_tree_sample_points lists them; outputs complex128

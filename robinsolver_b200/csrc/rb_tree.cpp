@@ -42,6 +42,7 @@
 #include "robin_b200.h"
 #include "rb_kernels.h"
 #include "rb_plan.hpp"
+#include "rb_tree_impl.hpp"
 
 namespace rb {
 static std::atomic<long long> g_launches{0};
@@ -58,143 +59,6 @@ void set_thread_error(const char* msg) { g_create_error = msg ? msg : ""; }
 
 using namespace rb;
 
-namespace {
-
-struct DevBuf {
-    void* p = nullptr;
-    size_t bytes = 0;
-};
-
-struct GJBatch {
-    GJDesc* d_desc = nullptr;
-    int count = 0;
-    int m = 0;
-};
-
-struct StageTimer {
-    const char* name;
-    double flops;
-    int ev;          // index of the start event in the pool (end = ev + 1)
-};
-
-}  // namespace
-
-struct rb_tree {
-    rb_geom geom;
-    Plan P;
-    std::string err;
-    cudaStream_t stream = nullptr;
-    cudaStream_t stream2 = nullptr;      // runs one merge GEMM per level beside the level's inversion
-    cudaStream_t stream3 = nullptr;      // host -> device copies of the inputs, beside running work
-    cudaEvent_t ev_copy = nullptr;
-    // RB_FLAG_ASYNC_FACTOR: rb_tree_factor returns once the factor is enqueued; its completion,
-    // time and status are taken by the next call that needs them (settle_factor)
-    bool async_factor = false;
-    bool factor_pending = false;
-    int* h_status = nullptr;             // pinned: [0] the factor's status word after the factor,
-                                         // [1] the same word as the overlapped solve saw it
-    bool solve_overlapped = false;       // the last solve ran beside its factor (on stream3)
-    std::vector<cudaEvent_t> ev_fork, ev_join;
-    // factor progress for a solve that overlaps it: [l] after level l's inversion, [L] after the leaves
-    std::vector<cudaEvent_t> ev_lvl;
-    cudaEvent_t ev_root_forms = nullptr; // the root's A2 (D) is formed, after level 1's maps
-    bool factor_deferred = false;        // RB_FLAG_ASYNC_FACTOR: potential copied, factor not launched
-    // device-side sampling and check_solution: rb_tree_sample_points' points, cached on first use
-    double* d_pts[3] = {nullptr, nullptr, nullptr};     // potential, source, boundary
-    double* d_par = nullptr;
-    size_t par_cap = 0;
-    double* d_err = nullptr;
-    z* d_uex = nullptr;
-    int device = 0;
-    bool factored = false;
-    double f_time = 0.0, s_time = 0.0;
-    z zeta, nu;
-    int64_t budget = 0;
-    std::vector<DevBuf> bufs;        // every allocation, for the budget and destroy
-    int64_t held = 0;
-    bool verbose = false;
-    bool skip_root = false;
-
-    // persistent factor storage
-    double* d_h = nullptr;
-    z* d_k = nullptr;
-    z* leaf_sinv = nullptr;
-    z* leaf_Y = nullptr;
-    std::vector<z*> rtr;             // per level < L
-    std::vector<z*> dinv, sinv;      // per level < L: inv(D), inv(S); in the K form A2, A1
-    // K form of the interface solve (nu not small): one inversion per node instead of two
-    bool kform = false;
-    std::vector<z*> kinv;            // per level < L, K form only
-    std::vector<int*> d_pmap1, d_pmap2;
-    std::vector<int*> d_pmapc;       // per level < L: pmap1 then pmap2 (the columns of Y1 and Y2)
-    int* d_status = nullptr;
-    // per level < L: [Y1; Y2] = M^-1 blockdiag(T1_iN, T2_iN), nnodes x m x (n1 + n2) each; the
-    // backward sweep below the root applies them to the node's incoming data
-    std::vector<z*> Y1, Y2;
-    z* gj_work = nullptr;
-    int* gj_ipiv = nullptr;
-    // factor launch batches
-    std::vector<GJBatch> gj_d, gj_s, gj_k;
-    std::vector<GemmBatch> fK, fM1, fM2, fM3, fM4;
-    bool factor_ready = false;
-
-    // solve storage
-    int cap_rhs = 0;                 // capacity of the solve buffers
-    int built_rhs = 0;               // nrhs the solve batches were built for
-    int nrhs = 0;                    // RHS held from the last solve
-    z* d_f = nullptr;
-    std::vector<z*> hbuf, gbuf;      // per level 0..L
-    z* tmp = nullptr;
-    z* sol = nullptr;
-    GemmBatch sL0;
-    std::vector<GemmBatch> sF12, sF3, sF4, sF5, sBY;
-    GemmBatch sR1;                   // root: x_i = h_i + T_iN g_N (no K^-1 needed)
-    std::vector<DevBuf> solve_bufs;
-
-    // timing: 0 off, 1 per stage, 2 per launch
-    int timing = 0;
-    struct StageTime { std::string name; double ms; double flops; };
-    std::vector<StageTime> stage_ms;
-    std::vector<StageTimer> timers;
-    std::vector<cudaEvent_t> ev_pool;
-    int ev_used = 0;
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    int64_t factor_launches = 0, solve_launches = 0;
-
-    // RB_PREC_MIXED: the GEMMs of the merge levels l >= 2 whose interface is at least one
-    // tensor-core tile tall (m >= 128) run on the tcgen05 split-TF32 kernel (~1e-6 relative);
-    // the top two levels, the interface inverses, the leaves and the FD residual stay FP64, and
-    // the solve refines every right-hand side against the FP64 residual to refine_tol
-    int prec = RB_PREC_FP64;          // precision of the current factorization
-    int gx_factor_prec = -1;          // precision the captured factor graph was recorded with
-    double refine_tol = 1e-10;
-    int refine_maxit = 8;
-    int refine_iters = 0;             // corrections the last solve applied
-    double refine_rho = 0.0;          // largest contraction factor seen
-    double refine_est = 0.0;          // estimated relative error after the last correction
-    double refine_res = 0.0;          // max |r| / max |x| of the last residual
-    std::vector<int> h_bclass;        // leaf boundary row -> root position or -1 - neighbour row
-    std::vector<std::vector<int>> h_ifrows;   // per level: interface points -> leaf boundary rows
-    int* d_bclass = nullptr;
-    std::vector<int*> d_ifrows;
-    int refine_cap = 0;
-    z* dsol = nullptr;                // the correction of the current refinement step
-    z* d_ri = nullptr;                // interface rows of the residual [rhs][leaf][nb]
-    double* d_norms = nullptr;        // [0, k) max|r|, [k, 2k) max|x|, [2k, 3k) max|dx|
-    double* h_norms = nullptr;
-    std::vector<DevBuf> refine_bufs;
-
-    // CUDA graphs: the factor and solve launch sequences are fixed per tree (and per RHS count),
-    // so after one direct run each is captured once and replayed
-    bool graphs = true;
-    int factor_runs = 0;
-    cudaGraphExec_t gx_factor = nullptr;
-    long long gx_factor_launches = 0;
-    int solve_runs = 0;
-    cudaGraphExec_t gx_solve = nullptr;
-    int gx_solve_rhs = 0;
-    long long gx_solve_launches = 0;
-};
 
 // ---------------------------------------------------------------------------------------------------
 #define RB_CK(call)                                                                              \
@@ -828,12 +692,15 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
         for (int l = 0; l < L; ++l)
             for (GemmBatch* gb : {&t->sF12[l], &t->sF3[l], &t->sF4[l], &t->sF5[l], &t->sBY[l]}) all.push_back(gb);
         long long wmax = 0;
-        for (GemmBatch* gb : all) wmax = std::max(wmax, gemm_plan_split(*gb));
+        for (GemmBatch* gb : all) {
+            wmax = std::max(wmax, gemm_plan_split(*gb));
+            wmax = std::max(wmax, gemm_plan_split_tc5(*gb));     // the same batch on tcgen05 (mixed)
+        }
         if (wmax > 0) {
             z* ws = nullptr;
             if ((rc = alloc_n(t, t->solve_bufs, (size_t)wmax, &ws))) return rc;
             for (GemmBatch* gb : all)
-                if (gb->ksplit > 1) gb->work = ws;
+                if (gb->ksplit > 1 || gb->t5_ksplit > 1) gb->work = ws;
         }
     }
     t->built_rhs = nrhs;
@@ -1619,6 +1486,25 @@ int rb_tree_launch_counts(const rb_tree* t, int64_t* fl, int64_t* sl) {
 // Accessors for the serving loop (rb_server.cpp), which drives handles through the C-ABI.
 
 namespace rb {
+// storage and launch batches of an FP64 factorization (for a forest that runs the factor itself)
+int tree_prepare_factor(rb_tree* t) {
+    if (int rc = settle_factor(t)) return rc;
+    t->factor_deferred = false;
+    return ensure_factor_storage(t);
+}
+// a factorization that a forest completed on the tree's storage
+void tree_mark_factored(rb_tree* t, double f_time) {
+    t->factored = true;
+    t->factor_pending = false;
+    t->factor_deferred = false;
+    t->nrhs = 0;
+    if (t->prec != RB_PREC_FP64) {
+        t->prec = RB_PREC_FP64;
+        drop_graph(t->gx_factor);
+        t->factor_runs = 0;
+    }
+    t->f_time = f_time;
+}
 // device address of the solutions of the last solve, [rhs][leaf][leaf_n]
 const z* tree_solutions(const rb_tree* t) { return t->sol; }
 int tree_device(const rb_tree* t) { return t->device; }
