@@ -81,6 +81,8 @@ def parse():
     ap.add_argument("--serve", action="store_true",
                     help="serving bench: 8 resident trees, Poisson solve stream at 0.5x and 0.9x of saturation")
     ap.add_argument("--requests", type=int, default=4000, help="solve requests per offered load (--serve)")
+    ap.add_argument("--forest", action="store_true",
+                    help="batching bench: 64 trees of uneven sizes factored as one forest vs one at a time")
     return ap.parse_args()
 
 
@@ -825,10 +827,103 @@ def serve_arm(args):
     return 0
 
 
+# ------------------------------------------------------------------------------------------------
+# Forest: 64 trees of uneven sizes factored in one schedule (rb_forest_*)
+# ------------------------------------------------------------------------------------------------
+
+FOREST_GRIDS = [(128, 4), (192, 6), (256, 6), (384, 8), (512, 8)]
+
+
+def forest_workloads(ntrees=64, seed=3000):
+    """64 trees, grids drawn from {128^2, 192^2, 256^2, 384^2, 512^2} with L giving 24^2 to 32^2
+    leaves, kb ~ U(20, 120), 20-60 bumps, 8 point-source right-hand sides each."""
+    from robinsolver_b200 import workloads as W
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(ntrees):
+        N, L = FOREST_GRIDS[int(rng.integers(len(FOREST_GRIDS)))]
+        out.append(W.make_workload(2, instance=200 + i, N=N, L=L, kb=float(rng.uniform(20.0, 120.0)),
+                                   nbumps=int(rng.integers(20, 61)), delta=0.005, nrhs=8, kinds="point"))
+    return out
+
+
+def forest_arm(args):
+    import torch
+
+    import robinsolver_b200 as rb
+    from robinsolver_b200 import _lib
+
+    torch.cuda.set_device(0)
+    dev = torch.device("cuda", 0)
+    wls = forest_workloads()
+    trees, d_k, FG = [], [], []
+    for wl in wls:
+        T = rb.robin_tree()
+        T.bndry_params = wl.bndry_params
+        T.plan(wl.L, rb.elliptic_operator(d=2, domain=wl.domain, k=wl.potential),
+               rb.solve_opts(h_tgt=wl.h_tgt, kb=wl.opts_kb))
+        kv = np.ascontiguousarray(wl.potential(T.sample_points(_lib.RB_POINTS_POTENTIAL)))
+        F, G = T.sample_rhs([rb.elliptic_rhs(d=2, f=r.f, g=[rb.bndry_rhs(g) for g in r.g]) for r in wl.rhs])
+        trees.append(T)
+        d_k.append(torch.from_numpy(kv).to(dev))
+        FG.append((torch.from_numpy(F).to(dev), torch.from_numpy(G).to(dev)))
+    lib = _lib.lib
+
+    # (a) every tree factored on its own, as graphs (second call on), one after the other
+    for T, k in zip(trees, d_k):
+        for _ in range(2):
+            assert lib.rb_tree_factor_device(T.handle, k.data_ptr(), _lib.RB_PREC_FP64, 1) == 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    reps = max(1, args.steps)
+    for _ in range(reps):
+        for T, k in zip(trees, d_k):
+            assert lib.rb_tree_factor_device(T.handle, k.data_ptr(), _lib.RB_PREC_FP64, 0) == 0
+    torch.cuda.synchronize()
+    single_s = (time.perf_counter() - t0) / reps
+    # (b) the forest: autotune once, capture, replay
+    Fo = rb.robin_forest(trees)
+    ptrs = [k.data_ptr() for k in d_k]
+    ta = time.perf_counter()
+    Fo.factor(ptrs, autotune=True)
+    tune_s = time.perf_counter() - ta
+    for _ in range(max(1, args.warmup)):
+        Fo.factor(ptrs, autotune=True)
+    ft = []
+    for _ in range(reps):
+        Fo.factor(ptrs, autotune=True)
+        ft.append(Fo.info()["f_time"])
+    forest_s = float(np.median(ft))
+    info = Fo.info()
+    # the forest's factors solve: 8 point sources per tree
+    t1 = time.perf_counter()
+    for T, (F, G) in zip(trees, FG):
+        assert lib.rb_tree_solve_device(T.handle, 8, F.data_ptr(), G.data_ptr(), 0) == 0
+    torch.cuda.synchronize()
+    solve_s = time.perf_counter() - t1
+    picks = {}
+    for h, st, eng, ms in Fo.tuning():
+        picks.setdefault((h, st), []).append((ms, eng))
+    chosen = {f"h{h}s{st}": min(v)[1] for (h, st), v in sorted(picks.items())}
+    out = {"metric": "64-tree batched factor: trees/s, forest vs one tree at a time (FP64, CUDA graphs)",
+           "value": len(trees) / forest_s, "unit": "trees/s", "forest_factor_ms": forest_s * 1e3,
+           "single_trees_factor_ms": single_s * 1e3, "speedup": single_s / forest_s,
+           "forest_launches": info["launches"], "tuned_stages": info["tuned_stages"], "autotune_s": tune_s,
+           "solve_8rhs_all_trees_ms": solve_s * 1e3, "engines": chosen,
+           "trees": {f"{N}^2 L={L}": sum(1 for w in wls if w.N == N) for N, L in FOREST_GRIDS}}
+    print(json.dumps(out), flush=True)
+    Fo.close()
+    for T in trees:
+        T.close()
+    return 0
+
+
 def main():
     args = parse()
     if args.serve:
         return serve_arm(args)
+    if args.forest:
+        return forest_arm(args)
     if args.impl == "reference":
         return reference_arm(args)
     return our_arm(args)

@@ -17,7 +17,7 @@ module robinsolver_b200
     integer, parameter :: dp = kind(1.0d0)
 
     public :: elliptic_operator, solve_opts, debug_opts, elliptic_rhs, bndry_rhs, leaf_solution, &
-              robin_tree, get_solution, scalar_proc, coeff_proc
+              robin_tree, get_solution, scalar_proc, coeff_proc, b200_opts
 
     abstract interface
         pure function coeff_proc(x) result(c)
@@ -71,6 +71,15 @@ module robinsolver_b200
         complex(dp), dimension(:), allocatable :: u
     end type
 
+    ! Extensions of this library, kept out of solve_opts so that it stays the reference's type:
+    ! precision 'fp64' (RB_PREC_FP64) or 'mixed' (RB_PREC_MIXED: split-TF32 tensor-core GEMMs on
+    ! the lower merge levels, every solve refined against the FP64 residual to tol).
+    type b200_opts
+        character(len=5) :: precision = 'fp64'
+        real(dp) :: tol = 1.0d-10
+        integer :: max_iter = 8
+    end type
+
     type robin_tree
         integer :: nlvls
         type(elliptic_operator) :: ell_op
@@ -78,6 +87,7 @@ module robinsolver_b200
         complex(dp), dimension(1:2,1:2) :: bndry_params
         logical :: factored = .false.
         real(dp) :: f_time, s_time
+        type(b200_opts) :: b200
         type(c_ptr) :: handle = c_null_ptr
     contains
         procedure :: factor => robin_tree_factor
@@ -152,6 +162,12 @@ module robinsolver_b200
             type(c_ptr), value :: t
             real(c_double), intent(out) :: f_time, s_time
         end function
+        integer(c_int) function rb_tree_set_refinement(t, tol, max_iter) bind(c, name='rb_tree_set_refinement')
+            import :: c_int, c_ptr, c_double
+            type(c_ptr), value :: t
+            real(c_double), value :: tol
+            integer(c_int), value :: max_iter
+        end function
     end interface
 
 contains
@@ -209,7 +225,9 @@ contains
         do p = 1, int(info%n_interior)
             k(p) = ell_op%k(xyz(3*p-2:3*p))
         end do
-        call check(rb_tree_factor(T%handle, k, 0_c_int), T%handle)
+        call check(rb_tree_set_refinement(T%handle, real(T%b200%tol, c_double), int(T%b200%max_iter, c_int)), &
+                   T%handle)
+        call check(rb_tree_factor(T%handle, k, merge(1_c_int, 0_c_int, T%b200%precision == 'mixed')), T%handle)
         call check(rb_tree_info(T%handle, info), T%handle)
         T%opts%h = info%h_last
         call check(rb_tree_times(T%handle, T%f_time, T%s_time), T%handle)

@@ -458,9 +458,12 @@ static int ensure_factor_storage(rb_tree* t) {
 #define RB_GEMM(batch, stream) RB_TIMED(gemm_stage_name(batch), (batch).flops, launch_gemm_batch(batch, stream))
 
 // merge level l of a mixed-precision factorization runs its GEMMs on the tcgen05 split-TF32
-// kernel: below the top two levels, and only where the interface fills the 128-row MMA tile
+// kernel: below the top two levels, and only where the interface fills the 128-row MMA tile.
+// Level L stands for the solve's leaf GEMM h = Y(:, nb:) f, which streams every leaf's Y once
+// (HBM-bound): on the tensor cores in the mixed solve as well.
 static bool mixed_level(const rb_tree* t, int l) {
-    return t->prec == RB_PREC_MIXED && l >= 2 && l < t->P.L && t->P.lv[l].m >= 128;
+    if (t->prec != RB_PREC_MIXED || l < 2) return false;
+    return l == t->P.L || t->P.lv[l].m >= 128;
 }
 static cudaError_t launch_gemm_level(rb_tree* t, const GemmBatch& b, int l, cudaStream_t s) {
     return mixed_level(t, l) ? launch_gemm_tc5(b, t->d_status, s) : launch_gemm_batch(b, s);
@@ -728,7 +731,7 @@ static int run_solve(rb_tree* t, int k, cudaStream_t s, const std::vector<cudaEv
     };
     if ((rc = timer_begin(t, "forward"))) return rc;
     if (wait) RB_CK(cudaStreamWaitEvent(s, (*wait)[L], 0));
-    RB_GEMM(t->sL0, s);
+    RB_GEMM_L(t->sL0, L, s);
     for (int l = L - 1; l >= 1; --l) {
         if (wait) RB_CK(cudaStreamWaitEvent(s, (*wait)[l], 0));
         if ((rc = inject_level(l))) return rc;
