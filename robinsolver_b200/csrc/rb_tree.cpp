@@ -875,13 +875,15 @@ static int ensure_refine_storage(rb_tree* t, int k) {
 // relative error is below refine_tol.  The error of x after adding d is about rho |d|, rho the
 // contraction of the iteration (|d| / |x| for the first correction, |d| / |d_previous| after),
 // so the loop stops when rho |d| <= tol |x| / 10.  The residual overwrites d_f and gbuf[0].
-static int refine_solve(rb_tree* t, int k, cudaStream_t s) {
+// wait (optional): the factor's progress events; the first sweep then runs beside the factor
+// (run_solve's overlap), and the corrections after it.
+static int refine_solve(rb_tree* t, int k, cudaStream_t s, const std::vector<cudaEvent_t>* wait = nullptr) {
     const Plan& P = t->P;
     int rc;
     if ((rc = ensure_refine_storage(t, k))) return rc;
     const size_t per = (size_t)P.nleaves() * P.leaf_n();
     RefineGeom rg{P.leaf_a(), P.leaf_b(), P.nleaves(), P.lv[0].nb, P.kb, t->zeta, t->nu};
-    if ((rc = run_solve(t, k, s, nullptr, t->sol, false))) return rc;
+    if ((rc = run_solve(t, k, s, wait, t->sol, false))) return rc;
     std::vector<double> dprev(k, 0.0), xn(k, 0.0);
     t->refine_iters = 0;
     t->refine_rho = 0.0;
@@ -1255,18 +1257,44 @@ static int solve_common(rb_tree* t, int nrhs, const double* f, const double* g, 
     t->nrhs = 0;
     t->solve_overlapped = false;
     if (t->prec == RB_PREC_MIXED) {
-        // mixed precision: a host-steered refinement loop after the factor (no overlap with it)
-        if (t->factor_deferred && (rc = launch_factor(t, nullptr))) return rc;
-        if ((rc = settle_factor(t))) return rc;
-        RB_CK(cudaStreamWaitEvent(t->stream, t->ev[3], 0));      // the last read-back is done
-        RB_CK(cudaMemcpyAsync(t->d_f, f, nrhs * nint * sizeof(z), kind, t->stream));
-        RB_CK(cudaMemcpyAsync(t->gbuf[0], g, nrhs * nroot * sizeof(z), kind, t->stream));
-        RB_CK(cudaEventRecord(t->ev[2], t->stream));
+        // mixed precision: a host-steered refinement loop on the copy stream.  Inputs go up there
+        // (beside a factor that may be running); with an asynchronous factor pending, the first
+        // sweep waits for the factor level by level as in the FP64 overlap, and the corrections
+        // follow it.  The root's Y1, Y2 and own map (read by no solve) may still run behind.
+        const bool overlap = t->factor_deferred && t->timing == 0;
+        cudaStream_t ss = overlap ? t->stream3 : t->stream;
+        if (!overlap) {
+            if (t->factor_deferred && (rc = launch_factor(t, nullptr))) return rc;
+            if ((rc = settle_factor(t))) return rc;
+        }
+        RB_CK(cudaEventRecord(t->ev_copy, t->stream));          // device inputs are ordered there
+        RB_CK(cudaStreamWaitEvent(ss, t->ev_copy, 0));
+        RB_CK(cudaStreamWaitEvent(ss, t->ev[3], 0));            // the last read-back is done
+        RB_CK(cudaMemcpyAsync(t->d_f, f, nrhs * nint * sizeof(z), kind, ss));
+        RB_CK(cudaMemcpyAsync(t->gbuf[0], g, nrhs * nroot * sizeof(z), kind, ss));
+        RB_CK(cudaEventRecord(t->ev[2], ss));
+        if (overlap && (rc = launch_factor(t, &t->ev_lvl))) return rc;
         const long long l0 = launch_count();
-        if ((rc = refine_solve(t, nrhs, t->stream))) return rc;
+        rc = refine_solve(t, nrhs, ss, overlap ? &t->ev_lvl : nullptr);
         t->solve_launches = launch_count() - l0;
-        RB_CK(cudaEventRecord(t->ev[3], t->stream));
-        RB_CK(cudaStreamSynchronize(t->stream));
+        if (overlap) {
+            // every status write of the factor precedes the root level's event, which the first
+            // sweep waited for
+            RB_CK(cudaMemcpyAsync(t->h_status + 1, t->d_status, sizeof(int), cudaMemcpyDeviceToHost, ss));
+        }
+        RB_CK(cudaEventRecord(t->ev[3], ss));
+        if (overlap) RB_CK(cudaStreamWaitEvent(t->stream, t->ev[3], 0));
+        RB_CK(cudaStreamSynchronize(ss));
+        if (overlap) {
+            t->solve_overlapped = true;
+            if (t->h_status[1]) {
+                t->factored = false;
+                t->nrhs = 0;
+                return fail(t, (t->h_status[1] & RB_STATUS_ZERO_PIVOT) ? RB_ERR_NUMERIC : RB_ERR_CUDA,
+                            "the factorization failed (zero pivot or a device wait timed out)");
+            }
+        }
+        if (rc) return rc;
         float ms = 0.f;
         RB_CK(cudaEventElapsedTime(&ms, t->ev[2], t->ev[3]));
         t->s_time = ms * 1e-3;
