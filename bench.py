@@ -903,7 +903,8 @@ def forest_arm(args):
     solve_s = time.perf_counter() - t1
     picks = {}
     for h, st, eng, ms in Fo.tuning():
-        picks.setdefault((h, st), []).append((ms, eng))
+        if ms >= 0:                      # -1: the shape could not launch on that stage
+            picks.setdefault((h, st), []).append((ms, eng))
     chosen = {f"h{h}s{st}": min(v)[1] for (h, st), v in sorted(picks.items())}
     out = {"metric": "64-tree batched factor: trees/s, forest vs one tree at a time (FP64, CUDA graphs)",
            "value": len(trees) / forest_s, "unit": "trees/s", "forest_factor_ms": forest_s * 1e3,

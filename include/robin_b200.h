@@ -289,7 +289,8 @@ int rb_forest_factor(rb_forest* forest, const double* const* d_k, int autotune);
  * shape the autotuner fixed (any output pointer may be NULL). */
 int rb_forest_info(const rb_forest* forest, double* f_time, int64_t* launches, int32_t* tuned_stages);
 /* The autotuner's measurements: min(n, count) entries of (height, stage 0..4 = K, B1, Y1, Y2, parent
- * map, engine id, ms per launch); returns the count.  rb_gemm_engine_name names an engine id. */
+ * map, engine id, ms per launch; -1 for a shape that could not launch on that stage); returns the
+ * count.  rb_gemm_engine_name names an engine id. */
 int rb_forest_tuning(const rb_forest* forest, int32_t* height, int32_t* stage, int32_t* engine, double* ms, int n);
 const char* rb_gemm_engine_name(int engine);
 

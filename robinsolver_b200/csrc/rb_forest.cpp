@@ -226,7 +226,13 @@ int run_gemm(rb_forest* f, GemmBatch& b, int h, int stage, bool tune, cudaStream
         int pick = -1;
         for (int c = 0; c < nc; ++c) {
             b.engine = cand[c];
-            FCK(launch_gemm_batch(b, s));                  // warm (and the first timing's cold start)
+            // a tile shape that cannot launch on this batch (its launch is refused before any
+            // device work) is no candidate
+            if (launch_gemm_batch(b, s) != cudaSuccess) {  // warm (and the first timing's cold start)
+                cudaGetLastError();
+                f->tune_log.push_back({h, stage, cand[c], -1.0f});
+                continue;
+            }
             FCK(cudaEventRecord(f->ev0, s));
             FCK(launch_gemm_batch(b, s));
             FCK(cudaEventRecord(f->ev1, s));
@@ -238,6 +244,10 @@ int run_gemm(rb_forest* f, GemmBatch& b, int h, int stage, bool tune, cudaStream
                 best = ms;
                 pick = cand[c];
             }
+        }
+        if (pick < 0) {
+            f->err = "rb_forest: no GEMM tile shape could run a merge stage";
+            return RB_ERR_CUDA;
         }
         b.engine = pick;
         std::lock_guard<std::mutex> lk(g_tune_mu);

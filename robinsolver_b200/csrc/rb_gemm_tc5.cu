@@ -12,13 +12,14 @@
 // iterative refinement against the FP64 residual (rb_refine.cu).
 //
 // CTA = one 128 x BN output tile of one problem (blockIdx.y), 9 warps:
-//   warps 0-7  producers: FP64 operand loads through the problem's ZViews (face gathers, row
-//              maps, skipped bands, exactly as the FP64 kernels), split to TF32 hi/lo in
-//              registers and stored to shared memory in the UMMA K-major no-swizzle layout; the
-//              loads of k-block kb+1 are in flight while block kb is converted and stored.
-//              Then the epilogue: tcgen05.ld of the accumulators (warp w reads lanes
-//              32 (w % 4) .. +31, half w / 4 of the columns), alpha/beta, scatter through the
-//              output maps.
+//   warps 0-7  producers: cp.async (16 bytes, zero-filled outside the problem) of the FP64 operands
+//              through the problem's ZViews (face gathers, row maps, skipped bands, exactly as the
+//              FP64 kernels) into a ring of STAGES shared-memory stages, STAGES - 1 k-blocks ahead of
+//              the one being converted.  A landed stage is split to TF32 hi/lo IN PLACE (the four
+//              TF32 parts of an element take the 16 bytes of its FP64 pair) into the UMMA K-major
+//              no-swizzle layout, then handed to the MMA warp.  Then the epilogue: tcgen05.ld of
+//              the accumulators (warp w reads lanes 32 (w % 4) .. +31, half w / 4 of the columns),
+//              alpha/beta, scatter through the output maps.
 //   warp 8     allocates 2*BN tensor-memory columns; one lane issues the MMAs of each stage once
 //              its producers have arrived, and releases the stage with tcgen05.commit.
 // Every mbarrier wait is bounded (RB_TC5_WAIT_NS on the global timer).  A wait that runs out sets
@@ -35,19 +36,23 @@ namespace {
 
 constexpr int TC5_BM = 128;          // output rows per tile = UMMA M (one lane per row)
 constexpr int TC5_KB = 16;           // complex k per stage: 4 chunks of 4 TF32 = two UMMA k-steps
-constexpr int TC5_STAGES = 3;
 constexpr int TC5_PRODUCERS = 256;   // warps 0-7
 constexpr int TC5_THREADS = TC5_PRODUCERS + 32;
 constexpr unsigned long long RB_TC5_WAIT_NS = 1000000000ull;   // 1 s per wait
 
 template <int BN>
 struct Tc5Cfg {
-    static constexpr int A_PART = TC5_BM * TC5_KB * 4;   // bytes of one TF32 part of the A tile
+    // one stage: A (128 rows x KB complex) then B (BN columns x KB complex), 16 bytes per element;
+    // raw FP64 pairs first, the four TF32 parts (re/im x hi/lo) in the same bytes after the split
+    static constexpr int A_BYTES = TC5_BM * TC5_KB * 16;
+    static constexpr int B_BYTES = BN * TC5_KB * 16;
+    static constexpr int A_PART = TC5_BM * TC5_KB * 4;     // one TF32 part of A
     static constexpr int B_PART = BN * TC5_KB * 4;
-    static constexpr int STAGE = 4 * A_PART + 4 * B_PART; // re/im x hi/lo of A and of B
-    // + 1024 for the alignment of the stages, + a guard of 16 row groups x one K chunk of A so
-    // that no operand descriptor of the last stage can point past the allocation
-    static constexpr int SMEM = TC5_STAGES * STAGE + 1024 + 16 * TC5_BM * 16;
+    static constexpr int STAGE = A_BYTES + B_BYTES;
+    static constexpr int STAGES = (196608 / STAGE) < 4 ? (196608 / STAGE) : 4;   // 3 (BN 128) or 4
+    static constexpr int AHEAD = STAGES - 1;               // k-blocks in flight beyond the converted one
+    // + 1024 for the alignment of the stages
+    static constexpr int SMEM = STAGES * STAGE + 1024;
     static constexpr int TMEM_COLS = 2 * BN;               // Cr, Ci
 };
 
@@ -152,19 +157,37 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// Per-thread share of one k-block: A units are (tile row, K chunk of 4), B units (column, chunk).
-template <int BN>
-struct Tc5Units {
-    static constexpr int A_UNITS = TC5_BM * (TC5_KB / 4) / TC5_PRODUCERS;           // 2
-    static constexpr int B_TOTAL = BN * (TC5_KB / 4);
-    static constexpr int B_UNITS = (B_TOTAL + TC5_PRODUCERS - 1) / TC5_PRODUCERS;  // 1 (BN <= 64), 2
-};
+__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool valid) {
+    // src-size 0 fills the 16 bytes with zeros (a row, column or k outside the problem)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+// the 256 producer threads only (the MMA warp runs its own loop)
+__device__ __forceinline__ void producers_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+// a producer barrier that also ORs a flag over the 256 producers: every one gets the same answer,
+// so they all leave the loop at the same iteration
+__device__ __forceinline__ bool producers_any(bool v) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred p, q;\n\t"
+        "setp.ne.u32 p, %1, 0;\n\t"
+        "bar.red.or.pred q, 1, 256, p;\n\t"
+        "selp.u32 %0, 1, 0, q;\n\t}"
+        : "=r"(r)
+        : "r"((uint32_t)v)
+        : "memory");
+    return r != 0;
+}
 
-template <int BN>
-struct Tc5Regs {
-    z a[Tc5Units<BN>::A_UNITS][4];
-    z b[Tc5Units<BN>::B_UNITS][4];
-};
+__device__ __forceinline__ void split4(const z (&v)[4], uint4& rh, uint4& rl, uint4& ih, uint4& il) {
+    split_tf32(v[0].x, rh.x, rl.x); split_tf32(v[0].y, ih.x, il.x);
+    split_tf32(v[1].x, rh.y, rl.y); split_tf32(v[1].y, ih.y, il.y);
+    split_tf32(v[2].x, rh.z, rl.z); split_tf32(v[2].y, ih.z, il.z);
+    split_tf32(v[3].x, rh.w, rl.w); split_tf32(v[3].y, ih.w, il.w);
+}
 
 }  // namespace
 
@@ -175,12 +198,12 @@ __global__ void __launch_bounds__(TC5_THREADS, 1) zgemm_tc5_kernel(const GemmDes
                                                                   int kchunk, z* part, long long pstride, int ldp,
                                                                   int ksplit) {
     using Cfg = Tc5Cfg<BN>;
-    using U = Tc5Units<BN>;
+    constexpr int STAGES = Cfg::STAGES;
     extern __shared__ __align__(1024) unsigned char tc5_smem[];
     __shared__ GemmDesc sd;
     __shared__ int a_rows[TC5_BM];          // row offsets of the tile's rows in A (-1: outside m)
     __shared__ long long b_cols[BN];        // column offsets of the tile's columns in B (-1: outside n)
-    __shared__ __align__(8) unsigned long long bars[2 * TC5_STAGES + 1];
+    __shared__ __align__(8) unsigned long long bars[2 * STAGES + 1];
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int abort_flag;
 
@@ -214,8 +237,8 @@ __global__ void __launch_bounds__(TC5_THREADS, 1) zgemm_tc5_kernel(const GemmDes
     unsigned char* stage_base = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(tc5_smem) + 1023) & ~uintptr_t(1023));
     const uint32_t full0 = smem_u32(&bars[0]);
-    const uint32_t empty0 = smem_u32(&bars[TC5_STAGES]);
-    const uint32_t done_bar = smem_u32(&bars[2 * TC5_STAGES]);
+    const uint32_t empty0 = smem_u32(&bars[STAGES]);
+    const uint32_t done_bar = smem_u32(&bars[2 * STAGES]);
 
     for (int i = tid; i < TC5_BM; i += TC5_THREADS) {
         const int gi = m0 + i;
@@ -227,7 +250,7 @@ __global__ void __launch_bounds__(TC5_THREADS, 1) zgemm_tc5_kernel(const GemmDes
     }
     if (tid == 0) {
         abort_flag = 0;
-        for (int s = 0; s < TC5_STAGES; ++s) {
+        for (int s = 0; s < STAGES; ++s) {
             mbar_init(full0 + 8 * s, TC5_PRODUCERS);
             mbar_init(empty0 + 8 * s, 1);
         }
@@ -251,8 +274,8 @@ __global__ void __launch_bounds__(TC5_THREADS, 1) zgemm_tc5_kernel(const GemmDes
         const uint32_t c_re = tmem, c_im = tmem + BN;
         bool ok = true;
         for (int kb = 0; kb < nkb && ok; ++kb) {
-            const int s = kb % TC5_STAGES;
-            const uint32_t par = (uint32_t)((kb / TC5_STAGES) & 1);
+            const int s = kb % STAGES;
+            const uint32_t par = (uint32_t)((kb / STAGES) & 1);
             ok = __all_sync(0xffffffffu, mbar_wait(full0 + 8 * s, par, &abort_flag));
             if (!ok) break;
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -260,7 +283,7 @@ __global__ void __launch_bounds__(TC5_THREADS, 1) zgemm_tc5_kernel(const GemmDes
                 const uint32_t st = smem_u32(stage_base + (size_t)s * Cfg::STAGE);
                 const uint32_t a_rh = st, a_rl = st + Cfg::A_PART, a_ih = st + 2 * Cfg::A_PART,
                                a_il = st + 3 * Cfg::A_PART;
-                const uint32_t bb = st + 4 * Cfg::A_PART;
+                const uint32_t bb = st + Cfg::A_BYTES;
                 const uint32_t b_rh = bb, b_rl = bb + Cfg::B_PART, b_ih = bb + 2 * Cfg::B_PART,
                                b_il = bb + 3 * Cfg::B_PART;
                 // K chunk c of A sits at + c * 128 * 16 bytes, of B at + c * BN * 16
@@ -305,60 +328,75 @@ __global__ void __launch_bounds__(TC5_THREADS, 1) zgemm_tc5_kernel(const GemmDes
         const z* __restrict__ Ap = sd.A.p;
         const z* __restrict__ Bp = sd.B.p;
         const long long lda = sd.A.ld;
-        Tc5Regs<BN> cur;
-        auto load = [&](int kb, Tc5Regs<BN>& r) {
+        // cp.async of k-block kb into stage s: A element (i, k) to A + (k * 128 + i) * 16 (consecutive
+        // threads take consecutive rows: A is column-major), B element (k, j) to B + (j * KB + k) * 16
+        // (consecutive threads take consecutive k of a column)
+        auto issue = [&](int kb, int s) {
             const int k0 = kbeg + kb * TC5_KB;
+            const uint32_t st = smem_u32(stage_base + (size_t)s * Cfg::STAGE);
 #pragma unroll
-            for (int u = 0; u < U::A_UNITS; ++u) {
-                const int unit = tid + u * TC5_PRODUCERS;       // (row, chunk): row fastest
-                const int row = unit % TC5_BM, c = unit / TC5_BM;
-                const int ro = a_rows[row];
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    const int k = k0 + 4 * c + e;
-                    r.a[u][e] = (ro >= 0 && k < K) ? __ldg(Ap + ro + (long long)vcol(sd.A, k) * lda) : zmk(0.0, 0.0);
-                }
+            for (int q = 0; q < TC5_BM * TC5_KB / TC5_PRODUCERS; ++q) {
+                const int e = tid + q * TC5_PRODUCERS;
+                const int i = e % TC5_BM, kk = e / TC5_BM, k = k0 + kk;
+                const int ro = a_rows[i];
+                const bool v = ro >= 0 && k < K;
+                const z* src = v ? Ap + ro + (long long)vcol(sd.A, k) * lda : Ap;
+                cp_async16(st + (uint32_t)(kk * TC5_BM + i) * 16, src, v);
             }
 #pragma unroll
-            for (int u = 0; u < U::B_UNITS; ++u) {
-                const int unit = tid + u * TC5_PRODUCERS;       // (column, chunk): chunk fastest
-                const int j = unit / 4, c = unit % 4;
-                const long long co = (unit < U::B_TOTAL) ? b_cols[j] : -1;
-#pragma unroll
-                for (int e = 0; e < 4; ++e) {
-                    const int k = k0 + 4 * c + e;
-                    r.b[u][e] = (co >= 0 && k < K) ? __ldg(Bp + vrow(sd.B, k) + co) : zmk(0.0, 0.0);
-                }
+            for (int q = 0; q < (BN * TC5_KB + TC5_PRODUCERS - 1) / TC5_PRODUCERS; ++q) {
+                const int e = tid + q * TC5_PRODUCERS;
+                if (e >= BN * TC5_KB) break;
+                const int kk = e % TC5_KB, j = e / TC5_KB, k = k0 + kk;
+                const long long co = b_cols[j];
+                const bool v = co >= 0 && k < K;
+                const z* src = v ? Bp + vrow(sd.B, k) + co : Bp;
+                cp_async16(st + Cfg::A_BYTES + (uint32_t)(j * TC5_KB + kk) * 16, src, v);
             }
         };
-        auto store = [&](int s, const Tc5Regs<BN>& r) {
+        // the landed FP64 pairs of stage s -> TF32 parts in place: A unit (row i, K chunk c) and B
+        // unit (column j, chunk c) read their 4 pairs, all producers pass a barrier, then write
+        // part p of A at A + p * A_PART + c * 128 * 16 + i * 16 and of B at B + p * B_PART +
+        // c * BN * 16 + j * 16 (16 bytes: the chunk's 4 TF32 values)
+        auto convert = [&](int s) {
             unsigned char* st = stage_base + (size_t)s * Cfg::STAGE;
+            unsigned char* sb = st + Cfg::A_BYTES;
+            constexpr int AU = TC5_BM * (TC5_KB / 4) / TC5_PRODUCERS;             // 2
+            constexpr int BT = BN * (TC5_KB / 4);
+            constexpr int BU = (BT + TC5_PRODUCERS - 1) / TC5_PRODUCERS;           // 1 or 2
+            z av[AU][4], bv[BU][4];
 #pragma unroll
-            for (int u = 0; u < U::A_UNITS; ++u) {
-                const int unit = tid + u * TC5_PRODUCERS;
-                const int row = unit % TC5_BM, c = unit / TC5_BM;
+            for (int u = 0; u < AU; ++u) {
+                const int unit = tid + u * TC5_PRODUCERS, i = unit % TC5_BM, c = unit / TC5_BM;
+#pragma unroll
+                for (int e = 0; e < 4; ++e) av[u][e] = *reinterpret_cast<const z*>(st + ((4 * c + e) * TC5_BM + i) * 16);
+            }
+#pragma unroll
+            for (int u = 0; u < BU; ++u) {
+                const int unit = tid + u * TC5_PRODUCERS, j = unit / 4, c = unit % 4;
+                if (unit < BT) {
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) bv[u][e] = *reinterpret_cast<const z*>(sb + (j * TC5_KB + 4 * c + e) * 16);
+                }
+            }
+            producers_sync();                    // every pair of the stage is read before any write
+#pragma unroll
+            for (int u = 0; u < AU; ++u) {
+                const int unit = tid + u * TC5_PRODUCERS, i = unit % TC5_BM, c = unit / TC5_BM;
                 uint4 rh, rl, ih, il;
-                split_tf32(r.a[u][0].x, rh.x, rl.x); split_tf32(r.a[u][0].y, ih.x, il.x);
-                split_tf32(r.a[u][1].x, rh.y, rl.y); split_tf32(r.a[u][1].y, ih.y, il.y);
-                split_tf32(r.a[u][2].x, rh.z, rl.z); split_tf32(r.a[u][2].y, ih.z, il.z);
-                split_tf32(r.a[u][3].x, rh.w, rl.w); split_tf32(r.a[u][3].y, ih.w, il.w);
-                const size_t off = (size_t)c * TC5_BM * 16 + (size_t)row * 16;
+                split4(av[u], rh, rl, ih, il);
+                const size_t off = (size_t)c * TC5_BM * 16 + (size_t)i * 16;
                 *reinterpret_cast<uint4*>(st + off) = rh;
                 *reinterpret_cast<uint4*>(st + Cfg::A_PART + off) = rl;
                 *reinterpret_cast<uint4*>(st + 2 * Cfg::A_PART + off) = ih;
                 *reinterpret_cast<uint4*>(st + 3 * Cfg::A_PART + off) = il;
             }
-            unsigned char* sb = st + 4 * Cfg::A_PART;
 #pragma unroll
-            for (int u = 0; u < U::B_UNITS; ++u) {
-                const int unit = tid + u * TC5_PRODUCERS;
-                if (unit >= U::B_TOTAL) continue;
-                const int j = unit / 4, c = unit % 4;
+            for (int u = 0; u < BU; ++u) {
+                const int unit = tid + u * TC5_PRODUCERS, j = unit / 4, c = unit % 4;
+                if (unit >= BT) continue;
                 uint4 rh, rl, ih, il;
-                split_tf32(r.b[u][0].x, rh.x, rl.x); split_tf32(r.b[u][0].y, ih.x, il.x);
-                split_tf32(r.b[u][1].x, rh.y, rl.y); split_tf32(r.b[u][1].y, ih.y, il.y);
-                split_tf32(r.b[u][2].x, rh.z, rl.z); split_tf32(r.b[u][2].y, ih.z, il.z);
-                split_tf32(r.b[u][3].x, rh.w, rl.w); split_tf32(r.b[u][3].y, ih.w, il.w);
+                split4(bv[u], rh, rl, ih, il);
                 const size_t off = (size_t)c * BN * 16 + (size_t)j * 16;
                 *reinterpret_cast<uint4*>(sb + off) = rh;
                 *reinterpret_cast<uint4*>(sb + Cfg::B_PART + off) = rl;
@@ -366,22 +404,39 @@ __global__ void __launch_bounds__(TC5_THREADS, 1) zgemm_tc5_kernel(const GemmDes
                 *reinterpret_cast<uint4*>(sb + 3 * Cfg::B_PART + off) = il;
             }
         };
-        load(0, cur);
+        constexpr int AHEAD = Cfg::AHEAD;
+        // prologue: the first AHEAD k-blocks into fresh stages, one commit group each
+        for (int q = 0; q < AHEAD; ++q) {
+            if (q < nkb) issue(q, q);
+            cp_async_commit();
+        }
         bool ok = true;
         for (int kb = 0; kb < nkb; ++kb) {
-            const int s = kb % TC5_STAGES;
-            Tc5Regs<BN> nxt;
-            if (kb + 1 < nkb) load(kb + 1, nxt);       // in flight during the wait and the stores
-            if (kb >= TC5_STAGES) {
-                // the MMAs of k-block kb - STAGES read this stage
-                ok = mbar_wait(empty0 + 8 * s, (uint32_t)(((kb / TC5_STAGES) - 1) & 1), &abort_flag);
-                if (!ok) break;
-            }
-            store(s, cur);
+            const int s = kb % STAGES;
+            // groups committed so far: AHEAD + kb; k-block kb is the (kb+1)-th
+            cp_async_wait<AHEAD - 1>();
+            producers_sync();                    // every producer's copies of stage s have landed
+            convert(s);
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // generic -> async proxy
             mbar_arrive(full0 + 8 * s);
-            if (kb + 1 < nkb) cur = nxt;
+            const int kn = kb + AHEAD;
+            if (kn < nkb) {
+                const int sn = kn % STAGES;
+                if (kn >= STAGES) {
+                    // the MMAs of k-block kn - STAGES (= kb - 1) read stage sn: one thread waits
+                    // (bounded), the others at the barrier, which also agrees on giving up
+                    bool bad = false;
+                    if (tid == 0) bad = !mbar_wait(empty0 + 8 * sn, (uint32_t)(((kn / STAGES) - 1) & 1), &abort_flag);
+                    if (producers_any(bad || abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                }
+                issue(kn, sn);
+            }
+            cp_async_commit();
         }
+        cp_async_wait<0>();                      // no copy may still target this CTA's memory
         if (!ok) {
             abort_flag = 1;
             atomicOr(status, RB_TC5_TIMEOUT);
@@ -486,15 +541,21 @@ long long gemm_plan_split_tc5(GemmBatch& b) {
 }
 
 int tc5_tile_n(const GemmBatch& b) {
-    // n columns per tile: the widest UMMA N that the problems fill, 64 for the merges, 32 for
-    // narrow solves
-    return b.max_n <= 32 ? 32 : 64;
+    // n columns per tile: 32 for the narrow solve products, 128 where the 128 x 128 tiles still
+    // fill a wave of the 148 SMs (twice the operand reuse of 128 x 64), else 64
+    if (b.max_n <= 32) return 32;
+    if (b.max_n <= 64) return 64;
+    const long long t128 = (long long)b.count * ((b.max_m + TC5_BM - 1) / TC5_BM) * ((b.max_n + 127) / 128);
+    return t128 >= 148 ? 128 : 64;
 }
 
 cudaError_t launch_gemm_tc5(const GemmBatch& b, int* status, cudaStream_t s) {
     if (b.count == 0 || b.max_m == 0 || b.max_n == 0) return cudaSuccess;
     if (!status) return cudaErrorInvalidValue;
-    return tc5_tile_n(b) == 32 ? launch_tc5<32>(b, status, s) : launch_tc5<64>(b, status, s);
+    const int bn = tc5_tile_n(b);
+    if (bn == 32) return launch_tc5<32>(b, status, s);
+    if (bn == 128) return launch_tc5<128>(b, status, s);
+    return launch_tc5<64>(b, status, s);
 }
 
 }  // namespace rb

@@ -67,7 +67,7 @@ __device__ __forceinline__ void atomic_max_nonneg(double* p, double v) {
 // ([rhs][leaf][nb]), all updated in place (ri read as zero when first).  bclass[leaf*nb + r]:
 // >= 0 the root boundary position of a domain-boundary point, < 0 -1 - (leaf'*nb + r') of the
 // neighbour's row for the same point.  rnorm[rhs]: max |r| over every row, accumulated.
-__global__ void __launch_bounds__(256) fd_residual_kernel(RefineGeom g, const z* __restrict__ d, z* f, z* groot,
+__global__ void __launch_bounds__(128) fd_residual_kernel(RefineGeom g, const z* __restrict__ d, z* f, z* groot,
                                                          z* ri, const z* __restrict__ kv, const double* __restrict__ hh,
                                                          const int* __restrict__ bclass, int first, double* rnorm) {
     extern __shared__ z ush[];
@@ -190,7 +190,7 @@ cudaError_t fd_residual(const RefineGeom& g, int nrhs, const z* d, z* f, z* groo
         cudaError_t e = ensure_smem_attr(fd_residual_kernel, sh, attr);
         if (e != cudaSuccess) return e;
     }
-    fd_residual_kernel<<<dim3(g.nleaves, nrhs), 256, sh, s>>>(g, d, f, groot, ri, kv, hh, bclass, first ? 1 : 0, rnorm);
+    fd_residual_kernel<<<dim3(g.nleaves, nrhs), 128, sh, s>>>(g, d, f, groot, ri, kv, hh, bclass, first ? 1 : 0, rnorm);
     note_launch();
     return cudaGetLastError();
 }

@@ -33,6 +33,7 @@
 #include <cmath>
 #include <atomic>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <functional>
@@ -468,6 +469,12 @@ static bool mixed_level(const rb_tree* t, int l) {
 static cudaError_t launch_gemm_level(rb_tree* t, const GemmBatch& b, int l, cudaStream_t s) {
     return mixed_level(t, l) ? launch_gemm_tc5(b, t->d_status, s) : launch_gemm_batch(b, s);
 }
+// RB_MIXED_SOLVE_ENGINE=fp64 (read at every solve): the mixed solve applies its factor with the
+// FP64 GEMMs; a comparison knob that separates the factor's rounding from the sweeps' own
+static bool mixed_solve_fp64() {
+    const char* v = std::getenv("RB_MIXED_SOLVE_ENGINE");
+    return v && std::strcmp(v, "fp64") == 0;
+}
 #define RB_GEMM_L(batch, level, stream)                                                          \
     RB_TIMED(mixed_level(t, level) ? "zgemm_tc5" : gemm_stage_name(batch), (batch).flops,         \
              launch_gemm_level(t, batch, level, stream))
@@ -722,6 +729,12 @@ static int run_solve(rb_tree* t, int k, cudaStream_t s, const std::vector<cudaEv
     const int L = P.L, nl = P.nleaves();
     LeafGeom lg{P.leaf_a(), P.leaf_b(), P.leaf_nb(), P.leaf_n(), P.kb};
     int rc;
+    const bool sweep_fp64 = mixed_solve_fp64();
+#define RB_GEMM_S(batch, level, stream)                                                          \
+    do {                                                                                         \
+        if (sweep_fp64) RB_GEMM(batch, stream);                                                  \
+        else RB_GEMM_L(batch, level, stream);                                                    \
+    } while (0)
     auto inject_level = [&](int l) -> int {
         if (!inject) return RB_OK;
         const PlanLevel& p = P.lv[l];
@@ -731,14 +744,14 @@ static int run_solve(rb_tree* t, int k, cudaStream_t s, const std::vector<cudaEv
     };
     if ((rc = timer_begin(t, "forward"))) return rc;
     if (wait) RB_CK(cudaStreamWaitEvent(s, (*wait)[L], 0));
-    RB_GEMM_L(t->sL0, L, s);
+    RB_GEMM_S(t->sL0, L, s);
     for (int l = L - 1; l >= 1; --l) {
         if (wait) RB_CK(cudaStreamWaitEvent(s, (*wait)[l], 0));
         if ((rc = inject_level(l))) return rc;
-        RB_GEMM_L(t->sF12[l], l, s);
-        RB_GEMM_L(t->sF3[l], l, s);
-        RB_GEMM_L(t->sF4[l], l, s);
-        RB_GEMM_L(t->sF5[l], l, s);
+        RB_GEMM_S(t->sF12[l], l, s);
+        RB_GEMM_S(t->sF3[l], l, s);
+        RB_GEMM_S(t->sF4[l], l, s);
+        RB_GEMM_S(t->sF5[l], l, s);
     }
     // the root: x = h + T_iN g_N needs level 1's maps (and the K form's first product, A2), not
     // the root's inverse, so it runs as soon as the root's A2 is formed
@@ -761,7 +774,7 @@ static int run_solve(rb_tree* t, int k, cudaStream_t s, const std::vector<cudaEv
         const PlanLevel& p = P.lv[l];
         RB_TIMED("sweep_aux", 0.0, sweep_scatter_down(p.nnodes, k, p.nb, p.nbc, p.m, p.o1, p.o2, p.n1, p.n2, t->d_pmap1[l],
                                      t->d_pmap2[l], t->gbuf[l], t->gbuf[l + 1], s));
-        RB_GEMM_L(t->sBY[l], l, s);
+        RB_GEMM_S(t->sBY[l], l, s);
     }
     if ((rc = timer_end(t))) return rc;
     if ((rc = timer_begin(t, "leaf_recover"))) return rc;
@@ -769,6 +782,7 @@ static int run_solve(rb_tree* t, int k, cudaStream_t s, const std::vector<cudaEv
                                                  out ? out : t->sol, s));
     if ((rc = timer_end(t))) return rc;
     return RB_OK;
+#undef RB_GEMM_S
 }
 
 // ---------------------------------------------------------------------------------------------------
