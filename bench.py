@@ -9,10 +9,11 @@ One step = the reference's hot path on one batch: robin_tree%factor of the 1024^
 (16x16 leaves, kb=200, seeded 100-bump potential with 0.002i*kb damping) followed by one batched
 solve of its 32 seeded plane-wave right-hand sides and get_solution.  ``value`` is right-hand
 sides per second with the factorization inside every step, so it moves with both factor time
-and solve throughput.  The headline arm is the mixed-precision path (RB_PREC_MIXED: split-TF32
-tcgen05 GEMMs on the merge levels 2-6, FP64 elsewhere, every solve refined to 1e-10 against the
-FP64 residual); the plain FP64 path is timed on the same inputs in the same run and reported
-beside it (``fp64``, ``mixed_vs_fp64``).
+and solve throughput.  Both precisions run on the same inputs in the same run: the plain FP64
+path (the headline arm, ``value``: the faster of the two on this workload) and the mixed-precision
+path (``mixed``: RB_PREC_MIXED, split-TF32 tcgen05 GEMMs on the merge levels 2-6 and the solve's
+leaf GEMM, FP64 elsewhere, every solve refined to 1e-10 against the FP64 residual), with
+``mixed_vs_fp64`` their factor, solve and step ratios.  ``--precision mixed`` swaps the roles.
 
 * value:  device-resident inputs (rb_tree_factor_device / rb_tree_solve_device /
           rb_get_solution_device), CUDA events on the library's stream, max over ranks.
@@ -73,7 +74,7 @@ def parse():
     ap.add_argument("--nrhs", type=int, default=None, help="right-hand sides per step (default: the config's)")
     ap.add_argument("--config", type=int, default=4, choices=[1, 2, 4],
                     help="workload: 4 = 1024^2 L=12 (the headline), 2 = 512^2 L=10, 1 = 64^2 L=4 (profiling/tests)")
-    ap.add_argument("--precision", default="mixed", choices=["mixed", "fp64"],
+    ap.add_argument("--precision", default="fp64", choices=["mixed", "fp64"],
                     help="the headline arm (value, e2e, roofline); the other precision is timed beside it")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
@@ -683,6 +684,7 @@ def our_arm(args):
 # ------------------------------------------------------------------------------------------------
 
 SERVE_GRIDS = [(256, 6), (384, 8), (512, 8), (768, 10), (1024, 12)]
+SERVE_BUFFERS = 8
 
 
 def serve_trees(seed=5000, ntrees=8):
@@ -796,11 +798,12 @@ def serve_arm(args):
         reqs = [srv.submit_factor(t, bumps=_bump_params(wl)) for t, wl in zip(tids, trees)]
         for r in reqs:
             srv.wait(r)
-        # pinned output buffers: 3 per tree of 64 right-hand sides
+        # pinned output buffers: NBUF per tree of 64 right-hand sides (a request waits for a free one
+        # of its tree; too few make the single submitter a head-of-line block for every tree)
         bufs = []
         for p in per:
             qq = queue.Queue()
-            for _ in range(3):
+            for _ in range(SERVE_BUFFERS):
                 qq.put(torch.empty(64 * p, dtype=torch.complex128).pin_memory().numpy())
             bufs.append(qq)
         srv.stats(reset=True)
@@ -823,6 +826,7 @@ def serve_arm(args):
         out[prec] = res
         srv.close()
     out["trees"] = [f"{wl.N}^2 L={wl.L} kb={wl.kb:.1f}" for wl in trees]
+    out["output_buffers_per_tree"] = SERVE_BUFFERS
     print(json.dumps(out), flush=True)
     return 0
 

@@ -109,6 +109,7 @@ module robinsolver_b200
         real(c_double) :: h_last(3)
         integer(c_int64_t) :: n_interior, device_bytes
         integer(c_int32_t) :: factored, nrhs
+        integer(c_int32_t) :: d, leaf_c, root_c, reserved
     end type
 
     integer(c_int), parameter :: RB_POINTS_POTENTIAL = 0, RB_POINTS_SOURCE = 1, RB_POINTS_BOUNDARY = 2
@@ -240,8 +241,8 @@ contains
         type(rb_info) :: info
         real(c_double), allocatable :: xf(:), xg(:)
         complex(c_double_complex), allocatable :: f(:), g(:)
-        integer :: p, face, first, last
-        integer :: bounds(5)
+        integer :: p, face, first, last, nfaces
+        integer :: bounds(7), pf(6)
         if (.not. T%factored) stop 'Error: Robin Tree must be factored first.'
         if (T%ell_op%d /= rhs%d) stop 'Error: Dimensions of Robin Tree and RHS do not match.'
         call check(rb_tree_info(T%handle, info), T%handle)
@@ -251,8 +252,19 @@ contains
         do p = 1, int(info%n_interior)
             f(p) = rhs%f(xf(3*p-2:3*p))
         end do
-        bounds = [0, info%root_b, 2*info%root_b, 2*info%root_b + info%root_a, info%root_nb]
-        do face = 1, 4
+        ! points per root face (get_pt_face, fd_module.f90:1033-1049), faces x1 x2 y1 y2 (z1 z2)
+        nfaces = 2*info%d
+        if (info%d == 2) then
+            pf(1:4) = [info%root_b, info%root_b, info%root_a, info%root_a]
+        else
+            pf = [info%root_b*info%root_c, info%root_b*info%root_c, info%root_a*info%root_c, &
+                  info%root_a*info%root_c, info%root_a*info%root_b, info%root_a*info%root_b]
+        end if
+        bounds(1) = 0
+        do face = 1, nfaces
+            bounds(face + 1) = bounds(face) + pf(face)
+        end do
+        do face = 1, nfaces
             first = bounds(face) + 1
             last = bounds(face + 1)
             do p = first, last

@@ -39,7 +39,8 @@ extern "C" {
 #define RB_ERR_NOT_FACTORED   -4  /* "Robin Tree must be factored first."                            */
 #define RB_ERR_DIM_MISMATCH   -5  /* "Dimensions of Robin Tree and RHS do not match."                */
 #define RB_ERR_GEOMETRY       -6  /* "Interface sizes of node children do not match." (non-uniform)   */
-#define RB_ERR_UNSUPPORTED    -7  /* a valid request this build does not implement (d = 3, ...)       */
+#define RB_ERR_UNSUPPORTED    -7  /* a valid request this build does not implement (interfaces over
+                                     1024 points, a mixed-precision or forest factor in 3D, ...)   */
 #define RB_ERR_CUDA           -8  /* CUDA runtime failure (message carries cudaGetErrorString)        */
 #define RB_ERR_OUT_OF_MEMORY  -9  /* device allocation refused or over the handle's byte budget       */
 #define RB_ERR_NUMERIC       -10  /* zero pivot / non-finite value met during the factorization       */
@@ -91,7 +92,7 @@ typedef struct rb_tree rb_tree;
  * type(solve_opts) (derived_type_module.f90:309-320), robin_tree%bndry_params
  * (robin_tree_module.f90:61) and the level count L of robin_tree%factor. */
 typedef struct rb_geom {
-    int32_t d;                 /* elliptic_operator%d; 2 (3 returns RB_ERR_UNSUPPORTED)             */
+    int32_t d;                 /* elliptic_operator%d; 2 or 3                                       */
     int32_t L;                 /* tree levels; leaves sit at level L                                */
     double  domain[6];         /* elliptic_operator%domain(1:2,1:3), Fortran column-major:
                                   [x_lo, x_hi, y_lo, y_hi, z_lo, z_hi]                              */
@@ -117,6 +118,11 @@ typedef struct rb_info {
     int64_t device_bytes;      /* device memory currently held by the handle                        */
     int32_t factored;          /* robin_tree%factored                                               */
     int32_t nrhs;              /* right-hand sides held from the last solve                         */
+    int32_t d;                 /* dimension, 2 or 3                                                 */
+    int32_t leaf_c, root_c;    /* grid in z of a leaf and of the whole domain (1 in 2D); in 3D
+                                  leaf_nb = 2(bc + ac + ab), leaf_n = leaf_nb + abc, root_nb likewise,
+                                  n_interior = nleaves * abc                                         */
+    int32_t reserved;
 } rb_info;
 
 /* Builds the tree (robin_tree_factor's setup and bin_tree, robin_tree_module.f90:114-159):
@@ -137,17 +143,19 @@ int rb_tree_info(const rb_tree* tree, rb_info* info);
 
 /* Coordinates (x, y, z triples) at which the caller evaluates its callbacks, in the order the
  * corresponding sample arrays must use:
- *  RB_POINTS_POTENTIAL: nleaves*a*b points, leaves in DFS order (child1 first), each leaf's
- *                       interior cell centres x-fastest; each leaf uses its own h, as
- *                       FD_matrix_row does (fd_module.f90:134-145).
+ *  RB_POINTS_POTENTIAL: nleaves*a*b (3D: *c) points, leaves in DFS order (child1 first), each
+ *                       leaf's interior cell centres x-fastest, then y, then z; each leaf uses
+ *                       its own h, as FD_matrix_row does (fd_module.f90:134-145).
  *  RB_POINTS_SOURCE:    the same points computed with robin_tree%opts%h as it stands after the
  *                       factorization (the last leaf's h), as fd_leaf_solve does
  *                       (fd_module.f90:427-431).
- *  RB_POINTS_BOUNDARY:  root_nb face-local coordinates, faces x1 x2 y1 y2 in turn, each face in
- *                       ascending order: the concatenation apply_bc builds at the root
- *                       (robin_tree_module.f90:1186-1237) of fd_make_bndry_vec's points
- *                       (fd_module.f90:636-651).  x-faces carry (y, 0, 0), y-faces (x, 0, 0).
- *                       The face a point belongs to follows from its index.
+ *  RB_POINTS_BOUNDARY:  root_nb face-local coordinates, faces x1 x2 y1 y2 (z1 z2) in turn: the
+ *                       concatenation apply_bc builds at the root (robin_tree_module.f90:
+ *                       1186-1237) of fd_make_bndry_vec's points (fd_module.f90:636-651), i.e.
+ *                       the face's leaves in leaf order, each leaf's points in the face's own
+ *                       order (first tangential index fastest).  2D: x-faces carry (y, 0, 0),
+ *                       y-faces (x, 0, 0); 3D: x-faces (y, z, 0), y-faces (x, z, 0), z-faces
+ *                       (x, y, 0).  The face a point belongs to follows from its index.
  *  RB_POINTS_SOLUTION:  nleaves*leaf_n points of proc2vec (robin_output_module.f90:258-265).
  * `xyz` holds 3 doubles per point.  Requires the tree to be created (not factored). */
 int rb_tree_sample_points(const rb_tree* tree, int which, double* xyz);
@@ -202,8 +210,9 @@ int rb_tree_set_timing(rb_tree* tree, int mode);
 int rb_tree_stage_times(const rb_tree* tree, double* ms, double* flops, const char** names, int n);
 int rb_tree_clear_stage_times(rb_tree* tree);
 
-/* Shape of level `level` (0 = root, L = leaves): shape[0] = nodes, shape[1], shape[2] = the grid
- * (ptbox) of each node in x and y (robin_tree_module.f90:404-407 for merged nodes). */
+/* Shape of level `level` (0 = root, L = leaves) into shape[0..3]: the node count and the grid
+ * (ptbox) of each node in x, y and z (robin_tree_module.f90:404-407 for merged nodes; z = 1 in
+ * 2D).  `shape` holds 4 entries. */
 int rb_tree_level_shape(const rb_tree* tree, int level, int32_t* shape);
 
 /* Robin-to-Robin matrix of node `node` (0-based, left to right; leaves in DFS order) of level

@@ -86,6 +86,10 @@ class rb_info(C.Structure):
         ("device_bytes", C.c_int64),
         ("factored", C.c_int32),
         ("nrhs", C.c_int32),
+        ("d", C.c_int32),
+        ("leaf_c", C.c_int32),
+        ("root_c", C.c_int32),
+        ("reserved", C.c_int32),
     ]
 
 

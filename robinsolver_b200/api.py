@@ -105,6 +105,13 @@ class leaf_solution:
 PRECISIONS = {"fp64": _lib.RB_PREC_FP64, "mixed": _lib.RB_PREC_MIXED}
 
 
+def _face_sizes(d, a, b, c=1):
+    """Points per face x1 x2 y1 y2 (z1 z2) of an a x b (x c) grid (get_pt_face, fd_module.f90:1033-1049)."""
+    if d == 2:
+        return [b, b, a, a]
+    return [b * c, b * c, a * c, a * c, a * b, a * b]
+
+
 def make_geom(L, ell_op, opts, bndry_params, flags=0, budget=0) -> _lib.rb_geom:
     """The C-ABI's rb_geom for robin_tree%factor(L, op, opts) with robin_tree%bndry_params."""
     g = _lib.rb_geom()
@@ -238,8 +245,8 @@ class robin_tree:
         inf = self._info
         Xf = self.sample_points(_lib.RB_POINTS_SOURCE)
         Xg = self.sample_points(_lib.RB_POINTS_BOUNDARY)
-        a, b = inf.root_a, inf.root_b
-        bounds = [0, b, 2 * b, 2 * b + a, 2 * b + 2 * a]
+        pf = _face_sizes(inf.d, inf.root_a, inf.root_b, inf.root_c)
+        bounds = np.concatenate([[0], np.cumsum(pf)])
         F = np.zeros((len(rhs_list), inf.n_interior), dtype=np.complex128)
         G = np.zeros((len(rhs_list), inf.root_nb), dtype=np.complex128)
         for r, rhs in enumerate(rhs_list):
@@ -247,7 +254,7 @@ class robin_tree:
                 raise RobinSolverError(_lib.RB_ERR_DIM_MISMATCH, "Error: Dimensions of Robin Tree and RHS do not match.")
             if rhs.f is not None:
                 F[r] = rhs.f(Xf)
-            for fc in range(4):
+            for fc in range(len(pf)):
                 gf = rhs.g[fc].g_face if isinstance(rhs.g[fc], bndry_rhs) else rhs.g[fc]
                 if gf is not None:
                     G[r, bounds[fc]:bounds[fc + 1]] = gf(Xg[bounds[fc]:bounds[fc + 1]])
@@ -298,18 +305,17 @@ class robin_tree:
         return u
 
     def get_rtr(self, level: int, node: int) -> np.ndarray:
-        """node%RtR of a node as one nb x nb matrix (faces x1 x2 y1 y2)."""
-        a, b = self._level_grid(level)
-        nb = 2 * (a + b)
+        """node%RtR of a node as one nb x nb matrix (faces x1 x2 y1 y2, then z1 z2 in 3D)."""
+        nb = int(sum(_face_sizes(self._info.d, *self._level_grid(level))))
         out = np.zeros((nb, nb), dtype=np.complex128, order="F")
         _check(lib.rb_tree_get_rtr(self._h, level, node, _lib.dptr(out)), self._h)
         return out
 
     def _level_grid(self, level: int):
-        """(a, b) grid of the nodes of a level."""
-        sh = (_lib.C.c_int32 * 3)()
+        """(a, b, c) grid of the nodes of a level (c = 1 in 2D)."""
+        sh = (_lib.C.c_int32 * 4)()
         _check(lib.rb_tree_level_shape(self._h, level, sh), self._h)
-        return sh[1], sh[2]
+        return sh[1], sh[2], sh[3]
 
     def stage_times(self, with_flops=False):
         """Timed entries as (name, ms) or (name, ms, flops)."""

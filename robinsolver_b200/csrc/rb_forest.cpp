@@ -311,6 +311,7 @@ int rb_forest_create(rb_tree* const* trees, int ntrees, rb_forest** out) {
             if (trees[j] == t) return bail(RB_ERR_INVALID, "rb_forest_create: a tree is listed twice");
         if (!t->kform)
             return bail(RB_ERR_UNSUPPORTED, "rb_forest_create: every tree needs the single-inversion (K form) merge");
+        if (t->P.d != 2) return bail(RB_ERR_UNSUPPORTED, "rb_forest_create: forests of 3D trees are not implemented");
         if (int rc = tree_prepare_factor(t)) return bail(rc, "rb_forest_create: " + t->err);
         if (t->device != f->device) return bail(RB_ERR_INVALID, "rb_forest_create: trees on different devices");
         f->trees.push_back(t);

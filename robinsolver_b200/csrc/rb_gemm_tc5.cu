@@ -519,6 +519,32 @@ static cudaError_t launch_tc5(const GemmBatch& b, int* status, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+long long gemm_plan_split_tc5_factor(GemmBatch& b) {
+    b.t5_ksplit = 1;
+    b.t5_kchunk = 0;
+    b.t5_pstride = 0;
+    // the factor's stages of the middle levels (a few nodes, m = 256 .. 512) give too few 128-row
+    // tiles for 148 SMs: split k until about 1.5 waves, each range at least 128 deep.  Stages
+    // that fill a wave already are left whole (their outputs are large: a reduction pass would
+    // cost more than it gains).
+    if (b.count == 0 || b.max_k < 256) return 0;
+    const int bn = tc5_tile_n(b);
+    const long long tiles =
+        (long long)b.count * ((b.max_m + TC5_BM - 1) / TC5_BM) * ((b.max_n + bn - 1) / bn);
+    if (tiles >= 148) return 0;
+    long long sp = (222 + tiles - 1) / tiles;
+    sp = std::min<long long>(sp, 8);
+    sp = std::min<long long>(sp, b.max_k / 128);
+    if (sp < 2) return 0;
+    const int kc = (int)(((b.max_k + sp - 1) / sp + TC5_KB - 1) / TC5_KB * TC5_KB);
+    const int ks = (b.max_k + kc - 1) / kc;
+    if (ks < 2) return 0;
+    b.t5_kchunk = kc;
+    b.t5_ksplit = ks;
+    b.t5_pstride = (long long)b.max_m * b.max_n;
+    return (long long)b.count * ks * b.t5_pstride;
+}
+
 long long gemm_plan_split_tc5(GemmBatch& b) {
     b.t5_ksplit = 1;
     b.t5_kchunk = 0;

@@ -61,6 +61,8 @@ const char* gemm_engine_name(int engine);
 // Chooses split-K of a batch on the tcgen05 kernel (sets t5_ksplit, t5_kchunk, t5_pstride; from
 // count, m and k only) and returns the workspace it needs in complex elements (0: no split).
 long long gemm_plan_split_tc5(GemmBatch& b);
+// The same for a factor stage: only stages with fewer 128-row tiles than SMs are split.
+long long gemm_plan_split_tc5_factor(GemmBatch& b);
 // Adds the split ranges' raw sums in range order and applies the problem's epilogue (alpha, beta,
 // C, output maps): the second pass of every split-K GEMM.
 cudaError_t launch_gemm_reduce(const GemmBatch& b, int ksplit, long long pstride, cudaStream_t s);
@@ -102,6 +104,17 @@ cudaError_t leaf_block_factor(const LeafGeom& g, int nleaves, const double* h, c
 // null for zero sources), gb is [leaf][rhs][nb].
 cudaError_t leaf_block_solve(const LeafGeom& g, int nleaves, int nrhs, const double* h, const z* f, const z* gb,
                              const z* sinv, z* sol, cudaStream_t s);
+
+// Dense 3D leaf (rb_leaf3d.cu): A (n x n, column-major, at A + leaf*n*n) from the leaf's spacings
+// hh (3 per leaf) and potential kv (a*b*c per leaf, x fastest); Y = R A^-1 (nb x n, ld nb) from
+// A^-1 in place of A.
+struct Leaf3Geom {
+    int a, b, c;       // interior grid
+    int nb, n;         // boundary points 2(bc+ac+ab), unknowns nb + abc
+    double kb;
+};
+cudaError_t leaf3_assemble(const Leaf3Geom& g, int nleaves, const double* hh, const z* kv, z* A, cudaStream_t s);
+cudaError_t leaf3_rtr(const Leaf3Geom& g, int nleaves, const double* hh, const z* Ainv, z* Y, cudaStream_t s);
 
 // ---- merge helpers -------------------------------------------------------------------------------------
 struct ChildStore {

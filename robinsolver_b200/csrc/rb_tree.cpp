@@ -255,7 +255,7 @@ static int run_graphed(rb_tree* t, cudaGraphExec_t& gx, long long& gx_launches, 
 static int ensure_factor_storage(rb_tree* t) {
     if (t->factor_ready) return RB_OK;
     const Plan& P = t->P;
-    const int L = P.L, nl = P.nleaves(), a = P.leaf_a(), b = P.leaf_b(), ab = a * b;
+    const int L = P.L, nl = P.nleaves(), a = P.leaf_a(), b = P.leaf_b(), nint = P.leaf_interior();
     const int nb = P.leaf_nb(), n = P.leaf_n();
     int rc;
     RB_CK(cudaGetDevice(&t->device));
@@ -284,10 +284,27 @@ static int ensure_factor_storage(rb_tree* t) {
         RB_CK(cudaEventCreateWithFlags(&t->ev_fork[l], cudaEventDisableTiming));
         RB_CK(cudaEventCreateWithFlags(&t->ev_join[l], cudaEventDisableTiming));
     }
-    if ((rc = alloc_n(t, t->bufs, 2 * (size_t)nl, &t->d_h))) return rc;
-    RB_CK(cudaMemcpy(t->d_h, P.leaf_h.data(), 2 * nl * sizeof(double), cudaMemcpyHostToDevice));
-    if ((rc = alloc_n(t, t->bufs, (size_t)nl * ab, &t->d_k))) return rc;
-    if ((rc = alloc_n(t, t->bufs, (size_t)nl * b * a * a, &t->leaf_sinv))) return rc;
+    if ((rc = alloc_n(t, t->bufs, (size_t)P.d * nl, &t->d_h))) return rc;
+    RB_CK(cudaMemcpy(t->d_h, P.leaf_h.data(), (size_t)P.d * nl * sizeof(double), cudaMemcpyHostToDevice));
+    if ((rc = alloc_n(t, t->bufs, (size_t)nl * nint, &t->d_k))) return rc;
+    if (P.d == 2) {
+        if ((rc = alloc_n(t, t->bufs, (size_t)nl * b * a * a, &t->leaf_sinv))) return rc;
+    } else {
+        // 3D: each leaf's dense FD matrix, inverted in place by the batched Gauss-Jordan kernels
+        if (n > 1024) return fail(t, RB_ERR_UNSUPPORTED, "3D leaf larger than 1024 unknowns");
+        if ((rc = alloc_n(t, t->bufs, (size_t)nl * n * n, &t->leaf_sinv))) return rc;
+        if ((rc = alloc_n(t, t->bufs, (size_t)nl * n, &t->leaf_ipiv))) return rc;
+        const long long ws = gj_workspace_elems(n);
+        if ((rc = alloc_n(t, t->bufs, (size_t)std::max<long long>(1, nl * ws), &t->leaf_gjwork))) return rc;
+        std::vector<GJDesc> v(nl);
+        for (int i = 0; i < nl; ++i) {
+            v[i].A = t->leaf_sinv + (long long)i * n * n;
+            v[i].ld = n;
+            v[i].ipiv = t->leaf_ipiv + (long long)i * n;
+            v[i].Zb = t->leaf_gjwork + (long long)i * ws;
+        }
+        if ((rc = upload_gj(t, t->bufs, v, n, t->gj_leaf))) return rc;
+    }
     if ((rc = alloc_n(t, t->bufs, (size_t)nl * nb * n, &t->leaf_Y))) return rc;
     if ((rc = alloc_n(t, t->bufs, 1, &t->d_status))) return rc;
     t->rtr.assign(L, nullptr);
@@ -475,6 +492,32 @@ static bool mixed_solve_fp64() {
     const char* v = std::getenv("RB_MIXED_SOLVE_ENGINE");
     return v && std::strcmp(v, "fp64") == 0;
 }
+// Split-K plans of the mixed levels' factor stages, with two workspaces: B1 runs on the second
+// stream beside K and its inverse, the other stages on the main stream.
+static int ensure_mixed_factor_plan(rb_tree* t) {
+    if (t->mixed_plan) return RB_OK;
+    long long wmain = 0, wside = 0;
+    for (int l = 0; l < t->P.L; ++l) {
+        if (!mixed_level(t, l)) continue;
+        for (GemmBatch* b : {&t->fK[l], &t->fM2[l], &t->fM3[l], &t->fM4[l]})
+            wmain = std::max(wmain, gemm_plan_split_tc5_factor(*b));
+        wside = std::max(wside, gemm_plan_split_tc5_factor(t->fM1[l]));
+    }
+    z* pm = nullptr;
+    z* ps = nullptr;
+    int rc;
+    if (wmain > 0 && (rc = alloc_n(t, t->mixed_bufs, (size_t)wmain, &pm))) return rc;
+    if (wside > 0 && (rc = alloc_n(t, t->mixed_bufs, (size_t)wside, &ps))) return rc;
+    for (int l = 0; l < t->P.L; ++l) {
+        if (!mixed_level(t, l)) continue;
+        for (GemmBatch* b : {&t->fK[l], &t->fM2[l], &t->fM3[l], &t->fM4[l]})
+            if (b->t5_ksplit > 1) b->work = pm;
+        if (t->fM1[l].t5_ksplit > 1) t->fM1[l].work = ps;
+    }
+    t->mixed_plan = true;
+    return RB_OK;
+}
+
 #define RB_GEMM_L(batch, level, stream)                                                          \
     RB_TIMED(mixed_level(t, level) ? "zgemm_tc5" : gemm_stage_name(batch), (batch).flops,         \
              launch_gemm_level(t, batch, level, stream))
@@ -499,8 +542,18 @@ static int run_factor(rb_tree* t, const z* dk, const std::vector<cudaEvent_t>* r
     int rc;
     RB_CK(cudaMemsetAsync(t->d_status, 0, sizeof(int), s));
     if ((rc = timer_begin(t, "leaf_factor"))) return rc;
-    RB_TIMED("leaf_factor", leaf_flops(lg) * nl, leaf_block_factor(lg, nl, t->d_h, dk, t->leaf_sinv, t->leaf_Y,
-                                                                    t->d_status, s));
+    if (P.d == 2) {
+        RB_TIMED("leaf_factor", leaf_flops(lg) * nl, leaf_block_factor(lg, nl, t->d_h, dk, t->leaf_sinv, t->leaf_Y,
+                                                                        t->d_status, s));
+    } else {
+        // 3D: assemble every leaf's FD matrix, invert it (RTR_solve's zgetrf/zgetrs with an identity
+        // right-hand side, robin_tree_module.f90:728-799), turn its face rows into Robin data
+        const Leaf3Geom g3{P.leaf_a(), P.leaf_b(), P.leaf_c(), P.leaf_nb(), P.leaf_n(), P.kb};
+        RB_TIMED("leaf_assemble", 0.0, leaf3_assemble(g3, nl, t->d_h, dk, t->leaf_sinv, s));
+        RB_TIMED("gj_invert", gj_flops(g3.n, nl),
+                 gj_invert_batch(t->gj_leaf.d_desc, nl, g3.n, t->leaf_gjwork, t->d_status, s));
+        RB_TIMED("leaf_rtr", 0.0, leaf3_rtr(g3, nl, t->d_h, t->leaf_sinv, t->leaf_Y, s));
+    }
     if ((rc = timer_end(t))) return rc;
     if (rec) RB_CK(cudaEventRecord((*rec)[L], s));
     static const char* lvl_names[] = {"merge_l0", "merge_l1", "merge_l2", "merge_l3", "merge_l4", "merge_l5",
@@ -562,7 +615,7 @@ static int run_factor(rb_tree* t, const z* dk, const std::vector<cudaEvent_t>* r
 // ---------------------------------------------------------------------------------------------------
 static int ensure_solve_storage(rb_tree* t, int nrhs) {
     const Plan& P = t->P;
-    const int L = P.L, nl = P.nleaves(), ab = P.leaf_a() * P.leaf_b(), nb = P.leaf_nb(), n = P.leaf_n();
+    const int L = P.L, nl = P.nleaves(), ab = P.leaf_interior(), nb = P.leaf_nb(), n = P.leaf_n();
     int rc;
     if (nrhs > t->cap_rhs) {
         drop_graph(t->gx_solve);
@@ -598,6 +651,26 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
                           zview(t->d_f + (long long)i * ab, (long long)nl * ab),
                           zout(t->hbuf[L] + (long long)i * nb * k, nb), one));
     if ((rc = upload_gemm(t, t->solve_bufs, v, t->sL0))) return rc;
+    t->sLg = GemmBatch();
+    t->sLf = GemmBatch();
+    if (P.d == 3) {
+        // the leaf solve of RTR_solve (u = A^-1 [g; f]) as two products with the stored inverse:
+        // u = A^-1(:, :nb) g, then u += A^-1(:, nb:) f; u is [rhs][leaf][n], g [leaf][rhs][nb]
+        std::vector<GemmDesc> vg, vf;
+        for (int i = 0; i < nl; ++i) {
+            const z* ainv = t->leaf_sinv + (long long)i * n * n;
+            z* u = t->sol + (long long)i * n;
+            vg.push_back(gdesc(n, k, nb, zview(ainv, n), zview(t->gbuf[L] + (long long)i * k * nb, nb),
+                               zout(u, (long long)nl * n), one));
+            GemmDesc gf = gdesc(n, k, ab, zview(ainv + (long long)nb * n, n),
+                                zview(t->d_f + (long long)i * ab, (long long)nl * ab), zout(u, (long long)nl * n), one);
+            gf.C = zview(u, (long long)nl * n);
+            gf.beta = one;
+            vf.push_back(gf);
+        }
+        if ((rc = upload_gemm(t, t->solve_bufs, vg, t->sLg))) return rc;
+        if ((rc = upload_gemm(t, t->solve_bufs, vf, t->sLf))) return rc;
+    }
     t->sF12.assign(L, GemmBatch()); t->sF3.assign(L, GemmBatch()); t->sF4.assign(L, GemmBatch());
     t->sF5.assign(L, GemmBatch()); t->sBY.assign(L, GemmBatch());
     t->sR1 = GemmBatch();
@@ -694,11 +767,14 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
     }
     t->sL0.fixed_order = true;
     t->sR1.fixed_order = true;
+    t->sLg.fixed_order = true;
+    t->sLf.fixed_order = true;
     for (int l = 0; l < L; ++l)
         for (GemmBatch* gb : {&t->sF12[l], &t->sF3[l], &t->sF4[l], &t->sF5[l], &t->sBY[l]}) gb->fixed_order = true;
     // split-K for the long-k, few-CTA solve GEMMs; one workspace serves them all (one stream)
     {
         std::vector<GemmBatch*> all{&t->sL0, &t->sR1};
+        if (P.d == 3) { all.push_back(&t->sLg); all.push_back(&t->sLf); }
         for (int l = 0; l < L; ++l)
             for (GemmBatch* gb : {&t->sF12[l], &t->sF3[l], &t->sF4[l], &t->sF5[l], &t->sBY[l]}) all.push_back(gb);
         long long wmax = 0;
@@ -778,8 +854,14 @@ static int run_solve(rb_tree* t, int k, cudaStream_t s, const std::vector<cudaEv
     }
     if ((rc = timer_end(t))) return rc;
     if ((rc = timer_begin(t, "leaf_recover"))) return rc;
-    RB_TIMED("leaf_solve", 0.0, leaf_block_solve(lg, nl, k, t->d_h, t->d_f, t->gbuf[L], t->leaf_sinv,
-                                                 out ? out : t->sol, s));
+    if (P.d == 2) {
+        RB_TIMED("leaf_solve", 0.0, leaf_block_solve(lg, nl, k, t->d_h, t->d_f, t->gbuf[L], t->leaf_sinv,
+                                                     out ? out : t->sol, s));
+    } else {
+        if (out && out != t->sol) return fail(t, RB_ERR_UNSUPPORTED, "3D leaf solve into a second buffer");
+        RB_GEMM(t->sLg, s);
+        RB_GEMM(t->sLf, s);
+    }
     if ((rc = timer_end(t))) return rc;
     return RB_OK;
 #undef RB_GEMM_S
@@ -837,7 +919,7 @@ static std::string build_refine_tables(const Plan& P, std::vector<int>& bclass, 
         const double* lo = &lf.lo[3 * i];
         const double* hi = &lf.hi[3 * i];
         for (int f = 0; f < 4; ++f) {
-            if (lf.isb[4 * i + f]) continue;
+            if (lf.isb[P.nf() * i + f]) continue;
             std::map<std::pair<double, double>, int>::const_iterator it;
             int fo;
             if (f == 0) { it = by_hix.find({lo[0], lo[1]}); fo = 1; if (it == by_hix.end()) return "refinement tables: no x1 neighbour"; }
@@ -955,6 +1037,14 @@ static int refine_solve(rb_tree* t, int k, cudaStream_t s, const std::vector<cud
 }
 
 // ---------------------------------------------------------------------------------------------------
+// persistent leaf storage of a plan in bytes: the leaf factors (2D: b blocks of a x a; 3D: the
+// dense n x n inverse), Y = R A^-1 and the potential samples
+static double leaf_factor_bytes(const Plan& Q) {
+    const double nint = (double)Q.leaf_interior(), n = (double)Q.leaf_n();
+    const double fac = Q.d == 2 ? (double)Q.leaf_b() * Q.leaf_a() * Q.leaf_a() : n * n;
+    return (double)Q.nleaves() * (fac + (double)Q.leaf_nb() * n + nint) * 16.0;
+}
+
 extern "C" {
 
 int rb_tree_create(const rb_geom* geom, rb_tree** out) {
@@ -975,6 +1065,19 @@ int rb_tree_create(const rb_geom* geom, rb_tree** out) {
     if (geom->ordering != 1) {
         g_create_error = "Invalid ordering parameter in igrid2lin";
         return RB_ERR_INVALID;
+    }
+    // the batched Gauss-Jordan inversions hold matrices of up to 1024 rows: every interface and,
+    // in 3D, every dense leaf
+    for (int l = 0; l < P.L; ++l)
+        if (P.lv[l].m > 1024) {
+            g_create_error = "interface of " + std::to_string(P.lv[l].m) + " points on level " + std::to_string(l) +
+                             ": interface inverses of more than 1024 points are not implemented";
+            return RB_ERR_UNSUPPORTED;
+        }
+    if (P.d == 3 && P.leaf_n() > 1024) {
+        g_create_error = "3D leaf of " + std::to_string(P.leaf_n()) +
+                         " unknowns: dense leaf inverses of more than 1024 unknowns are not implemented";
+        return RB_ERR_UNSUPPORTED;
     }
     // bndry_params(i,j) column-major, interleaved
     const double* bp = geom->bndry_params;
@@ -1007,8 +1110,7 @@ int rb_tree_create(const rb_geom* geom, rb_tree** out) {
     // refuse up front a problem the budget cannot hold (persistent factor storage only)
     if (t->budget > 0) {
         const Plan& Q = t->P;
-        const double ab = (double)Q.leaf_a() * Q.leaf_b();
-        double need = (double)Q.nleaves() * (ab * Q.leaf_a() + (double)Q.leaf_nb() * Q.leaf_n() + ab) * 16.0;
+        double need = leaf_factor_bytes(Q);
         for (int l = 0; l < Q.L; ++l)
             need += (double)Q.lv[l].nnodes *
                     ((double)Q.lv[l].nb * Q.lv[l].nb + (t->kform ? 3.0 : 2.0) * Q.lv[l].m * Q.lv[l].m +
@@ -1033,6 +1135,7 @@ int rb_tree_destroy(rb_tree* t) {
     drop_graph(t->gx_solve);
     free_list(t, t->solve_bufs);
     free_list(t, t->refine_bufs);
+    free_list(t, t->mixed_bufs);
     free_list(t, t->bufs);
     if (t->h_norms) cudaFreeHost(t->h_norms);
     for (auto& e : t->ev)
@@ -1066,7 +1169,11 @@ int rb_tree_info(const rb_tree* t, rb_info* info) {
     info->root_a = P.lv[0].a;
     info->root_b = P.lv[0].b;
     for (int j = 0; j < 3; ++j) info->h_last[j] = P.h_last[j];
-    info->n_interior = (int64_t)P.nleaves() * P.leaf_a() * P.leaf_b();
+    info->n_interior = (int64_t)P.nleaves() * P.leaf_interior();
+    info->d = P.d;
+    info->leaf_c = P.leaf_c();
+    info->root_c = P.lv[0].c;
+    info->reserved = 0;
     info->device_bytes = t->held;
     info->factored = t->factored ? 1 : 0;
     info->nrhs = t->nrhs;
@@ -1077,54 +1184,97 @@ int rb_tree_sample_points(const rb_tree* t, int which, double* xyz) {
     if (!t || !xyz) return RB_ERR_INVALID;
     const Plan& P = t->P;
     const PlanLevel& lf = P.lv[P.L];
-    const int a = lf.a, b = lf.b, nl = lf.nnodes;
-    // grid2real (fd_module.f90:669-700): lo + g*h - h/2, snapped to the face on the boundary
-    auto coord = [&](int leaf, int gi, int gj, const double* h, double* out) {
+    const int a = lf.a, b = lf.b, c = lf.c, nl = lf.nnodes, d = P.d;
+    // grid2real (fd_module.f90:669-700): lo + g*h - h/2, snapped to the face on the boundary; in 2D
+    // the third coordinate is lo_z (gk = 1, h_z = 0)
+    auto coord = [&](int leaf, int gi, int gj, int gk, const double* h, double* out) {
         const double* lo = &lf.lo[3 * leaf];
         const double* hi = &lf.hi[3 * leaf];
-        out[0] = (lo[0] + gi * h[0]) - h[0] / 2;
-        out[1] = (lo[1] + gj * h[1]) - h[1] / 2;
-        out[2] = (lo[2] + 1 * h[2]) - h[2] / 2;
-        if (gi == 0) out[0] = lo[0]; else if (gi == a + 1) out[0] = hi[0];
-        if (gj == 0) out[1] = lo[1]; else if (gj == b + 1) out[1] = hi[1];
+        const int g[3] = {gi, gj, gk}, sh[3] = {a, b, c};
+        for (int ax = 0; ax < 3; ++ax) {
+            out[ax] = (lo[ax] + g[ax] * h[ax]) - h[ax] / 2;
+            if (ax < d) {
+                if (g[ax] == 0) out[ax] = lo[ax];
+                else if (g[ax] == sh[ax] + 1) out[ax] = hi[ax];
+            }
+        }
     };
+    // the points of face f (0-based) of a leaf in the face's own order (lin2fgrid,
+    // fd_module.f90:867-939): the first tangential index fastest
+    auto face_grid = [&](int f, int s1, int s2, int* g) {
+        const int ax = f / 2, fix = (f % 2 == 0) ? 0 : (ax == 0 ? a : ax == 1 ? b : c) + 1;
+        int tang[2], q = 0;
+        for (int k = 0; k < 3; ++k)
+            if (k != ax) tang[q++] = k;
+        g[ax] = fix;
+        g[tang[0]] = s1;
+        g[tang[1]] = s2;
+        if (d == 2) g[2] = 1;
+    };
+    auto face_dims = [&](int f, int& n1, int& n2) {
+        const int ax = f / 2, sh[3] = {a, b, c};
+        int q = 0, dims[2] = {1, 1};
+        for (int k = 0; k < d; ++k)
+            if (k != ax) dims[q++] = sh[k];
+        n1 = dims[0];
+        n2 = dims[1];
+    };
+    const int nf = P.nf();
     size_t q = 0;
     if (which == RB_POINTS_POTENTIAL || which == RB_POINTS_SOURCE) {
         for (int i = 0; i < nl; ++i) {
-            double h[3] = {P.leaf_h[2 * i], P.leaf_h[2 * i + 1], 0.0};
+            double h[3] = {0.0, 0.0, 0.0};
+            for (int k = 0; k < d; ++k) h[k] = P.leaf_h[(size_t)d * i + k];
             const double* hp = which == RB_POINTS_POTENTIAL ? h : P.h_last;
-            for (int gj = 1; gj <= b; ++gj)
-                for (int gi = 1; gi <= a; ++gi, ++q) coord(i, gi, gj, hp, xyz + 3 * q);
+            for (int gk = 1; gk <= c; ++gk)
+                for (int gj = 1; gj <= b; ++gj)
+                    for (int gi = 1; gi <= a; ++gi, ++q) coord(i, gi, gj, gk, hp, xyz + 3 * q);
         }
         return RB_OK;
     }
     if (which == RB_POINTS_BOUNDARY) {
-        for (int f = 0; f < 4; ++f)
+        // the root's faces in turn; a face's points are its leaves' in leaf order (a merged face
+        // is child1's part then child2's), each leaf's in the face's own order
+        for (int f = 0; f < nf; ++f)
             for (int i = 0; i < nl; ++i) {
-                if (!lf.isb[4 * i + f]) continue;
-                const int cnt = f < 2 ? b : a;
-                for (int s = 1; s <= cnt; ++s, ++q) {
-                    double pt[3];
-                    if (f == 0) coord(i, 0, s, P.h_last, pt);
-                    else if (f == 1) coord(i, a + 1, s, P.h_last, pt);
-                    else if (f == 2) coord(i, s, 0, P.h_last, pt);
-                    else coord(i, s, b + 1, P.h_last, pt);
-                    // face-local coordinates as fd_make_bndry_vec leaves them (fd_module.f90:648-649)
-                    xyz[3 * q] = f < 2 ? pt[1] : pt[0];
-                    xyz[3 * q + 1] = 0.0;
-                    xyz[3 * q + 2] = 0.0;
-                }
+                if (!lf.isb[(size_t)nf * i + f]) continue;
+                int n1, n2;
+                face_dims(f, n1, n2);
+                const int ax = f / 2;
+                for (int s2 = 1; s2 <= n2; ++s2)
+                    for (int s1 = 1; s1 <= n1; ++s1, ++q) {
+                        int g[3];
+                        face_grid(f, s1, s2, g);
+                        double pt[3];
+                        coord(i, g[0], g[1], g[2], P.h_last, pt);
+                        // face-local coordinates as fd_make_bndry_vec leaves them (fd_module.f90:636-651):
+                        // the tangential coordinates in natural order
+                        int k = 0;
+                        double loc[3] = {0.0, 0.0, 0.0};
+                        for (int t2 = 0; t2 < d; ++t2)
+                            if (t2 != ax) loc[k++] = pt[t2];
+                        xyz[3 * q] = loc[0];
+                        xyz[3 * q + 1] = loc[1];
+                        xyz[3 * q + 2] = 0.0;
+                    }
             }
         return RB_OK;
     }
     if (which == RB_POINTS_SOLUTION) {
         for (int i = 0; i < nl; ++i) {
-            for (int s = 1; s <= b; ++s, ++q) coord(i, 0, s, P.h_last, xyz + 3 * q);
-            for (int s = 1; s <= b; ++s, ++q) coord(i, a + 1, s, P.h_last, xyz + 3 * q);
-            for (int s = 1; s <= a; ++s, ++q) coord(i, s, 0, P.h_last, xyz + 3 * q);
-            for (int s = 1; s <= a; ++s, ++q) coord(i, s, b + 1, P.h_last, xyz + 3 * q);
-            for (int gj = 1; gj <= b; ++gj)
-                for (int gi = 1; gi <= a; ++gi, ++q) coord(i, gi, gj, P.h_last, xyz + 3 * q);
+            for (int f = 0; f < nf; ++f) {
+                int n1, n2;
+                face_dims(f, n1, n2);
+                for (int s2 = 1; s2 <= n2; ++s2)
+                    for (int s1 = 1; s1 <= n1; ++s1, ++q) {
+                        int g[3];
+                        face_grid(f, s1, s2, g);
+                        coord(i, g[0], g[1], g[2], P.h_last, xyz + 3 * q);
+                    }
+            }
+            for (int gk = 1; gk <= c; ++gk)
+                for (int gj = 1; gj <= b; ++gj)
+                    for (int gi = 1; gi <= a; ++gi, ++q) coord(i, gi, gj, gk, P.h_last, xyz + 3 * q);
         }
         return RB_OK;
     }
@@ -1206,6 +1356,8 @@ static int factor_common(rb_tree* t, const double* k, int precision, bool host, 
     if (!k) return fail(t, RB_ERR_INVALID, "rb_tree_factor: null potential samples");
     if (precision != RB_PREC_FP64 && precision != RB_PREC_MIXED)
         return fail(t, RB_ERR_INVALID, "precision mode " + std::to_string(precision) + " is not defined");
+    if (precision == RB_PREC_MIXED && t->P.d != 2)
+        return fail(t, RB_ERR_UNSUPPORTED, "the mixed-precision factorization is 2D only");
     int rc = ensure_factor_storage(t);
     if (rc) return rc;
     // a previous factor nobody waited for: report it, unless this call asks not to wait at all;
@@ -1214,7 +1366,7 @@ static int factor_common(rb_tree* t, const double* k, int precision, bool host, 
     if (!host && !sync) t->factor_pending = false;
     else if ((rc = settle_factor(t))) return rc;
     const Plan& P = t->P;
-    const size_t nint = (size_t)P.nleaves() * P.leaf_a() * P.leaf_b();
+    const size_t nint = (size_t)P.nleaves() * P.leaf_interior();
     t->factored = false;
     t->nrhs = 0;
     if (precision != t->prec) {
@@ -1223,6 +1375,7 @@ static int factor_common(rb_tree* t, const double* k, int precision, bool host, 
         drop_graph(t->gx_factor);
         t->factor_runs = 0;
     }
+    if (precision == RB_PREC_MIXED && (rc = ensure_mixed_factor_plan(t))) return rc;
     if (t->timing == 1) {
         timers_collect(t);
         t->stage_ms.clear();
@@ -1265,7 +1418,7 @@ static int solve_common(rb_tree* t, int nrhs, const double* f, const double* g, 
     int rc = ensure_solve_storage(t, nrhs);
     if (rc) return rc;
     const Plan& P = t->P;
-    const size_t nint = (size_t)P.nleaves() * P.leaf_a() * P.leaf_b();
+    const size_t nint = (size_t)P.nleaves() * P.leaf_interior();
     const size_t nroot = (size_t)P.lv[0].nb;
     const cudaMemcpyKind kind = host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice;
     t->nrhs = 0;
@@ -1479,6 +1632,7 @@ int rb_tree_level_shape(const rb_tree* t, int level, int32_t* shape) {
     shape[0] = t->P.lv[level].nnodes;
     shape[1] = t->P.lv[level].a;
     shape[2] = t->P.lv[level].b;
+    shape[3] = t->P.lv[level].c;
     return RB_OK;
 }
 
@@ -1558,8 +1712,8 @@ int tree_device(const rb_tree* t) { return t->device; }
 // vectors, its split-K workspace bound and, for a mixed-precision factor, the refinement buffers)
 double tree_bytes_estimate(const rb_tree* t, int nrhs, int precision) {
     const Plan& Q = t->P;
-    const double ab = (double)Q.leaf_a() * Q.leaf_b();
-    double need = (double)Q.nleaves() * (ab * Q.leaf_a() + (double)Q.leaf_nb() * Q.leaf_n() + ab) * 16.0;
+    const double ab = (double)Q.leaf_interior();
+    double need = leaf_factor_bytes(Q);
     double per_rhs = (double)Q.nleaves() * (ab + Q.leaf_n()) * 16.0;
     for (int l = 0; l < Q.L; ++l) {
         need += (double)Q.lv[l].nnodes *
@@ -1581,7 +1735,7 @@ static int ensure_points(rb_tree* t, int which, double** out) {
     if (!t->d_pts[idx]) {
         const Plan& P = t->P;
         const size_t n = which == RB_POINTS_BOUNDARY ? (size_t)P.lv[0].nb
-                                                     : (size_t)P.nleaves() * P.leaf_a() * P.leaf_b();
+                                                     : (size_t)P.nleaves() * P.leaf_interior();
         std::vector<double> h(3 * n);
         int rc = rb_tree_sample_points(t, which, h.data());
         if (rc) return rc;
@@ -1609,7 +1763,7 @@ int rb_tree_sample_device(rb_tree* t, int kind, int count, const double* params,
     int rc;
     if (!t->stream) RB_CK(cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking));
     const Plan& P = t->P;
-    const long long nint = (long long)P.nleaves() * P.leaf_a() * P.leaf_b();
+    const long long nint = (long long)P.nleaves() * P.leaf_interior();
     const int nb = P.lv[0].nb;
     cudaStream_t s = t->stream;
     double* pts = nullptr;
@@ -1671,7 +1825,7 @@ static std::vector<std::pair<z*, size_t>> factor_sections(rb_tree* t) {
     const Plan& P = t->P;
     const size_t nl = P.nleaves(), a = P.leaf_a(), b = P.leaf_b(), nb = P.leaf_nb(), n = P.leaf_n();
     std::vector<std::pair<z*, size_t>> v;
-    v.push_back({t->leaf_sinv, nl * b * a * a});
+    v.push_back({t->leaf_sinv, P.d == 2 ? nl * b * a * a : nl * n * n});   // 3D: the dense leaf inverses
     v.push_back({t->leaf_Y, nl * nb * n});
     for (int l = 0; l < P.L; ++l) {
         const PlanLevel& p = P.lv[l];

@@ -74,8 +74,11 @@ struct rb_tree {
     // persistent factor storage
     double* d_h = nullptr;
     z* d_k = nullptr;
-    z* leaf_sinv = nullptr;
+    z* leaf_sinv = nullptr;          // 2D: the leaves' Sig_j^-1 blocks; 3D: each leaf's dense A^-1
     z* leaf_Y = nullptr;
+    GJBatch gj_leaf;                 // 3D: the leaves' Gauss-Jordan inversions (A^-1 in leaf_sinv)
+    int* leaf_ipiv = nullptr;
+    z* leaf_gjwork = nullptr;
     std::vector<z*> rtr;             // per level < L
     std::vector<z*> dinv, sinv;      // per level < L: inv(D), inv(S); in the K form A2, A1
     // K form of the interface solve (nu not small): one inversion per node instead of two
@@ -103,6 +106,7 @@ struct rb_tree {
     z* tmp = nullptr;
     z* sol = nullptr;
     GemmBatch sL0;
+    GemmBatch sLg, sLf;              // 3D leaf solve: u = A^-1(:, :nb) g, then u += A^-1(:, nb:) f
     std::vector<GemmBatch> sF12, sF3, sF4, sF5, sBY;
     GemmBatch sR1;                   // root: x_i = h_i + T_iN g_N (no K^-1 needed)
     std::vector<DevBuf> solve_bufs;
@@ -134,6 +138,8 @@ struct rb_tree {
     int* d_bclass = nullptr;
     std::vector<int*> d_ifrows;
     int refine_cap = 0;
+    bool mixed_plan = false;          // split-K plans and workspaces of the tcgen05 factor stages
+    std::vector<DevBuf> mixed_bufs;
     z* dsol = nullptr;                // the correction of the current refinement step
     z* d_ri = nullptr;                // interface rows of the residual [rhs][leaf][nb]
     double* d_norms = nullptr;        // [0, k) max|r|, [k, 2k) max|x|, [2k, 3k) max|dx|
