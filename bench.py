@@ -84,6 +84,9 @@ def parse():
     ap.add_argument("--requests", type=int, default=4000, help="solve requests per offered load (--serve)")
     ap.add_argument("--forest", action="store_true",
                     help="batching bench: 64 trees of uneven sizes factored as one forest vs one at a time")
+    ap.add_argument("--three-d", action="store_true",
+                    help="3D bench: factor and 8-RHS solve of the unit cube at 16^3 (L=6) and 32^3 (L=9), "
+                         "4^3 leaves, with the manufactured solution's error")
     return ap.parse_args()
 
 
@@ -588,6 +591,19 @@ def our_arm(args):
         pass
     roof = roofline_block(arms[main], torch, dev, args.steps, zpeak, peaks.get("bf16_tflops"))
 
+    # ---- forward errors against the FP64 CPU solve: joined here, so that the SuperLU process (all host
+    # cores, ~10 GB of host memory traffic) is done before the host-copy-bound e2e leg is timed ----------
+    from oracle import fd_global as FG
+    fwd = None
+    if superlu is not None:
+        pool, job = superlu
+        ref = job.get(timeout=1800)
+        pool.close()
+        pool.join()
+        fwd = {p: max(FG.forward_error(U[p][r], ref[i]) for i, r in enumerate(check_rows)) for p in U}
+        fwd["rhs_checked"] = check_rows
+        fwd["reference"] = "SuperLU solve of the assembled global FD system (oracle/fd_global.SparseFD), FP64, CPU"
+
     # ---- e2e through the host C-ABI ---------------------------------------------------------------------
     e2e = None
     if not args.no_e2e:
@@ -630,19 +646,9 @@ def our_arm(args):
     else:
         U_e2e = U[main]
 
-    # backward error of the solutions the user read back; forward errors against SuperLU
-    from oracle import fd_global as FG
+    # backward error of the solutions the user read back
     bw = max(FG.backward_error(wl.L, wl.domain, wl.h_tgt, wl.opts_kb, wl.bndry_params, kv.reshape(nleaf, -1),
                                U_e2e[r], F[r].reshape(nleaf, -1), G[r]) for r in check_rows)
-    fwd = None
-    if superlu is not None:
-        pool, job = superlu
-        ref = job.get(timeout=1800)
-        pool.close()
-        pool.join()
-        fwd = {p: max(FG.forward_error(U[p][r], ref[i]) for i, r in enumerate(check_rows)) for p in U}
-        fwd["rhs_checked"] = check_rows
-        fwd["reference"] = "SuperLU solve of the assembled global FD system (oracle/fd_global.SparseFD), FP64, CPU"
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -923,8 +929,86 @@ def forest_arm(args):
     return 0
 
 
+def three_d_arm(args):
+    """The 3D path (d = 3): the unit cube, 4^3-cell leaves, k = 1, kb = 1, bndry_params of the
+    reference's example, boundary data of the exact solution cos(x/sqrt3) cos(y/sqrt3) cos(z/sqrt3)
+    (Laplace u + u = 0).  Per grid: factor time (library device events, graph replay), solve time for
+    8 right-hand sides, the factor's stage shares (timing mode 1), and the max-norm error against the
+    exact solution (O(h^2) discretisation error, not a parity figure: parity is in the tests)."""
+    import torch
+
+    import robinsolver_b200 as rb
+    from robinsolver_b200 import _lib
+
+    torch.cuda.set_device(0)
+    s3 = 1.0 / np.sqrt(3.0)
+    dom = np.array([[0.0, 0.0, 0.0], [1.0, 1.0, 1.0]])
+
+    def exact(X):
+        return np.cos(s3 * X[:, 0]) * np.cos(s3 * X[:, 1]) * np.cos(s3 * X[:, 2])
+
+    def face(f):
+        ax, side = f // 2, f % 2
+        tang = [t for t in range(3) if t != ax]
+
+        def g(P):
+            X = np.zeros((P.shape[0], 3))
+            X[:, ax] = dom[side, ax]
+            X[:, tang[0]], X[:, tang[1]] = P[:, 0], P[:, 1]
+            d = -s3 * np.sin(s3 * X[:, ax])
+            for j in tang:
+                d = d * np.cos(s3 * X[:, j])
+            return (1.0 if side else -1.0) * d + 1j * exact(X)
+        return g
+
+    out = {"metric": "3D factor ms and 8-RHS solve ms (FP64, unit cube, 4^3 leaves)", "grids": {}}
+    for N, L in ((16, 6), (32, 9)):
+        T = rb.robin_tree()
+        T.bndry_params = np.array([[1j, 1.0], [-1j, 1.0]])
+        op = rb.elliptic_operator(d=3, domain=dom, k=lambda X: np.ones(X.shape[0], dtype=complex))
+        opts = rb.solve_opts(h_tgt=1.0 / N, kb=1.0)
+        T.factor(L, op, opts)
+        rhs = [rb.elliptic_rhs(d=3, f=lambda X: np.zeros(X.shape[0]), g=[face(f) for f in range(6)])] * 8
+        F, G = T.sample_rhs(rhs)
+        kv = np.ones(T.info().n_interior, dtype=np.complex128)
+        fts, sts = [], []
+        for it in range(max(3, args.warmup) + max(3, args.steps)):
+            T.factor_samples(kv)
+            T.solve_samples(F, G)
+            if it >= max(3, args.warmup):
+                fts.append(T.f_time)
+                sts.append(T.s_time)
+        X = T.sample_points(_lib.RB_POINTS_SOLUTION)
+        err = float(np.max(np.abs(T.solution_array(0).ravel() - exact(X))))
+        T.set_timing(1)
+        T.clear_stage_times()
+        T.factor_samples(kv)
+        st = T.stage_times(with_flops=True)
+        T.set_timing(0)
+        tot = sum(ms for _, ms, _ in st) or 1.0
+        fam = {}
+        for name, ms, fl in st:
+            a = fam.setdefault(name, [0.0, 0.0])
+            a[0] += ms
+            a[1] += fl
+        inf = T.info()
+        out["grids"][f"{N}^3 L={L}"] = {
+            "leaves": inf.nleaves, "leaf_unknowns": inf.leaf_n, "root_boundary": inf.root_nb,
+            "factor_ms": float(np.median(fts)) * 1e3, "solve_8rhs_ms": float(np.median(sts)) * 1e3,
+            "max_err_vs_exact": err,
+            "factor_stages": {k: {"ms": round(v[0], 3), "share": round(v[0] / tot, 3),
+                                  "tflops": round(v[1] / v[0] / 1e9, 2) if v[0] > 0 and v[1] > 0 else None}
+                              for k, v in sorted(fam.items(), key=lambda kv: -kv[1][0])},
+        }
+        T.close()
+    print(json.dumps(out), flush=True)
+    return 0
+
+
 def main():
     args = parse()
+    if args.three_d:
+        return three_d_arm(args)
     if args.serve:
         return serve_arm(args)
     if args.forest:

@@ -165,10 +165,12 @@ def _load():
         "rb_forest_tuning": (C.c_int, [P, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32), D,
                                        C.c_int]),
         "rb_gemm_engine_name": (C.c_char_p, [C.c_int]),
-        # test hook of the GEMM engines (rb_testing.cpp), not part of the drop-in boundary
+        # test hooks of the GEMM engines (rb_testing.cpp), not part of the drop-in boundary
         "rb_test_zgemm": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_longlong, C.c_longlong, P,
                                     C.c_longlong, C.c_longlong, P, C.c_longlong, C.c_longlong, C.c_double,
                                     C.c_double, C.c_double, C.c_double, C.c_int]),
+        # test hook of the batched Gauss-Jordan inversion (rb_testing.cpp)
+        "rb_test_zinvert": (C.c_int, [C.c_int, C.c_int, P, C.c_longlong, C.c_longlong, C.c_int, D]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -1,4 +1,4 @@
-// rb_testing.cpp -- test hooks of the GEMM engines, outside the drop-in C-ABI.
+// rb_testing.cpp -- test hooks of the GEMM and inversion engines, outside the drop-in C-ABI.
 //
 // rb_test_zgemm runs `count` complex GEMMs D_i = alpha A_i B_i + beta D_i (column-major, device
 // pointers, plain strided views) on one engine, so that the tests can hold each engine against a
@@ -64,4 +64,64 @@ extern "C" int rb_test_zgemm(int engine, int m, int n, int k, const double* dA, 
     cudaFree(b.d_desc);
     cudaFree(d_status);
     return rc;
+}
+
+// rb_test_zinvert inverts `count` complex m x m matrices in place (column-major, device pointers,
+// A_i = dA + i * stride, leading dimension ld) with the batched Gauss-Jordan kernels of the
+// factorization, `reps` times in a row (each call inverts the previous result), and writes the
+// mean device time of one batched inversion in milliseconds to *ms (may be null).  It returns 0,
+// a negative RB_ERR_* code, or the device status word's bits (> 0) when a kernel reported one
+// (1: a zero pivot; 2: a resident CTA gave up waiting).
+extern "C" int rb_test_zinvert(int m, int count, double* dA, long long ld, long long stride, int reps, double* ms) {
+    if (m <= 0 || count <= 0 || reps <= 0 || !dA || ld < m || (count > 1 && stride < ld * m)) return RB_ERR_INVALID;
+    z* A = reinterpret_cast<z*>(dA);
+    const long long ws = gj_workspace_elems(m);
+    std::vector<GJDesc> h(count);
+    GJDesc* d_desc = nullptr;
+    int* d_ipiv = nullptr;
+    int* d_status = nullptr;
+    z* d_work = nullptr;
+    auto release = [&]() {
+        cudaFree(d_desc);
+        cudaFree(d_ipiv);
+        cudaFree(d_status);
+        cudaFree(d_work);
+    };
+    cudaError_t e = cudaMalloc(&d_desc, sizeof(GJDesc) * count);
+    if (e == cudaSuccess) e = cudaMalloc(&d_ipiv, sizeof(int) * (size_t)m * count);
+    if (e == cudaSuccess) e = cudaMalloc(&d_status, sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&d_work, sizeof(z) * (size_t)std::max<long long>(1, ws * count));
+    if (e != cudaSuccess) {
+        release();
+        set_thread_error((std::string("rb_test_zinvert: ") + cudaGetErrorString(e)).c_str());
+        return RB_ERR_CUDA;
+    }
+    for (int i = 0; i < count; ++i) {
+        h[i].A = A + (long long)i * stride;
+        h[i].ld = ld;
+        h[i].ipiv = d_ipiv + (long long)i * m;
+        h[i].Zb = d_work + (long long)i * ws;
+    }
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    e = cudaMemcpy(d_desc, h.data(), sizeof(GJDesc) * count, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(d_status, 0, sizeof(int));
+    if (e == cudaSuccess) e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e == cudaSuccess) e = cudaEventRecord(e0, 0);
+    for (int r = 0; r < reps && e == cudaSuccess; ++r) e = gj_invert_batch(d_desc, count, m, d_work, d_status, 0);
+    if (e == cudaSuccess) e = cudaEventRecord(e1, 0);
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    float t = 0.0f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+    int st = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&st, d_status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    release();
+    if (e != cudaSuccess) {
+        set_thread_error((std::string("rb_test_zinvert: ") + cudaGetErrorString(e)).c_str());
+        return RB_ERR_CUDA;
+    }
+    if (ms) *ms = t / reps;
+    return st;
 }
