@@ -293,11 +293,15 @@ __device__ bool cta_wait_geq(const int* flag, int target, int* status, int* s_ok
     return ok;
 }
 
+// Slots of one elimination column, double-buffered by column parity: column kk writes set kk & 1,
+// so a column's slots are rewritten two columns later, after every thread has passed the block
+// barrier that follows its last read of them -- one barrier per column fewer than single slots.
 template <int NB>
 struct ResShared {
-    z xb[NB], prow[NB];
-    unsigned kh[32], kl[32];
-    int ki[32];
+    z xb[2][NB], prow[2][NB];
+    unsigned kh[2][32], kl[2][32];
+    int ki[2][32];
+    int spv[NB];                         // pivots of the step being applied
     int ok;
 };
 
@@ -311,48 +315,41 @@ __device__ __forceinline__ void warp_key_max(unsigned& hi, unsigned& lo, int& id
     lo = ml;
 }
 
-// CTA-wide argmax of v over the valid rows (largest first, then smallest row): one block
-// barrier; every thread gets the row
+// CTA-wide argmax of v over the valid rows (largest first, then smallest row), in slot set b:
+// one block barrier; every thread gets the row
 template <int NB>
-__device__ __forceinline__ int block_argmax(double v, bool valid, int r, ResShared<NB>& sh) {
+__device__ __forceinline__ int block_argmax(double v, bool valid, int r, ResShared<NB>& sh, int b) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = (blockDim.x + 31) >> 5;
     unsigned hi = valid ? (unsigned)__double2hiint(v) : 0u;
     unsigned lo = valid ? (unsigned)__double2loint(v) : 0u;
     int id = valid ? r : 0x7fffffff;
     warp_key_max(hi, lo, id);
     if (lane == 0) {
-        sh.kh[warp] = hi;
-        sh.kl[warp] = lo;
-        sh.ki[warp] = id;
+        sh.kh[b][warp] = hi;
+        sh.kl[b][warp] = lo;
+        sh.ki[b][warp] = id;
     }
     __syncthreads();
-    hi = lane < nwarps ? sh.kh[lane] : 0u;
-    lo = lane < nwarps ? sh.kl[lane] : 0u;
-    id = lane < nwarps ? sh.ki[lane] : 0x7fffffff;
+    hi = lane < nwarps ? sh.kh[b][lane] : 0u;
+    lo = lane < nwarps ? sh.kl[b][lane] : 0u;
+    id = lane < nwarps ? sh.ki[b][lane] : 0x7fffffff;
     warp_key_max(hi, lo, id);
     return id;
 }
 
-// Eliminates the panel held at local columns [q0, q0+nbk) (matrix columns k0..): RPT rows per
-// thread (rows tid + i*blockDim.x) in registers, two block barriers per column (pivot
-// candidates; scaled pivot row and displaced row).  W is left in the local columns and copied
-// to Wg (ld wld); pivots go to ipiv.
+// Eliminates a panel of nbk columns (matrix columns k0..) whose current values are in row[][]:
+// RPT rows per thread (rows tid + i*blockDim.x), two block barriers per column (pivot candidates;
+// scaled pivot row and displaced row).  On return row[][] holds the panel's transform W and the
+// pivots are in ipiv.
 template <int NB, int RPT>
-__device__ __noinline__ void res_eliminate(z* cols, int m, int q0, int k0, int nbk, z* Wg, long long wld, int* ipiv,
-                                           int* status, ResShared<NB>& sh) {
+__device__ __forceinline__ void res_eliminate_regs(z (&row)[RPT][NB], int m, int k0, int nbk, int* ipiv, int* status,
+                                                   ResShared<NB>& sh) {
     const int tid = threadIdx.x, nt = blockDim.x;
-    z row[RPT][NB];
-#pragma unroll
-    for (int i = 0; i < RPT; ++i) {
-        const int r = tid + i * nt;
-#pragma unroll
-        for (int kk = 0; kk < NB; ++kk) row[i][kk] = (r < m && kk < nbk) ? cols[r + (q0 + kk) * m] : zmk(0.0, 0.0);
-    }
     bool bad = false;
 #pragma unroll
     for (int kk = 0; kk < NB; ++kk) {
         if (kk >= nbk) break;
-        const int c = k0 + kk;
+        const int c = k0 + kk, b = kk & 1;
         // this thread's candidate: its largest entry on or below row c, first on ties
         double v = 0.0;
         int vr = -1;
@@ -362,7 +359,7 @@ __device__ __noinline__ void res_eliminate(z* cols, int m, int q0, int k0, int n
             const double a = zabs1(row[i][kk]);
             if (r < m && r >= c && (vr < 0 || a > v)) { v = a; vr = r; }
         }
-        const int p = block_argmax<NB>(v, vr >= 0, vr, sh);
+        const int p = block_argmax<NB>(v, vr >= 0, vr, sh, b);
 #pragma unroll
         for (int i = 0; i < RPT; ++i) {
             const int r = tid + i * nt;
@@ -370,12 +367,12 @@ __device__ __noinline__ void res_eliminate(z* cols, int m, int q0, int k0, int n
                 if (zis0(row[i][kk])) bad = true;
                 const z pinv = zrcp(row[i][kk]);
 #pragma unroll
-                for (int j = 0; j < NB; ++j) sh.prow[j] = (j == kk) ? pinv : zmul(row[i][j], pinv);
+                for (int j = 0; j < NB; ++j) sh.prow[b][j] = (j == kk) ? pinv : zmul(row[i][j], pinv);
                 ipiv[c] = p;
             }
             if (r == c && p != c) {
 #pragma unroll
-                for (int j = 0; j < NB; ++j) sh.xb[j] = row[i][j];
+                for (int j = 0; j < NB; ++j) sh.xb[b][j] = row[i][j];
             }
         }
         __syncthreads();
@@ -384,21 +381,29 @@ __device__ __noinline__ void res_eliminate(z* cols, int m, int q0, int k0, int n
             const int r = tid + i * nt;
             if (r == c) {
 #pragma unroll
-                for (int j = 0; j < NB; ++j) row[i][j] = sh.prow[j];
+                for (int j = 0; j < NB; ++j) row[i][j] = sh.prow[b][j];
             } else if (r < m) {
                 if (r == p) {
 #pragma unroll
-                    for (int j = 0; j < NB; ++j) row[i][j] = sh.xb[j];
+                    for (int j = 0; j < NB; ++j) row[i][j] = sh.xb[b][j];
                 }
                 const z f = row[i][kk];
 #pragma unroll
                 for (int j = 0; j < NB; ++j)
-                    if (j != kk) zfms(row[i][j], f, sh.prow[j]);
-                row[i][kk] = zneg(zmul(f, sh.prow[kk]));
+                    if (j != kk) zfms(row[i][j], f, sh.prow[b][j]);
+                row[i][kk] = zneg(zmul(f, sh.prow[b][kk]));
             }
         }
-        __syncthreads();                 // prow / xb / candidate slots are rewritten next column
     }
+    if (bad) atomicOr(status, 1);
+}
+
+// Stores an eliminated panel: W to the local columns [q0, q0+nbk) and to Wg (ld wld), then a
+// block barrier.
+template <int NB, int RPT>
+__device__ __forceinline__ void res_store_panel(const z (&row)[RPT][NB], z* cols, int m, int q0, int nbk, z* Wg,
+                                                long long wld) {
+    const int tid = threadIdx.x, nt = blockDim.x;
 #pragma unroll
     for (int i = 0; i < RPT; ++i) {
         const int r = tid + i * nt;
@@ -410,12 +415,27 @@ __device__ __noinline__ void res_eliminate(z* cols, int m, int q0, int k0, int n
             Wg[r + (long long)kk * wld] = row[i][kk];
         }
     }
-    if (bad) atomicOr(status, 1);
     __syncthreads();
 }
 
-// Applies step (panel at matrix columns k0.., nbk wide, pivots at piv, W at W with ld wld, read
-// through L2 when w_global) to the local columns [qa, qb) except [xa, xb).  The panel's row
+// Eliminates the panel held at local columns [q0, q0+nbk) (matrix columns k0..) and stores it.
+template <int NB, int RPT>
+__device__ __noinline__ void res_eliminate(z* cols, int m, int q0, int k0, int nbk, z* Wg, long long wld, int* ipiv,
+                                           int* status, ResShared<NB>& sh) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    z row[RPT][NB];
+#pragma unroll
+    for (int i = 0; i < RPT; ++i) {
+        const int r = tid + i * nt;
+#pragma unroll
+        for (int kk = 0; kk < NB; ++kk) row[i][kk] = (r < m && kk < nbk) ? cols[r + (q0 + kk) * m] : zmk(0.0, 0.0);
+    }
+    res_eliminate_regs<NB, RPT>(row, m, k0, nbk, ipiv, status, sh);
+    res_store_panel<NB, RPT>(row, cols, m, q0, nbk, Wg, wld);
+}
+
+// Applies step (panel at matrix columns k0.., nbk wide, pivots at piv (shared memory), W at W with
+// ld wld, read through L2 when w_global) to the local columns [qa, qb) except [xa, xb).  The panel's row
 // exchanges move only the panel rows and the pivot rows below the panel; their exchanged values
 // (row a takes stored row src(a), src = the transpositions traced backwards) are gathered in
 // parallel into zs (2*NB slots per column: slot t < NB panel row k0+t, slot NB+t pivot row t
@@ -431,7 +451,7 @@ __device__ __noinline__ void res_apply(z* cols, z* zs, int m, int k0, int nbk, c
     {
         int pv[NB];
 #pragma unroll
-        for (int kk = 0; kk < NB; ++kk) pv[kk] = kk < nbk ? __ldcg(piv + kk) : -1;
+        for (int kk = 0; kk < NB; ++kk) pv[kk] = kk < nbk ? piv[kk] : -1;
         for (int e = tid; e < 2 * NB * nq; e += nt) {
             const int t = e % (2 * NB), q = qa + e / (2 * NB);
             if (q >= xa && q < xb) continue;
@@ -529,9 +549,13 @@ __global__ void __launch_bounds__(MAXT, MAXT <= 256 ? 512 / MAXT : 1) gj_residen
         const int k0 = p * NB, nbk = min(NB, m - k0);
         const bool own = p >= pa && p < pb;
         if (!own && !cta_wait_geq(pub, p + 1, status, &sh.ok)) return;
+        // the step's pivots, read once by the CTA: read by every thread, the same 32 bytes made an
+        // L2 hot spot of thousands of requests per step that cost the chain ~2.5 us a panel
+        if (tid < NB) sh.spv[tid] = tid < nbk ? __ldcg(g.ipiv + k0 + tid) : -1;
+        __syncthreads();
         const z* W = own ? cols + (size_t)(k0 - c0) * m : g.A + (long long)k0 * g.ld;
         const long long wld = own ? m : g.ld;
-        const int* piv = g.ipiv + k0;
+        const int* piv = sh.spv;
         const int xa = own ? k0 - c0 : 0, xb = own ? k0 - c0 + nbk : 0;
         const int nx = p + 1;
         if (nx < npanels && nx >= pa && nx < pb) {
