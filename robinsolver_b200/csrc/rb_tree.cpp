@@ -260,7 +260,16 @@ static int ensure_factor_storage(rb_tree* t) {
     int rc;
     RB_CK(cudaGetDevice(&t->device));
     if (!t->stream) RB_CK(cudaStreamCreateWithFlags(&t->stream, cudaStreamNonBlocking));
-    if (!t->stream2) RB_CK(cudaStreamCreateWithFlags(&t->stream2, cudaStreamNonBlocking));
+    {
+        // the level chain (stream2) and B1 (stream4) above the main stream, so that their CTAs are
+        // dispatched ahead of the waves of the large GEMM they overlap; the solve (stream3) above
+        // both
+        int least = 0, greatest = 0;
+        RB_CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        const int side = greatest < least ? std::max(greatest, least - 1 - (least - greatest) / 2) : least;
+        if (!t->stream2) RB_CK(cudaStreamCreateWithPriority(&t->stream2, cudaStreamNonBlocking, side));
+        if (!t->stream4) RB_CK(cudaStreamCreateWithPriority(&t->stream4, cudaStreamNonBlocking, side));
+    }
     if (!t->stream3) {
         // the solve runs here beside a factor: at the highest priority its small, latency-bound
         // kernels take SMs ahead of the factor's large GEMMs as their CTAs retire
@@ -280,6 +289,11 @@ static int ensure_factor_storage(rb_tree* t) {
     t->ev_lvl.assign(L + 1, nullptr);
     for (int l = 0; l <= L; ++l) RB_CK(cudaEventCreateWithFlags(&t->ev_lvl[l], cudaEventDisableTiming));
     if (!t->ev_root_forms) RB_CK(cudaEventCreateWithFlags(&t->ev_root_forms, cudaEventDisableTiming));
+    if (!t->ev_root_gj) RB_CK(cudaEventCreateWithFlags(&t->ev_root_gj, cudaEventDisableTiming));
+    for (auto* v : {&t->ev_face, &t->ev_rest, &t->ev_d, &t->ev_m1, &t->ev_m3}) {
+        v->assign(L + 1, nullptr);
+        for (auto& e : *v) RB_CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
     for (int l = 0; l < L; ++l) {
         RB_CK(cudaEventCreateWithFlags(&t->ev_fork[l], cudaEventDisableTiming));
         RB_CK(cudaEventCreateWithFlags(&t->ev_join[l], cudaEventDisableTiming));
@@ -361,6 +375,7 @@ static int ensure_factor_storage(rb_tree* t) {
     t->gj_s.resize(L);
     t->gj_k.resize(L);
     t->fK.resize(L); t->fM1.resize(L); t->fM2.resize(L); t->fM3.resize(L); t->fM4.resize(L);
+    t->fM4F.assign(L, GemmBatch()); t->fM4N.assign(L, GemmBatch());
     const z one = zmk(1.0, 0.0);
     const z mone = zmk(-1.0, 0.0);
     const z mnu = zneg(t->nu);
@@ -375,7 +390,43 @@ static int ensure_factor_storage(rb_tree* t) {
             if ((rc = upload_gj(t, t->bufs, gj_descs(t->sinv[l], (long long)m * m, m, nn, m), m, t->gj_s[l]))) return rc;
         }
         const ChildStore cs = child_store(t, l);
-        std::vector<GemmDesc> mk, m1, m2, m3, m4;
+        std::vector<GemmDesc> mk, m1, m2, m3, m4, m4f, m4n;
+        // The pipelined factor's row split of this level's parent maps (levels 1..L-1, K form): for
+        // a node that is its parent's child1 (par 0) or child2 (par 1), the rows of its map on the
+        // face the parent merges across, and the others.  Per child a of the node: sel = the rows'
+        // physical rows in child a's map (its non-interface points t, past the interface band),
+        // out = their rows in the node's map (pmap_a[t]).
+        int* d_sel[2][2][2] = {};
+        int* d_out[2][2][2] = {};
+        int cnt[2][2][2] = {};
+        const bool split = l >= 1 && t->kform;
+        if (split) {
+            const PlanLevel& pp = P.lv[l - 1];
+            for (int par = 0; par < 2; ++par) {
+                const int f = par == 0 ? pp.iface1 : pp.iface2;
+                const int lo = p.off[f - 1], hi = lo + p.pf[f - 1];
+                for (int a = 0; a < 2; ++a) {
+                    const std::vector<int>& pm = a == 0 ? p.pmap1 : p.pmap2;
+                    const int oa = a == 0 ? o1 : o2;
+                    std::vector<int> sel[2], out[2];
+                    for (int tt = 0; tt < (int)pm.size(); ++tt) {
+                        const int kind = (pm[tt] >= lo && pm[tt] < hi) ? 0 : 1;
+                        sel[kind].push_back(tt < oa ? tt : tt + m);
+                        out[kind].push_back(pm[tt]);
+                    }
+                    for (int kind = 0; kind < 2; ++kind) {
+                        cnt[par][a][kind] = (int)sel[kind].size();
+                        if (sel[kind].empty()) continue;
+                        if ((rc = alloc_n(t, t->bufs, sel[kind].size(), &d_sel[par][a][kind]))) return rc;
+                        if ((rc = alloc_n(t, t->bufs, out[kind].size(), &d_out[par][a][kind]))) return rc;
+                        RB_CK(cudaMemcpy(d_sel[par][a][kind], sel[kind].data(), sel[kind].size() * sizeof(int),
+                                         cudaMemcpyHostToDevice));
+                        RB_CK(cudaMemcpy(d_out[par][a][kind], out[kind].data(), out[kind].size() * sizeof(int),
+                                         cudaMemcpyHostToDevice));
+                    }
+                }
+            }
+        }
         for (int i = 0; i < nn; ++i) {
             const z* r1 = cs.rtr + (2LL * i) * cs.stride;
             const z* r2 = cs.rtr + (2LL * i + 1) * cs.stride;
@@ -443,6 +494,33 @@ static int ensure_factor_storage(rb_tree* t) {
                 g22.C = band_view(r2, ld, o2, m, o2, m);
                 g22.beta = one;
                 m4.push_back(g11); m4.push_back(g12); m4.push_back(g21); m4.push_back(g22);
+                if (split) {
+                    // the same four products, each split by rows into the face and the other rows:
+                    // T_a,Ni(rows, :) Y_b (+ T_a,NN(rows, :) when a = b), rows to pmap_a, columns to pmap_b
+                    const int par_ = i & 1;
+                    for (int kind = 0; kind < 2; ++kind)
+                        for (int a = 0; a < 2; ++a)
+                            for (int b2 = 0; b2 < 2; ++b2) {
+                                const int rows = cnt[par_][a][kind];
+                                if (rows == 0) continue;
+                                const z* ra = a == 0 ? r1 : r2;
+                                const int oa = a == 0 ? o1 : o2;
+                                ZView A = zview(ra + (long long)oa * ld, ld);
+                                A.rmap = d_sel[par_][a][kind];
+                                const z* yb = (a == 0 ? y1 : y2) + (b2 == 0 ? 0LL : (long long)m * n1);
+                                ZOut D = zout(par, p.nb);
+                                D.rmap = d_out[par_][a][kind];
+                                D.cmap = b2 == 0 ? t->d_pmap1[l] : t->d_pmap2[l];
+                                GemmDesc g = gdesc(rows, b2 == 0 ? n1 : n2, m, A, zview(yb, m), D, one);
+                                if (a == b2) {
+                                    ZView C = band_view(ra, ld, INT_MAX, 0, oa, m);
+                                    C.rmap = d_sel[par_][a][kind];
+                                    g.C = C;
+                                    g.beta = one;
+                                }
+                                (kind == 0 ? m4f : m4n).push_back(g);
+                            }
+                }
             }
         }
         if ((rc = upload_gemm(t, t->bufs, mk, t->fK[l]))) return rc;
@@ -450,6 +528,8 @@ static int ensure_factor_storage(rb_tree* t) {
         if ((rc = upload_gemm(t, t->bufs, m2, t->fM2[l]))) return rc;
         if ((rc = upload_gemm(t, t->bufs, m3, t->fM3[l]))) return rc;
         if ((rc = upload_gemm(t, t->bufs, m4, t->fM4[l]))) return rc;
+        if ((rc = upload_gemm(t, t->bufs, m4f, t->fM4F[l]))) return rc;
+        if ((rc = upload_gemm(t, t->bufs, m4n, t->fM4N[l]))) return rc;
     }
     t->factor_ready = true;
     return RB_OK;
@@ -529,6 +609,71 @@ static double leaf_flops(const LeafGeom& g) {
     return 8.0 * g.a * g.a * g.a * g.b + 16.0 * g.a * g.a * (double)g.nb * g.b;
 }
 
+// The FP64 K-form merges, pipelined across levels (all but the timed and mixed-precision runs).
+// Level l's parent map is formed in two row sets: the rows on the face its parent merges across
+// (fM4F), which are all the parent's interface system reads (A1, A2 and K from the ii blocks, B1
+// and Y1 from the iN blocks), and the other rows (fM4N).  The parent level's chain -- forms, K,
+// its Gauss-Jordan inversion, Y1, Y2 and its own face rows -- runs on a second stream as soon as
+// the face rows exist, beside the main stream's fM4N of the level below: the inversions, whose
+// serial panel chains keep most SMs waiting, overlap the largest GEMMs of the step.  B1 runs on
+// a third stream beside the inversion.  The two row sets of a map are disjoint, and no reader of
+// a map's other rows starts before its fM4N (the parent's own map and the solve's sweep at that
+// level wait for it); the root's map is formed whole, on the main stream, after the hook.
+static bool factor_pipelined(const rb_tree* t) {
+    static const bool off = [] {
+        const char* v = std::getenv("RB_FACTOR_PIPELINE");
+        return v && v[0] == '0';
+    }();
+    return !off && t->timing == 0 && t->kform && t->prec == RB_PREC_FP64 && t->P.L >= 2;
+}
+
+static int run_merges_pipelined(rb_tree* t, const std::vector<cudaEvent_t>* rec,
+                                const std::function<int()>* before_root_tail) {
+    const Plan& P = t->P;
+    const int L = P.L;
+    cudaStream_t s = t->stream, c = t->stream2, s4 = t->stream4;
+    int rc;
+    RB_CK(cudaEventRecord(t->ev_face[L], s));            // the leaves' maps, whole
+    RB_CK(cudaEventRecord(t->ev_rest[L], s));
+    for (int l = L - 1; l >= 0; --l) {
+        const PlanLevel& p = P.lv[l];
+        const ChildStore cs = child_store(t, l);
+        RB_CK(cudaStreamWaitEvent(c, t->ev_face[l + 1], 0));
+        RB_LAUNCH(merge_form_d(cs, p.nnodes, p.m, p.o2, t->zeta, t->dinv[l], c));
+        if (rec && l == 0) RB_CK(cudaEventRecord(t->ev_root_forms, c));
+        RB_CK(cudaEventRecord(t->ev_d[l], c));
+        RB_CK(cudaStreamWaitEvent(s4, t->ev_d[l], 0));
+        RB_LAUNCH(launch_gemm_batch(t->fM1[l], s4));          // B1 = -A2 T1_iN
+        RB_CK(cudaEventRecord(t->ev_m1[l], s4));
+        RB_LAUNCH(merge_form_s(cs, p.nnodes, p.m, p.o1, t->zeta, zmk(0.0, 0.0), t->dinv[l], t->sinv[l], c));
+        RB_LAUNCH(merge_form_k(p.nnodes, p.m, t->nu, t->kinv[l], c));
+        RB_LAUNCH(launch_gemm_batch(t->fK[l], c));
+        RB_LAUNCH(gj_invert_batch(t->gj_k[l].d_desc, p.nnodes, p.m, t->gj_work, t->d_status, c));
+        // from here on the children's maps are needed whole (this level's map; the solve's sweep)
+        RB_CK(cudaStreamWaitEvent(c, t->ev_rest[l + 1], 0));
+        if (rec) RB_CK(cudaEventRecord((*rec)[l], c));
+        RB_CK(cudaStreamWaitEvent(c, t->ev_m1[l], 0));
+        if (l == 0) {
+            RB_CK(cudaEventRecord(t->ev_root_gj, c));
+            RB_CK(cudaStreamWaitEvent(s, t->ev_root_gj, 0));   // joins both side streams
+            if (before_root_tail && (rc = (*before_root_tail)())) return rc;
+            RB_LAUNCH(launch_gemm_batch(t->fM2[0], s));
+            RB_LAUNCH(launch_gemm_batch(t->fM3[0], s));
+            RB_LAUNCH(launch_gemm_batch(t->fM4[0], s));
+        } else {
+            RB_LAUNCH(launch_gemm_batch(t->fM2[l], c));
+            RB_LAUNCH(launch_gemm_batch(t->fM3[l], c));
+            RB_CK(cudaEventRecord(t->ev_m3[l], c));
+            RB_LAUNCH(launch_gemm_batch(t->fM4F[l], c));
+            RB_CK(cudaEventRecord(t->ev_face[l], c));
+            RB_CK(cudaStreamWaitEvent(s, t->ev_m3[l], 0));
+            RB_LAUNCH(launch_gemm_batch(t->fM4N[l], s));
+            RB_CK(cudaEventRecord(t->ev_rest[l], s));
+        }
+    }
+    return RB_OK;
+}
+
 // rec (optional): events recorded as the factor progresses, for a solve on another stream
 // rec: progress events, one per level (the leaves at L), for a solve that overlaps the factor.
 // before_root_tail: enqueued once the root's interface inverse is ready (and rec[0] recorded),
@@ -556,6 +701,7 @@ static int run_factor(rb_tree* t, const z* dk, const std::vector<cudaEvent_t>* r
     }
     if ((rc = timer_end(t))) return rc;
     if (rec) RB_CK(cudaEventRecord((*rec)[L], s));
+    if (factor_pipelined(t)) return run_merges_pipelined(t, rec, before_root_tail);
     static const char* lvl_names[] = {"merge_l0", "merge_l1", "merge_l2", "merge_l3", "merge_l4", "merge_l5",
                                       "merge_l6", "merge_l7", "merge_l8", "merge_l9", "merge_l10", "merge_l11",
                                       "merge_l12", "merge_l13", "merge_l14", "merge_l15", "merge_l16"};
@@ -1144,12 +1290,16 @@ int rb_tree_destroy(rb_tree* t) {
     for (auto& e : t->ev_fork) if (e) cudaEventDestroy(e);
     for (auto& e : t->ev_join) if (e) cudaEventDestroy(e);
     for (auto& e : t->ev_lvl) if (e) cudaEventDestroy(e);
+    for (auto* v : {&t->ev_face, &t->ev_rest, &t->ev_d, &t->ev_m1, &t->ev_m3})
+        for (auto& e : *v) if (e) cudaEventDestroy(e);
+    if (t->ev_root_gj) cudaEventDestroy(t->ev_root_gj);
     if (t->ev_root_forms) cudaEventDestroy(t->ev_root_forms);
     if (t->stream3) cudaStreamSynchronize(t->stream3);
     if (t->ev_copy) cudaEventDestroy(t->ev_copy);
     if (t->h_status) cudaFreeHost(t->h_status);
     if (t->stream3) cudaStreamDestroy(t->stream3);
     if (t->stream2) cudaStreamDestroy(t->stream2);
+    if (t->stream4) cudaStreamDestroy(t->stream4);
     if (t->stream) cudaStreamDestroy(t->stream);
     delete t;
     return RB_OK;

@@ -95,6 +95,13 @@ struct rb_tree {
     // factor launch batches
     std::vector<GJBatch> gj_d, gj_s, gj_k;
     std::vector<GemmBatch> fK, fM1, fM2, fM3, fM4;
+    // Level-pipelined FP64 factor: level l's parent map split by rows into the rows on the face
+    // its parent merges across (fM4F: all the parent's interface solve reads) and the others
+    // (fM4N), so that the parent level's forms, K and inversion run beside fM4N (levels 1..L-1)
+    std::vector<GemmBatch> fM4F, fM4N;
+    cudaStream_t stream4 = nullptr;      // the pipelined factor's B1 product beside the inversion
+    std::vector<cudaEvent_t> ev_face, ev_rest, ev_d, ev_m1, ev_m3;   // per level
+    cudaEvent_t ev_root_gj = nullptr;
     bool factor_ready = false;
 
     // solve storage
