@@ -635,6 +635,7 @@ static int run_merges_pipelined(rb_tree* t, const std::vector<cudaEvent_t>* rec,
     int rc;
     RB_CK(cudaEventRecord(t->ev_face[L], s));            // the leaves' maps, whole
     RB_CK(cudaEventRecord(t->ev_rest[L], s));
+    t->factor_was_pipelined = true;
     for (int l = L - 1; l >= 0; --l) {
         const PlanLevel& p = P.lv[l];
         const ChildStore cs = child_store(t, l);
@@ -649,11 +650,11 @@ static int run_merges_pipelined(rb_tree* t, const std::vector<cudaEvent_t>* rec,
         RB_LAUNCH(merge_form_k(p.nnodes, p.m, t->nu, t->kinv[l], c));
         RB_LAUNCH(launch_gemm_batch(t->fK[l], c));
         RB_LAUNCH(gj_invert_batch(t->gj_k[l].d_desc, p.nnodes, p.m, t->gj_work, t->d_status, c));
-        // from here on the children's maps are needed whole (this level's map; the solve's sweep)
-        RB_CK(cudaStreamWaitEvent(c, t->ev_rest[l + 1], 0));
+        // a solve's sweep at this level also waits for ev_rest[l + 1] (run_solve)
         if (rec) RB_CK(cudaEventRecord((*rec)[l], c));
         RB_CK(cudaStreamWaitEvent(c, t->ev_m1[l], 0));
         if (l == 0) {
+            RB_CK(cudaStreamWaitEvent(c, t->ev_rest[1], 0));
             RB_CK(cudaEventRecord(t->ev_root_gj, c));
             RB_CK(cudaStreamWaitEvent(s, t->ev_root_gj, 0));   // joins both side streams
             if (before_root_tail && (rc = (*before_root_tail)())) return rc;
@@ -661,9 +662,11 @@ static int run_merges_pipelined(rb_tree* t, const std::vector<cudaEvent_t>* rec,
             RB_LAUNCH(launch_gemm_batch(t->fM3[0], s));
             RB_LAUNCH(launch_gemm_batch(t->fM4[0], s));
         } else {
+            // Y1 and Y2 read only the children's face rows; this level's map reads them whole
             RB_LAUNCH(launch_gemm_batch(t->fM2[l], c));
             RB_LAUNCH(launch_gemm_batch(t->fM3[l], c));
             RB_CK(cudaEventRecord(t->ev_m3[l], c));
+            RB_CK(cudaStreamWaitEvent(c, t->ev_rest[l + 1], 0));
             RB_LAUNCH(launch_gemm_batch(t->fM4F[l], c));
             RB_CK(cudaEventRecord(t->ev_face[l], c));
             RB_CK(cudaStreamWaitEvent(s, t->ev_m3[l], 0));
@@ -701,6 +704,7 @@ static int run_factor(rb_tree* t, const z* dk, const std::vector<cudaEvent_t>* r
     }
     if ((rc = timer_end(t))) return rc;
     if (rec) RB_CK(cudaEventRecord((*rec)[L], s));
+    t->factor_was_pipelined = false;
     if (factor_pipelined(t)) return run_merges_pipelined(t, rec, before_root_tail);
     static const char* lvl_names[] = {"merge_l0", "merge_l1", "merge_l2", "merge_l3", "merge_l4", "merge_l5",
                                       "merge_l6", "merge_l7", "merge_l8", "merge_l9", "merge_l10", "merge_l11",
@@ -969,6 +973,9 @@ static int run_solve(rb_tree* t, int k, cudaStream_t s, const std::vector<cudaEv
     RB_GEMM_S(t->sL0, L, s);
     for (int l = L - 1; l >= 1; --l) {
         if (wait) RB_CK(cudaStreamWaitEvent(s, (*wait)[l], 0));
+        // a pipelined factor records level l's event after the inversion, before the children's
+        // maps are whole; the parent h of this level reads their non-interface rows
+        if (wait && t->factor_was_pipelined) RB_CK(cudaStreamWaitEvent(s, t->ev_rest[l + 1], 0));
         if ((rc = inject_level(l))) return rc;
         RB_GEMM_S(t->sF12[l], l, s);
         RB_GEMM_S(t->sF3[l], l, s);

@@ -102,6 +102,7 @@ struct rb_tree {
     cudaStream_t stream4 = nullptr;      // the pipelined factor's B1 product beside the inversion
     std::vector<cudaEvent_t> ev_face, ev_rest, ev_d, ev_m1, ev_m3;   // per level
     cudaEvent_t ev_root_gj = nullptr;
+    bool factor_was_pipelined = false;   // the last factor ran the pipelined schedule
     bool factor_ready = false;
 
     // solve storage
