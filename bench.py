@@ -58,11 +58,13 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "Factor time + solves/s on 1024² 2D Helmholtz, mixed vs FP64 GPU @1e-10; p99 ms"
 
-# DRAM bytes (read + write) per launch of the dominant kernel families in one step of the 1024^2,
-# L=12 workload, from one ncu capture of this script (dram__bytes_read.sum + dram__bytes_write.sum;
-# the profiles/ directory keeps the capture's summary and command).  ncu cannot run inside this
-# script, so the figures are carried here; they are reported for the 1024^2 workload only.
-DRAM_BYTES_PER_LAUNCH = {}
+# DRAM bytes (read + write) per algorithmic flop of the contiguous-k FP64 tensor-core GEMM
+# ("zgemm_tc"), from an ncu capture of dram__bytes_read.sum + dram__bytes_write.sum over two full
+# factors of the 512^2, L=10 workload (--config 2 --single-arm): 0.76 GB for 71.2 GFLOP.  ncu cannot
+# run inside this script, and a capture of that kind on the 1024^2 workload would be too large, so
+# the ratio is carried here and scaled to the timed launches by their flops.  The tile reads each
+# operand panel once per output tile, so its traffic grows with the flops at a fixed tile shape.
+DRAM_BYTES_PER_FLOP = {"zgemm_tc": 0.0107}
 
 
 def parse():
@@ -515,7 +517,10 @@ def roofline_block(arm, torch, dev, steps, zpeak, bf16_peak):
     return {
         "bound": "tensor", "pipe": pipe, "kernel": dname, "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
         "frac": (achieved / peak) if (achieved and peak) else None,
-        "traffic": DRAM_BYTES_PER_LAUNCH.get(dname) if arm.T.nlvls == 12 else None, "launches": dcnt, "ms_total": dms,
+        "traffic": (DRAM_BYTES_PER_FLOP[dname] * dflops / dcnt) if (dname in DRAM_BYTES_PER_FLOP and dcnt) else None,
+        "traffic_note": "bytes per launch: a measured bytes-per-flop ratio of this kernel (512^2 capture) times this "
+                        "run's flops per launch" if dname in DRAM_BYTES_PER_FLOP else None,
+        "launches": dcnt, "ms_total": dms,
         "share_of_step": shares.get(dname), "peak_source": src,
         "flop_count": "algorithmic 8mnk per complex GEMM, 8m^3 per Gauss-Jordan inverse",
         "families": fams, "shares": shares,
