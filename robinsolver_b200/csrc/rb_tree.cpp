@@ -576,23 +576,30 @@ static bool mixed_solve_fp64() {
 // stream beside K and its inverse, the other stages on the main stream.
 static int ensure_mixed_factor_plan(rb_tree* t) {
     if (t->mixed_plan) return RB_OK;
-    long long wmain = 0, wside = 0;
+    // one split-K workspace per stream that runs mixed-level GEMMs: the chain stream (K, Y1, Y2,
+    // the face rows; in the serial schedule also the whole map), B1's stream, and the main stream's
+    // remaining map rows of the pipelined schedule
+    long long wmain = 0, wside = 0, wrest = 0;
     for (int l = 0; l < t->P.L; ++l) {
         if (!mixed_level(t, l)) continue;
-        for (GemmBatch* b : {&t->fK[l], &t->fM2[l], &t->fM3[l], &t->fM4[l]})
+        for (GemmBatch* b : {&t->fK[l], &t->fM2[l], &t->fM3[l], &t->fM4[l], &t->fM4F[l]})
             wmain = std::max(wmain, gemm_plan_split_tc5_factor(*b));
         wside = std::max(wside, gemm_plan_split_tc5_factor(t->fM1[l]));
+        wrest = std::max(wrest, gemm_plan_split_tc5_factor(t->fM4N[l]));
     }
     z* pm = nullptr;
     z* ps = nullptr;
+    z* pr = nullptr;
     int rc;
     if (wmain > 0 && (rc = alloc_n(t, t->mixed_bufs, (size_t)wmain, &pm))) return rc;
     if (wside > 0 && (rc = alloc_n(t, t->mixed_bufs, (size_t)wside, &ps))) return rc;
+    if (wrest > 0 && (rc = alloc_n(t, t->mixed_bufs, (size_t)wrest, &pr))) return rc;
     for (int l = 0; l < t->P.L; ++l) {
         if (!mixed_level(t, l)) continue;
-        for (GemmBatch* b : {&t->fK[l], &t->fM2[l], &t->fM3[l], &t->fM4[l]})
+        for (GemmBatch* b : {&t->fK[l], &t->fM2[l], &t->fM3[l], &t->fM4[l], &t->fM4F[l]})
             if (b->t5_ksplit > 1) b->work = pm;
         if (t->fM1[l].t5_ksplit > 1) t->fM1[l].work = ps;
+        if (t->fM4N[l].t5_ksplit > 1) t->fM4N[l].work = pr;
     }
     t->mixed_plan = true;
     return RB_OK;
@@ -609,7 +616,7 @@ static double leaf_flops(const LeafGeom& g) {
     return 8.0 * g.a * g.a * g.a * g.b + 16.0 * g.a * g.a * (double)g.nb * g.b;
 }
 
-// The FP64 K-form merges, pipelined across levels (all but the timed and mixed-precision runs).
+// The K-form merges, pipelined across levels (every untimed run; FP64 and mixed precision).
 // Level l's parent map is formed in two row sets: the rows on the face its parent merges across
 // (fM4F), which are all the parent's interface system reads (A1, A2 and K from the ii blocks, B1
 // and Y1 from the iN blocks), and the other rows (fM4N).  The parent level's chain -- forms, K,
@@ -624,7 +631,7 @@ static bool factor_pipelined(const rb_tree* t) {
         const char* v = std::getenv("RB_FACTOR_PIPELINE");
         return v && v[0] == '0';
     }();
-    return !off && t->timing == 0 && t->kform && t->prec == RB_PREC_FP64 && t->P.L >= 2;
+    return !off && t->timing == 0 && t->kform && t->P.L >= 2;
 }
 
 static int run_merges_pipelined(rb_tree* t, const std::vector<cudaEvent_t>* rec,
@@ -644,11 +651,11 @@ static int run_merges_pipelined(rb_tree* t, const std::vector<cudaEvent_t>* rec,
         if (rec && l == 0) RB_CK(cudaEventRecord(t->ev_root_forms, c));
         RB_CK(cudaEventRecord(t->ev_d[l], c));
         RB_CK(cudaStreamWaitEvent(s4, t->ev_d[l], 0));
-        RB_LAUNCH(launch_gemm_batch(t->fM1[l], s4));          // B1 = -A2 T1_iN
+        RB_LAUNCH(launch_gemm_level(t, t->fM1[l], l, s4));          // B1 = -A2 T1_iN
         RB_CK(cudaEventRecord(t->ev_m1[l], s4));
         RB_LAUNCH(merge_form_s(cs, p.nnodes, p.m, p.o1, t->zeta, zmk(0.0, 0.0), t->dinv[l], t->sinv[l], c));
         RB_LAUNCH(merge_form_k(p.nnodes, p.m, t->nu, t->kinv[l], c));
-        RB_LAUNCH(launch_gemm_batch(t->fK[l], c));
+        RB_LAUNCH(launch_gemm_level(t, t->fK[l], l, c));
         RB_LAUNCH(gj_invert_batch(t->gj_k[l].d_desc, p.nnodes, p.m, t->gj_work, t->d_status, c));
         // a solve's sweep at this level also waits for ev_rest[l + 1] (run_solve)
         if (rec) RB_CK(cudaEventRecord((*rec)[l], c));
@@ -658,19 +665,19 @@ static int run_merges_pipelined(rb_tree* t, const std::vector<cudaEvent_t>* rec,
             RB_CK(cudaEventRecord(t->ev_root_gj, c));
             RB_CK(cudaStreamWaitEvent(s, t->ev_root_gj, 0));   // joins both side streams
             if (before_root_tail && (rc = (*before_root_tail)())) return rc;
-            RB_LAUNCH(launch_gemm_batch(t->fM2[0], s));
-            RB_LAUNCH(launch_gemm_batch(t->fM3[0], s));
-            RB_LAUNCH(launch_gemm_batch(t->fM4[0], s));
+            RB_LAUNCH(launch_gemm_level(t, t->fM2[0], 0, s));
+            RB_LAUNCH(launch_gemm_level(t, t->fM3[0], 0, s));
+            RB_LAUNCH(launch_gemm_level(t, t->fM4[0], 0, s));
         } else {
             // Y1 and Y2 read only the children's face rows; this level's map reads them whole
-            RB_LAUNCH(launch_gemm_batch(t->fM2[l], c));
-            RB_LAUNCH(launch_gemm_batch(t->fM3[l], c));
+            RB_LAUNCH(launch_gemm_level(t, t->fM2[l], l, c));
+            RB_LAUNCH(launch_gemm_level(t, t->fM3[l], l, c));
             RB_CK(cudaEventRecord(t->ev_m3[l], c));
             RB_CK(cudaStreamWaitEvent(c, t->ev_rest[l + 1], 0));
-            RB_LAUNCH(launch_gemm_batch(t->fM4F[l], c));
+            RB_LAUNCH(launch_gemm_level(t, t->fM4F[l], l, c));
             RB_CK(cudaEventRecord(t->ev_face[l], c));
             RB_CK(cudaStreamWaitEvent(s, t->ev_m3[l], 0));
-            RB_LAUNCH(launch_gemm_batch(t->fM4N[l], s));
+            RB_LAUNCH(launch_gemm_level(t, t->fM4N[l], l, s));
             RB_CK(cudaEventRecord(t->ev_rest[l], s));
         }
     }
