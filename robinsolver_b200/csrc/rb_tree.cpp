@@ -566,11 +566,14 @@ static bool mixed_level(const rb_tree* t, int l) {
 static cudaError_t launch_gemm_level(rb_tree* t, const GemmBatch& b, int l, cudaStream_t s) {
     return mixed_level(t, l) ? launch_gemm_tc5(b, t->d_status, s) : launch_gemm_batch(b, s);
 }
-// RB_MIXED_SOLVE_ENGINE=fp64 (read at every solve): the mixed solve applies its factor with the
-// FP64 GEMMs; a comparison knob that separates the factor's rounding from the sweeps' own
+// The mixed solve applies its factor with the FP64 GEMMs: the sweeps' products are narrow (n =
+// the right-hand sides), where the tcgen05 tile is slower than the FP64 one (1024^2, L=12, 32
+// RHS: 21.4 against 26.2 ms for the refined solve), and the refinement's contraction is set by
+// the factor's rounding, not the sweeps'.  RB_MIXED_SOLVE_ENGINE=tc5 (read at every solve) runs
+// the sweeps' mixed levels on the tcgen05 kernel instead.
 static bool mixed_solve_fp64() {
     const char* v = std::getenv("RB_MIXED_SOLVE_ENGINE");
-    return v && std::strcmp(v, "fp64") == 0;
+    return !(v && std::strcmp(v, "tc5") == 0);
 }
 // Split-K plans of the mixed levels' factor stages, with two workspaces: B1 runs on the second
 // stream beside K and its inverse, the other stages on the main stream.

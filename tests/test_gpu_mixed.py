@@ -1,6 +1,6 @@
-"""Mixed precision (RB_PREC_MIXED): split-TF32 tcgen05 GEMMs on the merge levels l >= 2 whose
-interface has at least 128 points and on the solve's leaf GEMM, FP64 elsewhere, and solves refined
-against the FP64 residual of the global FD system (run on a GPU).
+"""Mixed precision (RB_PREC_MIXED): split-TF32 tcgen05 GEMMs on the factor's merge levels l >= 2
+whose interface has at least 128 points, FP64 elsewhere, and solves that apply that factor (with
+FP64 GEMMs) refined against the FP64 residual of the global FD system (run on a GPU).
 
 Bars: every refined solution within 1e-10 relative (max norm) of the FP64 GPU solution of the
 same problem, as BASELINE's precision configuration asks; the merged maps of a tensor-core level
@@ -69,8 +69,8 @@ def test_mixed_tolerance_and_repeat_solves():
 
 
 def test_mixed_small_tree():
-    """A tree without 128-point interfaces below level 1 (64^2, L=4): every merge is FP64 and only
-    the solve's leaf GEMM runs on the tensor cores; refinement recovers the FP64 solution."""
+    """A tree without 128-point interfaces below level 1 (64^2, L=4): every merge is FP64, so the
+    refined solve recovers the FP64 solution at once."""
     wl = W.make_workload(1)
     Tf, Tm = _pair(wl)
     Uf = _solve(Tf, wl.rhs)
