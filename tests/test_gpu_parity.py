@@ -136,6 +136,30 @@ def test_skip_root_rtr_gives_the_same_solution():
     Ts.close()
 
 
+@pytest.mark.parametrize("wlkw,precision", [(dict(N=128, L=6, nrhs=3), "fp64"), (dict(nrhs=2), "fp64"),
+                                            (dict(nrhs=2), "mixed")])
+def test_pipelined_factor_equals_serial_bitwise(wlkw, precision):
+    """The pipelined factor (parent maps split into face rows and the rest, level chains on side
+    streams) computes every element with the same kernels and operands in the same order as the
+    serial schedule that timing mode 1 runs: every level's map and the solutions agree bit for
+    bit, in FP64 and in mixed precision (512^2, L=10 has tensor-core levels 2-4)."""
+    wl = W.make_workload(2, **wlkw)
+    out = {}
+    from robinsolver_b200 import _lib
+    for timing in (0, 1):
+        T, op, opts = gpu_tree(wl)
+        T.plan(wl.L, op, opts)
+        T.set_timing(timing)
+        T.factor_samples(op.k(T.sample_points(_lib.RB_POINTS_POTENTIAL)), precision)
+        T.set_timing(0)
+        maps = [T.get_rtr(l, i) for l in range(1, wl.L + 1) for i in (0, 2 ** l - 1)]
+        out[timing] = (maps, _solve(T, wl.rhs))
+        T.close()
+    for a, b in zip(out[0][0], out[1][0]):
+        assert np.array_equal(a, b)
+    assert np.array_equal(out[0][1], out[1][1])
+
+
 @pytest.mark.parametrize("cfg", [2, pytest.param(4, marks=pytest.mark.slow)])
 def test_resident_gauss_jordan_equals_blocked_bitwise(cfg, monkeypatch):
     """The one-launch resident inversion performs the blocked path's arithmetic in the same order:
