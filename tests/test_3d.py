@@ -216,3 +216,56 @@ def test_gpu3d_refuses_mixed_precision():
         T.factor(3, rb.elliptic_operator(d=3, domain=np.array([[0.0, 0.0, 0.0], [1.0, 1.0, 1.0]]),
                                          k=bump_potential), rb.solve_opts(h_tgt=1.0 / 8, kb=1.0), precision="mixed")
     assert ei.value.code == _lib.RB_ERR_UNSUPPORTED
+
+
+@pytest.mark.gpu
+def test_gpu3d_reference_merge_form_matches_oracle():
+    """The reference's interface solve (inv(D), inv(S), RB_FLAG_MERGE_DS) in 3D: maps and a solve
+    within 1e-11 of the oracle at 16^3, L=5."""
+    import robinsolver_b200 as rb
+    L, N = 5, 16
+    T = rb.robin_tree(merge_ds=True)
+    T.bndry_params = BP_GEN
+    T.factor(L, rb.elliptic_operator(d=3, domain=np.array([[0.0, 0.0, 0.0], [1.0, 1.0, 1.0]]), k=bump_potential),
+             rb.solve_opts(h_tgt=1.0 / N, kb=1.0))
+    O = oracle_tree(L, N, bump_potential, bp=BP_GEN)
+    for l in (1, 3, L):
+        assert rel_err(T.get_rtr(l, 0), O.levels[l][0].rtr) < 1e-11, l
+    T.solve(rb.elliptic_rhs(d=3, f=source, g=plane_faces()))
+    O.solve([H.EllipticRHS(3, source, plane_faces())])
+    ref = np.stack([u[:, 0] for _, u in O.get_solution()])
+    assert rel_err(T.solution_array(0), ref) < 1e-11
+    T.close()
+
+
+@pytest.mark.gpu
+def test_gpu3d_save_load_solves_identically(tmp_path):
+    import robinsolver_b200 as rb
+    T = _gpu_tree(4, 16, bump_potential)
+    rhs = rb.elliptic_rhs(d=3, f=source, g=plane_faces())
+    T.solve(rhs)
+    U = T.solution_array(0)
+    T.save(str(tmp_path / "tree3d.bin"))
+    T2 = rb.robin_tree.load(str(tmp_path / "tree3d.bin"))
+    F, G = T.sample_rhs([rhs])
+    T2.solve_samples(F, G)
+    assert np.array_equal(T2.solution_array(0), U)
+    T.close()
+    T2.close()
+
+
+@pytest.mark.gpu
+def test_gpu3d_refuses_2d_only_features():
+    """Forests and device-side sampling are 2D only: RB_ERR_UNSUPPORTED, no device fault."""
+    import robinsolver_b200 as rb
+    from robinsolver_b200 import _lib
+    T = _planned3d(3, 8)
+    with pytest.raises(rb.RobinSolverError) as ei:
+        rb.robin_forest([T])
+    assert ei.value.code == _lib.RB_ERR_UNSUPPORTED
+    T.close()
+    T = _gpu_tree(3, 8, bump_potential)
+    with pytest.raises(rb.RobinSolverError) as ei:
+        T.sample_device(_lib.RB_FIELD_PLANE_WAVE, 1, [[1.0, 1.0, 0.0]])
+    assert ei.value.code == _lib.RB_ERR_UNSUPPORTED
+    T.close()
