@@ -169,6 +169,9 @@ def _load():
         "rb_test_zgemm": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_longlong, C.c_longlong, P,
                                     C.c_longlong, C.c_longlong, P, C.c_longlong, C.c_longlong, C.c_double,
                                     C.c_double, C.c_double, C.c_double, C.c_int]),
+        "rb_test_zgemm_timed": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P, C.c_longlong, C.c_longlong, P,
+                                          C.c_longlong, C.c_longlong, P, C.c_longlong, C.c_longlong, C.c_double,
+                                          C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, D]),
         # test hook of the batched Gauss-Jordan inversion (rb_testing.cpp)
         "rb_test_zinvert": (C.c_int, [C.c_int, C.c_int, P, C.c_longlong, C.c_longlong, C.c_int, D]),
     }

@@ -117,6 +117,11 @@ struct GemmBatch {
     int t5_ksplit = 1;
     int t5_kchunk = 0;
     long long t5_pstride = 0;
+    // the tcgen05 kernel's operand planes (tc5_plane_bytes(batch) bytes, 256-byte aligned): every
+    // operand element split once into four TF32 parts and laid out block by block as the kernel's
+    // shared-memory stages hold them
+    void* t5_planes = nullptr;
+    size_t t5_plane_cap = 0;      // bytes at t5_planes; a launch that needs more is refused
     // FP64 engine (tile shape) chosen by an autotuner; -1: the launcher's own rule
     int engine = -1;
 };

@@ -11,22 +11,31 @@
 // columns each).  The result carries ~1e-6 relative error: the solve recovers FP64 accuracy by
 // iterative refinement against the FP64 residual (rb_refine.cu).
 //
-// CTA = one 128 x BN output tile of one problem (blockIdx.y), 9 warps:
-//   warps 0-7  producers: cp.async (16 bytes, zero-filled outside the problem) of the FP64 operands
-//              through the problem's ZViews (face gathers, row maps, skipped bands, exactly as the
-//              FP64 kernels) into a ring of STAGES shared-memory stages, STAGES - 1 k-blocks ahead of
-//              the one being converted.  A landed stage is split to TF32 hi/lo IN PLACE (the four
-//              TF32 parts of an element take the 16 bytes of its FP64 pair) into the UMMA K-major
-//              no-swizzle layout, then handed to the MMA warp.  Then the epilogue: tcgen05.ld of
-//              the accumulators (warp w reads lanes 32 (w % 4) .. +31, half w / 4 of the columns),
-//              alpha/beta, scatter through the output maps.
-//   warp 8     allocates 2*BN tensor-memory columns; one lane issues the MMAs of each stage once
-//              its producers have arrived, and releases the stage with tcgen05.commit.
+// Two kernels per batch:
+//  1. tc5_split_kernel converts every operand element ONCE: it reads the FP64 operands through
+//     the problems' ZViews (face gathers, row maps, skipped bands, exactly as the FP64 kernels
+//     read them), splits each value into TF32 hi/lo with integer operations on the FP64 bit
+//     pattern (the FP64 -> FP32 conversion instructions run on the narrow XU pipe, which bounded
+//     a kernel that converted inside the GEMM once per output tile), and writes "planes": per
+//     problem, per 128-row (A) or BN-column (B) tile and per 16-deep k-block one contiguous block
+//     laid out exactly as the GEMM's shared-memory stage holds it (the UMMA K-major no-swizzle
+//     layout: 16-byte rows of four K values, 128-byte core matrices of 8 rows), zero outside the
+//     problem.
+//  2. zgemm_tc5_kernel, one CTA per 128 x BN output tile, 8 warps:
+//       warp 0   one lane streams the k-blocks of A and B into a ring of shared-memory stages with
+//                two 1-D bulk copies each (cp.async.bulk, completion counted in bytes on the
+//                stage's mbarrier; no multicast);
+//       warp 1   allocates 2*BN tensor-memory columns; one lane issues the stage's MMAs once its
+//                bytes have landed and releases the stage with tcgen05.commit;
+//       all 8   the epilogue: tcgen05.ld of the accumulators (warp w reads lanes 32 (w % 4) ..
+//                +31, half w / 4 of the columns), alpha/beta, scatter through the output maps.
 // Every mbarrier wait is bounded (RB_TC5_WAIT_NS on the global timer).  A wait that runs out sets
-// RB_TC5_TIMEOUT in the status word, the CTA stops issuing work, waits (bounded) for the MMAs it
-// issued, frees its tensor memory and returns.
+// RB_TC5_TIMEOUT in the status word, the CTA stops issuing work, waits (bounded) for the copies
+// and MMAs it issued, frees its tensor memory and returns.
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
+#include <cstring>
 
 #include "rb_kernels.h"
 
@@ -35,24 +44,19 @@ namespace rb {
 namespace {
 
 constexpr int TC5_BM = 128;          // output rows per tile = UMMA M (one lane per row)
-constexpr int TC5_KB = 16;           // complex k per stage: 4 chunks of 4 TF32 = two UMMA k-steps
-constexpr int TC5_PRODUCERS = 256;   // warps 0-7
-constexpr int TC5_THREADS = TC5_PRODUCERS + 32;
+constexpr int TC5_KB = 16;           // complex k per block / stage: 4 chunks of 4 TF32 = two UMMA k-steps
+constexpr int TC5_THREADS = 256;     // 8 warps
+constexpr int TC5_A_BLOCK = TC5_BM * TC5_KB * 16;          // bytes of one A plane block (32 KB)
 constexpr unsigned long long RB_TC5_WAIT_NS = 1000000000ull;   // 1 s per wait
 
 template <int BN>
 struct Tc5Cfg {
-    // one stage: A (128 rows x KB complex) then B (BN columns x KB complex), 16 bytes per element;
-    // raw FP64 pairs first, the four TF32 parts (re/im x hi/lo) in the same bytes after the split
-    static constexpr int A_BYTES = TC5_BM * TC5_KB * 16;
-    static constexpr int B_BYTES = BN * TC5_KB * 16;
-    static constexpr int A_PART = TC5_BM * TC5_KB * 4;     // one TF32 part of A
+    static constexpr int A_PART = TC5_BM * TC5_KB * 4;     // one TF32 part of an A block
+    static constexpr int B_BLOCK = BN * TC5_KB * 16;       // bytes of one B plane block
     static constexpr int B_PART = BN * TC5_KB * 4;
-    static constexpr int STAGE = A_BYTES + B_BYTES;
-    static constexpr int STAGES = (196608 / STAGE) < 4 ? (196608 / STAGE) : 4;   // 3 (BN 128) or 4
-    static constexpr int AHEAD = STAGES - 1;               // k-blocks in flight beyond the converted one
-    // + 1024 for the alignment of the stages
-    static constexpr int SMEM = STAGES * STAGE + 1024;
+    static constexpr int STAGE = TC5_A_BLOCK + B_BLOCK;
+    static constexpr int STAGES = (204800 / STAGE) < 4 ? (204800 / STAGE) : 4;   // 4, 4, 3, 2 for BN 32..256
+    static constexpr int SMEM = STAGES * STAGE + 1024;     // + 1024 for the alignment of the stages
     static constexpr int TMEM_COLS = 2 * BN;               // Cr, Ci
 };
 
@@ -70,11 +74,9 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
 }
 
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-    asm volatile(
-        "{\n\t.reg .b64 st;\n\t"
-        "mbarrier.arrive.release.cta.shared::cta.b64 st, [%0];\n\t}" ::"r"(bar)
-        : "memory");
+// one arrival that also announces `bytes` of bulk-copy data the phase must wait for
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
 
 __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
@@ -90,29 +92,24 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
 }
 
 // waits for the phase with the given parity to complete; false after RB_TC5_WAIT_NS or when
-// another warp has already given up (*abort)
+// another warp has already given up (*abort, if given)
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort) {
     if (mbar_try(bar, parity)) return true;
     const unsigned long long t0 = global_ns();
     for (unsigned it = 0;; ++it) {
         if (mbar_try(bar, parity)) return true;
         if ((it & 63) == 63) {
-            if (*abort) return false;
+            if (abort && *abort) return false;
             if (global_ns() - t0 > RB_TC5_WAIT_NS) return false;
         }
     }
 }
 
-__device__ __forceinline__ uint32_t tf32_rna(float x) {
-    uint32_t r;
-    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
-    return r;
-}
-
-// x -> (hi, lo): hi = tf32(x), lo = tf32(x - hi) with the difference taken in FP64
-__device__ __forceinline__ void split_tf32(double x, uint32_t& hi, uint32_t& lo) {
-    hi = tf32_rna(static_cast<float>(x));
-    lo = tf32_rna(static_cast<float>(x - static_cast<double>(__uint_as_float(hi))));
+// 1-D bulk copy global -> this CTA's shared memory, completion counted on an mbarrier
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
 }
 
 // UMMA shared-memory descriptor, K-major, no swizzle: core matrices of 8 rows x 16 bytes, rows
@@ -157,52 +154,133 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-__device__ __forceinline__ void cp_async16(uint32_t dst, const void* src, bool valid) {
-    // src-size 0 fills the 16 bytes with zeros (a row, column or k outside the problem)
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(valid ? 16 : 0)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
-// the 256 producer threads only (the MMA warp runs its own loop)
-__device__ __forceinline__ void producers_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
-// a producer barrier that also ORs a flag over the 256 producers: every one gets the same answer,
-// so they all leave the loop at the same iteration
-__device__ __forceinline__ bool producers_any(bool v) {
-    uint32_t r;
-    asm volatile(
-        "{\n\t.reg .pred p, q;\n\t"
-        "setp.ne.u32 p, %1, 0;\n\t"
-        "bar.red.or.pred q, 1, 256, p;\n\t"
-        "selp.u32 %0, 1, 0, q;\n\t}"
-        : "=r"(r)
-        : "r"((uint32_t)v)
-        : "memory");
-    return r != 0;
+// TF32 bit pattern (an FP32 pattern whose low 13 mantissa bits are zero) of a double given by
+// its high word, rounded already to 10 mantissa bits (the low 10 bits of hw and the low word
+// are zero).  Below the FP32 normal range: signed zero; above it (and inf/NaN): signed infinity.
+__device__ __forceinline__ uint32_t tf32_of_rounded_hiword(uint32_t hw) {
+    const uint32_t e = (hw >> 20) & 0x7FFu;
+    const uint32_t sign = hw & 0x80000000u;
+    if (e <= 896u) return sign;
+    if (e >= 1151u) return sign | 0x7F800000u;
+    // ((e - 896) << 23) | (top 10 mantissa bits << 13): the exponent rebiased from 1023 to 127
+    return sign | (((hw & 0x7FFFFFFFu) - (896u << 20)) << 3);
 }
 
-__device__ __forceinline__ void split4(const z (&v)[4], uint4& rh, uint4& rl, uint4& ih, uint4& il) {
-    split_tf32(v[0].x, rh.x, rl.x); split_tf32(v[0].y, ih.x, il.x);
-    split_tf32(v[1].x, rh.y, rl.y); split_tf32(v[1].y, ih.y, il.y);
-    split_tf32(v[2].x, rh.z, rl.z); split_tf32(v[2].y, ih.z, il.z);
-    split_tf32(v[3].x, rh.w, rl.w); split_tf32(v[3].y, ih.w, il.w);
+// x -> (hi, lo) TF32 patterns: hi = x rounded to 11 significant bits (to nearest, ties away
+// from zero), lo = (x - hi) rounded the same way; x - hi is exact in FP64.  Integer operations
+// and one FP64 subtraction only.
+__device__ __forceinline__ void split_tf32(double x, uint32_t& hi, uint32_t& lo) {
+    const uint32_t hr = ((uint32_t)__double2hiint(x) + 0x200u) & 0xFFFFFC00u;
+    hi = tf32_of_rounded_hiword(hr);
+    const double r = x - __hiloint2double((int)hr, 0);
+    lo = tf32_of_rounded_hiword(((uint32_t)__double2hiint(r) + 0x200u) & 0xFFFFFC00u);
+}
+
+// Operand plane geometry of a batch: MT 128-row tiles of A, NT BN-column tiles of B, KBN
+// 16-deep k-blocks; A blocks first ([problem][mt][kb]), then B blocks ([problem][nt][kb]).
+struct PlaneGeom {
+    int MT, NT, KBN;
+    long long a_bytes;     // all A blocks
+};
+PlaneGeom plane_geom(const GemmBatch& b, int bn) {
+    PlaneGeom g;
+    g.MT = (b.max_m + TC5_BM - 1) / TC5_BM;
+    g.NT = (b.max_n + bn - 1) / bn;
+    g.KBN = (b.max_k + TC5_KB - 1) / TC5_KB;
+    g.a_bytes = (long long)b.count * g.MT * g.KBN * TC5_A_BLOCK;
+    return g;
 }
 
 }  // namespace
 
-// Split-K (part != nullptr): blockIdx.z takes k in [z * kchunk, (z + 1) * kchunk) and writes its raw
-// sums to part + (problem * ksplit + z) * pstride + i + j * ldp; the reduction kernel finishes.
+// One CTA converts one slab: 128 rows of an A block (row i of A = output row), or up to 128
+// columns of a B block (column j of B = output column), 16 k deep.  Slab s < nA: A slab
+// (problem, mt, kb); else B slab (problem, nt, kb, half) with BN / min(BN, 128) slabs per block.
 template <int BN>
-__global__ void __launch_bounds__(TC5_THREADS, 1) zgemm_tc5_kernel(const GemmDesc* __restrict__ descs, int* status,
+__global__ void __launch_bounds__(256) tc5_split_kernel(const GemmDesc* __restrict__ descs, int MT, int NT, int KBN,
+                                                        long long nA, unsigned char* __restrict__ planes,
+                                                        long long a_bytes) {
+    constexpr int BR = BN < 128 ? BN : 128;           // rows of a B slab
+    constexpr int BSLABS = BN / BR;                   // slabs per B block
+    __shared__ z S[128][TC5_KB + 1];                  // [row][k], padded against bank conflicts
+    const int tid = threadIdx.x;
+    long long s = blockIdx.x;
+    const bool isA = s < nA;
+    int prob, tile, kb, half = 0;
+    if (isA) {
+        kb = (int)(s % KBN);
+        s /= KBN;
+        tile = (int)(s % MT);
+        prob = (int)(s / MT);
+    } else {
+        s -= nA;
+        half = (int)(s % BSLABS);
+        s /= BSLABS;
+        kb = (int)(s % KBN);
+        s /= KBN;
+        tile = (int)(s % NT);
+        prob = (int)(s / NT);
+    }
+    const GemmDesc& g = descs[prob];
+    const int k0 = kb * TC5_KB;
+    const int R = isA ? 128 : BR;
+    const int r0 = isA ? tile * TC5_BM : tile * BN + half * BR;     // first row (A) / column (B)
+    if (isA) {
+        // consecutive threads take consecutive rows of one column of A (column-major)
+        const ZView v = g.A;
+        for (int e = tid; e < 128 * TC5_KB; e += 256) {
+            const int r = e % 128, kk = e / 128, i = r0 + r, k = k0 + kk;
+            z val = zmk(0.0, 0.0);
+            if (i < g.m && k < g.k) val = v.p[vrow(v, i) + (long long)vcol(v, k) * v.ld];
+            S[r][kk] = val;
+        }
+    } else {
+        // consecutive threads take consecutive k of one column of B
+        const ZView v = g.B;
+        for (int e = tid; e < BR * TC5_KB; e += 256) {
+            const int kk = e % TC5_KB, r = e / TC5_KB, j = r0 + r, k = k0 + kk;
+            z val = zmk(0.0, 0.0);
+            if (j < g.n && k < g.k) val = v.p[vrow(v, k) + (long long)vcol(v, j) * v.ld];
+            S[r][kk] = val;
+        }
+    }
+    __syncthreads();
+    // unit (row r, K chunk c): four k values -> four 16-byte TF32 parts at
+    // block + ((part * 4 + c) * ROWS + row) * 16
+    const int ROWS = isA ? TC5_BM : BN;
+    unsigned char* blk = isA ? planes + (((long long)prob * MT + tile) * KBN + kb) * TC5_A_BLOCK
+                             : planes + a_bytes + (((long long)prob * NT + tile) * KBN + kb) * (long long)(BN * TC5_KB * 16);
+    const int rofs = isA ? 0 : half * BR;
+    for (int u = tid; u < R * 4; u += 256) {
+        const int r = u % R, c = u / R;
+        uint4 rh, rl, ih, il;
+        split_tf32(S[r][4 * c + 0].x, rh.x, rl.x); split_tf32(S[r][4 * c + 0].y, ih.x, il.x);
+        split_tf32(S[r][4 * c + 1].x, rh.y, rl.y); split_tf32(S[r][4 * c + 1].y, ih.y, il.y);
+        split_tf32(S[r][4 * c + 2].x, rh.z, rl.z); split_tf32(S[r][4 * c + 2].y, ih.z, il.z);
+        split_tf32(S[r][4 * c + 3].x, rh.w, rl.w); split_tf32(S[r][4 * c + 3].y, ih.w, il.w);
+        const long long row = rofs + r;
+        uint4* o = reinterpret_cast<uint4*>(blk);
+        o[(0 * 4 + c) * (long long)ROWS + row] = rh;
+        o[(1 * 4 + c) * (long long)ROWS + row] = rl;
+        o[(2 * 4 + c) * (long long)ROWS + row] = ih;
+        o[(3 * 4 + c) * (long long)ROWS + row] = il;
+    }
+}
+
+// Split-K (part != nullptr): blockIdx.z takes k in [z * kchunk, (z + 1) * kchunk) (kchunk a
+// multiple of 16) and writes its raw sums to part + (problem * ksplit + z) * pstride + i + j * ldp;
+// the reduction kernel finishes.  prob0: index of descs[0] in the batch (the planes are indexed
+// by the batch's problem index).
+template <int BN>
+__global__ void __launch_bounds__(TC5_THREADS, 1) zgemm_tc5_kernel(const GemmDesc* __restrict__ descs, int prob0,
+                                                                  int* status, const unsigned char* __restrict__ planes,
+                                                                  int MT, int NT, int KBN, long long a_bytes,
                                                                   int kchunk, z* part, long long pstride, int ldp,
                                                                   int ksplit) {
     using Cfg = Tc5Cfg<BN>;
     constexpr int STAGES = Cfg::STAGES;
     extern __shared__ __align__(1024) unsigned char tc5_smem[];
     __shared__ GemmDesc sd;
-    __shared__ int a_rows[TC5_BM];          // row offsets of the tile's rows in A (-1: outside m)
-    __shared__ long long b_cols[BN];        // column offsets of the tile's columns in B (-1: outside n)
     __shared__ __align__(8) unsigned long long bars[2 * STAGES + 1];
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int abort_flag;
@@ -231,8 +309,14 @@ __global__ void __launch_bounds__(TC5_THREADS, 1) zgemm_tc5_kernel(const GemmDes
         }
         return;      // uniform over the CTA
     }
-    const int m0 = (blockIdx.x % tiles_m) * TC5_BM;
-    const int n0 = (blockIdx.x / tiles_m) * BN;
+    const int tm = blockIdx.x % tiles_m, tn = blockIdx.x / tiles_m;
+    const int m0 = tm * TC5_BM;
+    const int n0 = tn * BN;
+    const int kb0 = kbeg / TC5_KB;
+    const int nkb = (K - kbeg + TC5_KB - 1) / TC5_KB;
+    const long long prob = prob0 + (long long)blockIdx.y;
+    const unsigned char* gA = planes + ((prob * MT + tm) * KBN + kb0) * (long long)TC5_A_BLOCK;
+    const unsigned char* gB = planes + a_bytes + ((prob * NT + tn) * KBN + kb0) * (long long)Cfg::B_BLOCK;
 
     unsigned char* stage_base = reinterpret_cast<unsigned char*>(
         (reinterpret_cast<uintptr_t>(tc5_smem) + 1023) & ~uintptr_t(1023));
@@ -240,24 +324,16 @@ __global__ void __launch_bounds__(TC5_THREADS, 1) zgemm_tc5_kernel(const GemmDes
     const uint32_t empty0 = smem_u32(&bars[STAGES]);
     const uint32_t done_bar = smem_u32(&bars[2 * STAGES]);
 
-    for (int i = tid; i < TC5_BM; i += TC5_THREADS) {
-        const int gi = m0 + i;
-        a_rows[i] = gi < m ? vrow(sd.A, gi) : -1;
-    }
-    for (int j = tid; j < BN; j += TC5_THREADS) {
-        const int gj = n0 + j;
-        b_cols[j] = gj < n ? (long long)vcol(sd.B, gj) * sd.B.ld : -1;
-    }
     if (tid == 0) {
         abort_flag = 0;
         for (int s = 0; s < STAGES; ++s) {
-            mbar_init(full0 + 8 * s, TC5_PRODUCERS);
+            mbar_init(full0 + 8 * s, 1);
             mbar_init(empty0 + 8 * s, 1);
         }
         mbar_init(done_bar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (warp == 8) {
+    if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_slot)),
                      "r"((uint32_t)Cfg::TMEM_COLS));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
@@ -266,10 +342,38 @@ __global__ void __launch_bounds__(TC5_THREADS, 1) zgemm_tc5_kernel(const GemmDes
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_slot;
-    const int nkb = (K - kbeg + TC5_KB - 1) / TC5_KB;
 
-    if (warp == 8) {
-        // ---------------- MMA issuer: one lane, the warp kept converged ----------------------
+    if (warp == 0) {
+        // ---------------- producer: one lane, the warp kept converged --------------------------------
+        bool ok = true;
+        int issued = 0;
+        for (int kb = 0; kb < nkb; ++kb) {
+            const int s = kb % STAGES;
+            if (kb >= STAGES) {
+                // the MMAs of k-block kb - STAGES read stage s
+                ok = __all_sync(0xffffffffu, mbar_wait(empty0 + 8 * s, (uint32_t)(((kb / STAGES) - 1) & 1), &abort_flag));
+                if (!ok) break;
+            }
+            if (lane == 0) {
+                const uint32_t st = smem_u32(stage_base + (size_t)s * Cfg::STAGE);
+                mbar_arrive_expect_tx(full0 + 8 * s, (uint32_t)Cfg::STAGE);
+                bulk_g2s(st, gA + (long long)kb * TC5_A_BLOCK, (uint32_t)TC5_A_BLOCK, full0 + 8 * s);
+                bulk_g2s(st + TC5_A_BLOCK, gB + (long long)kb * Cfg::B_BLOCK, (uint32_t)Cfg::B_BLOCK, full0 + 8 * s);
+            }
+            __syncwarp();
+            issued = kb + 1;
+        }
+        if (!ok) {
+            abort_flag = 1;
+            if (lane == 0) atomicOr(status, RB_TC5_TIMEOUT);
+            // no copy may still target this CTA's memory when it exits: wait (bounded) for the
+            // stages filled last, whatever the MMA warp did with them
+            for (int kb = max(0, issued - STAGES); kb < issued; ++kb)
+                mbar_wait(full0 + 8 * (kb % STAGES), (uint32_t)((kb / STAGES) & 1), nullptr);
+        }
+        __syncwarp();
+    } else if (warp == 1) {
+        // ---------------- MMA issuer: one lane, the warp kept converged ----------------------------
         const uint32_t id_pos = tc5_idesc(BN, false), id_neg = tc5_idesc(BN, true);
         const uint32_t c_re = tmem, c_im = tmem + BN;
         bool ok = true;
@@ -283,7 +387,7 @@ __global__ void __launch_bounds__(TC5_THREADS, 1) zgemm_tc5_kernel(const GemmDes
                 const uint32_t st = smem_u32(stage_base + (size_t)s * Cfg::STAGE);
                 const uint32_t a_rh = st, a_rl = st + Cfg::A_PART, a_ih = st + 2 * Cfg::A_PART,
                                a_il = st + 3 * Cfg::A_PART;
-                const uint32_t bb = st + Cfg::A_BYTES;
+                const uint32_t bb = st + TC5_A_BLOCK;
                 const uint32_t b_rh = bb, b_rl = bb + Cfg::B_PART, b_ih = bb + 2 * Cfg::B_PART,
                                b_il = bb + 3 * Cfg::B_PART;
                 // K chunk c of A sits at + c * 128 * 16 bytes, of B at + c * BN * 16
@@ -323,172 +427,55 @@ __global__ void __launch_bounds__(TC5_THREADS, 1) zgemm_tc5_kernel(const GemmDes
         // this arrives: commit tracks all prior MMAs of this thread
         if (lane == 0) umma_commit(done_bar);
         __syncwarp();
+    }
+
+    // ---------------- epilogue: all 8 warps ----------------------------------------------------------
+    // warp-uniform: the accumulator reads below are warp-collective
+    const bool done = __all_sync(0xffffffffu, mbar_wait(done_bar, 0u, nullptr) && !abort_flag);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!done) {
+        if (lane == 0 && !abort_flag) atomicOr(status, RB_TC5_TIMEOUT);
     } else {
-        // ---------------- producers --------------------------------------------------------------
-        const z* __restrict__ Ap = sd.A.p;
-        const z* __restrict__ Bp = sd.B.p;
-        const long long lda = sd.A.ld;
-        // cp.async of k-block kb into stage s: A element (i, k) to A + (k * 128 + i) * 16 (consecutive
-        // threads take consecutive rows: A is column-major), B element (k, j) to B + (j * KB + k) * 16
-        // (consecutive threads take consecutive k of a column)
-        auto issue = [&](int kb, int s) {
-            const int k0 = kbeg + kb * TC5_KB;
-            const uint32_t st = smem_u32(stage_base + (size_t)s * Cfg::STAGE);
-#pragma unroll
-            for (int q = 0; q < TC5_BM * TC5_KB / TC5_PRODUCERS; ++q) {
-                const int e = tid + q * TC5_PRODUCERS;
-                const int i = e % TC5_BM, kk = e / TC5_BM, k = k0 + kk;
-                const int ro = a_rows[i];
-                const bool v = ro >= 0 && k < K;
-                const z* src = v ? Ap + ro + (long long)vcol(sd.A, k) * lda : Ap;
-                cp_async16(st + (uint32_t)(kk * TC5_BM + i) * 16, src, v);
-            }
-#pragma unroll
-            for (int q = 0; q < (BN * TC5_KB + TC5_PRODUCERS - 1) / TC5_PRODUCERS; ++q) {
-                const int e = tid + q * TC5_PRODUCERS;
-                if (e >= BN * TC5_KB) break;
-                const int kk = e % TC5_KB, j = e / TC5_KB, k = k0 + kk;
-                const long long co = b_cols[j];
-                const bool v = co >= 0 && k < K;
-                const z* src = v ? Bp + vrow(sd.B, k) + co : Bp;
-                cp_async16(st + Cfg::A_BYTES + (uint32_t)(j * TC5_KB + kk) * 16, src, v);
-            }
-        };
-        // the landed FP64 pairs of stage s -> TF32 parts in place: A unit (row i, K chunk c) and B
-        // unit (column j, chunk c) read their 4 pairs, all producers pass a barrier, then write
-        // part p of A at A + p * A_PART + c * 128 * 16 + i * 16 and of B at B + p * B_PART +
-        // c * BN * 16 + j * 16 (16 bytes: the chunk's 4 TF32 values)
-        auto convert = [&](int s) {
-            unsigned char* st = stage_base + (size_t)s * Cfg::STAGE;
-            unsigned char* sb = st + Cfg::A_BYTES;
-            constexpr int AU = TC5_BM * (TC5_KB / 4) / TC5_PRODUCERS;             // 2
-            constexpr int BT = BN * (TC5_KB / 4);
-            constexpr int BU = (BT + TC5_PRODUCERS - 1) / TC5_PRODUCERS;           // 1 or 2
-            z av[AU][4], bv[BU][4];
-#pragma unroll
-            for (int u = 0; u < AU; ++u) {
-                const int unit = tid + u * TC5_PRODUCERS, i = unit % TC5_BM, c = unit / TC5_BM;
-#pragma unroll
-                for (int e = 0; e < 4; ++e) av[u][e] = *reinterpret_cast<const z*>(st + ((4 * c + e) * TC5_BM + i) * 16);
-            }
-#pragma unroll
-            for (int u = 0; u < BU; ++u) {
-                const int unit = tid + u * TC5_PRODUCERS, j = unit / 4, c = unit % 4;
-                if (unit < BT) {
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) bv[u][e] = *reinterpret_cast<const z*>(sb + (j * TC5_KB + 4 * c + e) * 16);
-                }
-            }
-            producers_sync();                    // every pair of the stage is read before any write
-#pragma unroll
-            for (int u = 0; u < AU; ++u) {
-                const int unit = tid + u * TC5_PRODUCERS, i = unit % TC5_BM, c = unit / TC5_BM;
-                uint4 rh, rl, ih, il;
-                split4(av[u], rh, rl, ih, il);
-                const size_t off = (size_t)c * TC5_BM * 16 + (size_t)i * 16;
-                *reinterpret_cast<uint4*>(st + off) = rh;
-                *reinterpret_cast<uint4*>(st + Cfg::A_PART + off) = rl;
-                *reinterpret_cast<uint4*>(st + 2 * Cfg::A_PART + off) = ih;
-                *reinterpret_cast<uint4*>(st + 3 * Cfg::A_PART + off) = il;
-            }
-#pragma unroll
-            for (int u = 0; u < BU; ++u) {
-                const int unit = tid + u * TC5_PRODUCERS, j = unit / 4, c = unit % 4;
-                if (unit >= BT) continue;
-                uint4 rh, rl, ih, il;
-                split4(bv[u], rh, rl, ih, il);
-                const size_t off = (size_t)c * BN * 16 + (size_t)j * 16;
-                *reinterpret_cast<uint4*>(sb + off) = rh;
-                *reinterpret_cast<uint4*>(sb + Cfg::B_PART + off) = rl;
-                *reinterpret_cast<uint4*>(sb + 2 * Cfg::B_PART + off) = ih;
-                *reinterpret_cast<uint4*>(sb + 3 * Cfg::B_PART + off) = il;
-            }
-        };
-        constexpr int AHEAD = Cfg::AHEAD;
-        // prologue: the first AHEAD k-blocks into fresh stages, one commit group each
-        for (int q = 0; q < AHEAD; ++q) {
-            if (q < nkb) issue(q, q);
-            cp_async_commit();
+        const int quarter = warp & 3, half = warp >> 2;
+        const int row = quarter * 32 + lane;
+        const int gi = m0 + row;
+        const bool live = gi < m;
+        long long dro = 0, cro = 0;
+        bool use_c = false;
+        if (live) {
+            dro = vrow(sd.D, gi);
+            use_c = sd.C.p && !(gi >= sd.nobeta_r0 && gi < sd.nobeta_r1);
+            if (use_c) cro = vrow(sd.C, gi);
         }
-        bool ok = true;
-        for (int kb = 0; kb < nkb; ++kb) {
-            const int s = kb % STAGES;
-            // groups committed so far: AHEAD + kb; k-block kb is the (kb+1)-th
-            cp_async_wait<AHEAD - 1>();
-            producers_sync();                    // every producer's copies of stage s have landed
-            convert(s);
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // generic -> async proxy
-            mbar_arrive(full0 + 8 * s);
-            const int kn = kb + AHEAD;
-            if (kn < nkb) {
-                const int sn = kn % STAGES;
-                if (kn >= STAGES) {
-                    // the MMAs of k-block kn - STAGES (= kb - 1) read stage sn: one thread waits
-                    // (bounded), the others at the barrier, which also agrees on giving up
-                    bool bad = false;
-                    if (tid == 0) bad = !mbar_wait(empty0 + 8 * sn, (uint32_t)(((kn / STAGES) - 1) & 1), &abort_flag);
-                    if (producers_any(bad || abort_flag)) {
-                        ok = false;
-                        break;
-                    }
-                }
-                issue(kn, sn);
-            }
-            cp_async_commit();
-        }
-        cp_async_wait<0>();                      // no copy may still target this CTA's memory
-        if (!ok) {
-            abort_flag = 1;
-            atomicOr(status, RB_TC5_TIMEOUT);
-        }
-        // ---------------- epilogue ------------------------------------------------------------------
-        // warp-uniform: the accumulator reads below are warp-collective
-        const bool done = __all_sync(0xffffffffu, mbar_wait(done_bar, 0u, &abort_flag) && !abort_flag);
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        if (!done) {
-            if (lane == 0 && !abort_flag) atomicOr(status, RB_TC5_TIMEOUT);
-        } else {
-            const int quarter = warp & 3, half = warp >> 2;
-            const int row = quarter * 32 + lane;
-            const int gi = m0 + row;
-            const bool live = gi < m;
-            long long dro = 0, cro = 0;
-            bool use_c = false;
-            if (live) {
-                dro = vrow(sd.D, gi);
-                use_c = sd.C.p && !(gi >= sd.nobeta_r0 && gi < sd.nobeta_r1);
-                if (use_c) cro = vrow(sd.C, gi);
-            }
-            const z alpha = sd.alpha, beta = sd.beta;
-            z* pp = part ? part + ((long long)blockIdx.y * ksplit + blockIdx.z) * pstride : nullptr;
-            constexpr int HALF = BN / 2;
-            constexpr int CH = HALF < 16 ? HALF : 16;
+        const z alpha = sd.alpha, beta = sd.beta;
+        z* pp = part ? part + ((long long)blockIdx.y * ksplit + blockIdx.z) * pstride : nullptr;
+        constexpr int HALF = BN / 2;
+        constexpr int CH = HALF < 16 ? HALF : 16;
 #pragma unroll 1
-            for (int c0 = half * HALF; c0 < (half + 1) * HALF; c0 += CH) {
-                float vr[16], vi[16];
-                const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
-                tmem_ld16(tmem + lane_base + (uint32_t)c0, vr);
-                tmem_ld16(tmem + lane_base + (uint32_t)(BN + c0), vi);
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                if (!live) continue;
+        for (int c0 = half * HALF; c0 < (half + 1) * HALF; c0 += CH) {
+            float vr[16], vi[16];
+            const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+            tmem_ld16(tmem + lane_base + (uint32_t)c0, vr);
+            tmem_ld16(tmem + lane_base + (uint32_t)(BN + c0), vi);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (!live) continue;
 #pragma unroll
-                for (int e = 0; e < CH; ++e) {
-                    const int gj = n0 + c0 + e;
-                    if (gj >= n) break;
-                    if (pp) {
-                        pp[gi + (long long)gj * ldp] = zmk((double)vr[e], (double)vi[e]);
-                        continue;
-                    }
-                    z v = zmul(alpha, zmk((double)vr[e], (double)vi[e]));
-                    if (use_c) zfma(v, beta, sd.C.p[cro + (long long)vcol(sd.C, gj) * sd.C.ld]);
-                    sd.D.p[dro + (long long)vcol(sd.D, gj) * sd.D.ld] = v;
+            for (int e = 0; e < CH; ++e) {
+                const int gj = n0 + c0 + e;
+                if (gj >= n) break;
+                if (pp) {
+                    pp[gi + (long long)gj * ldp] = zmk((double)vr[e], (double)vi[e]);
+                    continue;
                 }
+                z v = zmul(alpha, zmk((double)vr[e], (double)vi[e]));
+                if (use_c) zfma(v, beta, sd.C.p[cro + (long long)vcol(sd.C, gj) * sd.C.ld]);
+                sd.D.p[dro + (long long)vcol(sd.D, gj) * sd.D.ld] = v;
             }
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (warp == 8) {
+    if (warp == 1) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)Cfg::TMEM_COLS));
     }
@@ -500,11 +487,27 @@ static cudaError_t launch_tc5(const GemmBatch& b, int* status, cudaStream_t s) {
     static DeviceAttrCache attr;
     cudaError_t e = ensure_smem_attr(zgemm_tc5_kernel<BN>, Cfg::SMEM, attr, true);
     if (e != cudaSuccess) return e;
+    const PlaneGeom pg = plane_geom(b, BN);
+    unsigned char* planes = static_cast<unsigned char*>(b.t5_planes);
+    // 1. the operand planes: every A slab, then every B slab
+    {
+        constexpr int BSLABS = BN / (BN < 128 ? BN : 128);
+        const long long nA = (long long)b.count * pg.MT * pg.KBN;
+        const long long nB = (long long)b.count * pg.NT * pg.KBN * BSLABS;
+        if (nA + nB > 0x7FFFFFFFLL) return cudaErrorInvalidValue;
+        tc5_split_kernel<BN><<<(unsigned)(nA + nB), 256, 0, s>>>(b.d_desc, pg.MT, pg.NT, pg.KBN, nA, planes,
+                                                                 pg.a_bytes);
+        note_launch();
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    // 2. the products
     const int tiles = ((b.max_m + TC5_BM - 1) / TC5_BM) * ((b.max_n + BN - 1) / BN);
     if (b.t5_ksplit > 1 && b.work) {
-        if (b.count > 65535 || b.t5_ksplit > 65535) return cudaErrorInvalidValue;
+        if (b.count > 65535 || b.t5_ksplit > 65535 || b.t5_kchunk % TC5_KB) return cudaErrorInvalidValue;
         zgemm_tc5_kernel<BN><<<dim3(tiles, b.count, b.t5_ksplit), TC5_THREADS, Cfg::SMEM, s>>>(
-            b.d_desc, status, b.t5_kchunk, b.work, b.t5_pstride, b.max_m, b.t5_ksplit);
+            b.d_desc, 0, status, planes, pg.MT, pg.NT, pg.KBN, pg.a_bytes, b.t5_kchunk, b.work, b.t5_pstride,
+            b.max_m, b.t5_ksplit);
         note_launch();
         e = cudaGetLastError();
         if (e != cudaSuccess) return e;
@@ -512,8 +515,8 @@ static cudaError_t launch_tc5(const GemmBatch& b, int* status, cudaStream_t s) {
     }
     for (int off = 0; off < b.count; off += 65535) {
         const int cnt = (b.count - off) < 65535 ? (b.count - off) : 65535;
-        zgemm_tc5_kernel<BN><<<dim3(tiles, cnt), TC5_THREADS, Cfg::SMEM, s>>>(b.d_desc + off, status, 0, nullptr, 0,
-                                                                             0, 1);
+        zgemm_tc5_kernel<BN><<<dim3(tiles, cnt), TC5_THREADS, Cfg::SMEM, s>>>(
+            b.d_desc + off, off, status, planes, pg.MT, pg.NT, pg.KBN, pg.a_bytes, 0, nullptr, 0, 0, 1);
         note_launch();
     }
     return cudaGetLastError();
@@ -567,21 +570,37 @@ long long gemm_plan_split_tc5(GemmBatch& b) {
 }
 
 int tc5_tile_n(const GemmBatch& b) {
-    // n columns per tile: 32 for the narrow solve products, 128 where the 128 x 128 tiles still
-    // fill a wave of the 148 SMs (twice the operand reuse of 128 x 64), else 64
+    // RB_TC5_BN (32, 64, 128 or 256; read at every call) overrides the rule, for measurements
+    if (const char* v = std::getenv("RB_TC5_BN")) {
+        const int f = std::atoi(v);
+        if (f == 32 || f == 64 || f == 128 || f == 256) return f;
+    }
+    // n columns per tile: 32 / 64 for the narrow solve products; 256 where the 128 x 256 tiles
+    // still fill a wave of the 148 SMs (each A block then serves twice the columns), else 128
     if (b.max_n <= 32) return 32;
     if (b.max_n <= 64) return 64;
-    const long long t128 = (long long)b.count * ((b.max_m + TC5_BM - 1) / TC5_BM) * ((b.max_n + 127) / 128);
-    return t128 >= 148 ? 128 : 64;
+    const long long tm = (long long)b.count * ((b.max_m + TC5_BM - 1) / TC5_BM);
+    if (tm * ((b.max_n + 255) / 256) >= 148) return 256;
+    return 128;
+}
+
+size_t tc5_plane_bytes(const GemmBatch& b) {
+    if (b.count == 0 || b.max_m == 0 || b.max_n == 0 || b.max_k == 0) return 0;
+    const int bn = tc5_tile_n(b);
+    const PlaneGeom pg = plane_geom(b, bn);
+    return (size_t)pg.a_bytes + (size_t)b.count * pg.NT * pg.KBN * (size_t)bn * TC5_KB * 16;
 }
 
 cudaError_t launch_gemm_tc5(const GemmBatch& b, int* status, cudaStream_t s) {
     if (b.count == 0 || b.max_m == 0 || b.max_n == 0) return cudaSuccess;
-    if (!status) return cudaErrorInvalidValue;
+    if (!status || !b.t5_planes || (reinterpret_cast<uintptr_t>(b.t5_planes) & 255) ||
+        tc5_plane_bytes(b) > b.t5_plane_cap)
+        return cudaErrorInvalidValue;
     const int bn = tc5_tile_n(b);
     if (bn == 32) return launch_tc5<32>(b, status, s);
-    if (bn == 128) return launch_tc5<128>(b, status, s);
-    return launch_tc5<64>(b, status, s);
+    if (bn == 64) return launch_tc5<64>(b, status, s);
+    if (bn == 256) return launch_tc5<256>(b, status, s);
+    return launch_tc5<128>(b, status, s);
 }
 
 }  // namespace rb

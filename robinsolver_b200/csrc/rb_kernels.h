@@ -53,6 +53,8 @@ cudaError_t launch_gemm_batch(const GemmBatch& b, cudaStream_t s);
 // for the mixed-precision levels.  status: device word for RB_TC5_TIMEOUT.
 cudaError_t launch_gemm_tc5(const GemmBatch& b, int* status, cudaStream_t s);
 int tc5_tile_n(const GemmBatch& b);
+// Bytes of operand planes launch_gemm_tc5 needs for this batch (b.t5_planes).
+size_t tc5_plane_bytes(const GemmBatch& b);
 // Engines (tile shapes) of the FP64 launcher that can run a non-fixed-order batch, for the
 // autotuner: writes up to 8 engine ids to out (a batch's `engine` field takes one) and returns
 // the count.  gemm_engine_name gives each a stage-timer name.

@@ -16,10 +16,14 @@
 
 using namespace rb;
 
-extern "C" int rb_test_zgemm(int engine, int m, int n, int k, const double* dA, long long lda, long long strideA,
-                             const double* dB, long long ldb, long long strideB, double* dC, long long ldc,
-                             long long strideC, double ar, double ai, double br, double bi, int count) {
-    if (m <= 0 || n <= 0 || k <= 0 || count <= 0 || !dA || !dB || !dC || lda < m || ldb < k || ldc < m)
+// rb_test_zgemm_timed is the same call repeated `reps` times after one untimed run, and writes
+// the mean device time of one batched launch in milliseconds to *ms (CUDA events; the engine's
+// operand-split pass included).
+static int test_zgemm(int engine, int m, int n, int k, const double* dA, long long lda, long long strideA,
+                      const double* dB, long long ldb, long long strideB, double* dC, long long ldc,
+                      long long strideC, double ar, double ai, double br, double bi, int count, int reps,
+                      double* ms) {
+    if (m <= 0 || n <= 0 || k <= 0 || count <= 0 || !dA || !dB || !dC || lda < m || ldb < k || ldc < m || reps < 0)
         return RB_ERR_INVALID;
     std::vector<GemmDesc> h(count);
     const z* A = reinterpret_cast<const z*>(dA);
@@ -48,11 +52,32 @@ extern "C" int rb_test_zgemm(int engine, int m, int n, int k, const double* dA, 
         cudaFree(b.d_desc);
         return RB_ERR_CUDA;
     }
+    cudaError_t e = cudaSuccess;
+    if (engine == 1) {
+        const size_t pb = tc5_plane_bytes(b);
+        if (pb) e = cudaMalloc(&b.t5_planes, pb);
+        b.t5_plane_cap = pb;
+    }
+    auto run = [&]() { return engine == 1 ? launch_gemm_tc5(b, d_status, 0) : launch_gemm_batch(b, 0); };
     int rc = RB_OK;
-    cudaError_t e = cudaMemcpy(b.d_desc, h.data(), sizeof(GemmDesc) * count, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(b.d_desc, h.data(), sizeof(GemmDesc) * count, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(d_status, 0, sizeof(int));
-    if (e == cudaSuccess) e = engine == 1 ? launch_gemm_tc5(b, d_status, 0) : launch_gemm_batch(b, 0);
+    if (e == cudaSuccess) e = run();
     if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e == cudaSuccess && reps > 0) {
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        e = cudaEventCreate(&e0);
+        if (e == cudaSuccess) e = cudaEventCreate(&e1);
+        if (e == cudaSuccess) e = cudaEventRecord(e0, 0);
+        for (int r = 0; r < reps && e == cudaSuccess; ++r) e = run();
+        if (e == cudaSuccess) e = cudaEventRecord(e1, 0);
+        if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+        float t = 0.0f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&t, e0, e1);
+        if (e == cudaSuccess && ms) *ms = (double)t / reps;
+        if (e0) cudaEventDestroy(e0);
+        if (e1) cudaEventDestroy(e1);
+    }
     int st = 0;
     if (e == cudaSuccess) e = cudaMemcpy(&st, d_status, sizeof(int), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) {
@@ -63,7 +88,23 @@ extern "C" int rb_test_zgemm(int engine, int m, int n, int k, const double* dA, 
     }
     cudaFree(b.d_desc);
     cudaFree(d_status);
+    if (b.t5_planes) cudaFree(b.t5_planes);
     return rc;
+}
+
+extern "C" int rb_test_zgemm(int engine, int m, int n, int k, const double* dA, long long lda, long long strideA,
+                             const double* dB, long long ldb, long long strideB, double* dC, long long ldc,
+                             long long strideC, double ar, double ai, double br, double bi, int count) {
+    return test_zgemm(engine, m, n, k, dA, lda, strideA, dB, ldb, strideB, dC, ldc, strideC, ar, ai, br, bi, count,
+                      0, nullptr);
+}
+
+extern "C" int rb_test_zgemm_timed(int engine, int m, int n, int k, const double* dA, long long lda,
+                                   long long strideA, const double* dB, long long ldb, long long strideB, double* dC,
+                                   long long ldc, long long strideC, double ar, double ai, double br, double bi,
+                                   int count, int reps, double* ms) {
+    return test_zgemm(engine, m, n, k, dA, lda, strideA, dB, ldb, strideB, dC, ldc, strideC, ar, ai, br, bi, count,
+                      reps, ms);
 }
 
 // rb_test_zinvert inverts `count` complex m x m matrices in place (column-major, device pointers,

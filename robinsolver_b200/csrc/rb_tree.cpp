@@ -590,19 +590,39 @@ static int ensure_mixed_factor_plan(rb_tree* t) {
         wside = std::max(wside, gemm_plan_split_tc5_factor(t->fM1[l]));
         wrest = std::max(wrest, gemm_plan_split_tc5_factor(t->fM4N[l]));
     }
+    // and one operand-plane workspace per stream (the tcgen05 kernel's split operands)
+    size_t qmain = 0, qside = 0, qrest = 0;
+    for (int l = 0; l < t->P.L; ++l) {
+        if (!mixed_level(t, l)) continue;
+        for (GemmBatch* b : {&t->fK[l], &t->fM2[l], &t->fM3[l], &t->fM4[l], &t->fM4F[l]})
+            qmain = std::max(qmain, tc5_plane_bytes(*b));
+        qside = std::max(qside, tc5_plane_bytes(t->fM1[l]));
+        qrest = std::max(qrest, tc5_plane_bytes(t->fM4N[l]));
+    }
     z* pm = nullptr;
     z* ps = nullptr;
     z* pr = nullptr;
+    unsigned char *qm = nullptr, *qs = nullptr, *qr = nullptr;
     int rc;
     if (wmain > 0 && (rc = alloc_n(t, t->mixed_bufs, (size_t)wmain, &pm))) return rc;
     if (wside > 0 && (rc = alloc_n(t, t->mixed_bufs, (size_t)wside, &ps))) return rc;
     if (wrest > 0 && (rc = alloc_n(t, t->mixed_bufs, (size_t)wrest, &pr))) return rc;
+    if (qmain > 0 && (rc = alloc_n(t, t->mixed_bufs, qmain, &qm))) return rc;
+    if (qside > 0 && (rc = alloc_n(t, t->mixed_bufs, qside, &qs))) return rc;
+    if (qrest > 0 && (rc = alloc_n(t, t->mixed_bufs, qrest, &qr))) return rc;
     for (int l = 0; l < t->P.L; ++l) {
         if (!mixed_level(t, l)) continue;
-        for (GemmBatch* b : {&t->fK[l], &t->fM2[l], &t->fM3[l], &t->fM4[l], &t->fM4F[l]})
+        for (GemmBatch* b : {&t->fK[l], &t->fM2[l], &t->fM3[l], &t->fM4[l], &t->fM4F[l]}) {
             if (b->t5_ksplit > 1) b->work = pm;
+            b->t5_planes = qm;
+            b->t5_plane_cap = qmain;
+        }
         if (t->fM1[l].t5_ksplit > 1) t->fM1[l].work = ps;
+        t->fM1[l].t5_planes = qs;
+        t->fM1[l].t5_plane_cap = qside;
         if (t->fM4N[l].t5_ksplit > 1) t->fM4N[l].work = pr;
+        t->fM4N[l].t5_planes = qr;
+        t->fM4N[l].t5_plane_cap = qrest;
     }
     t->mixed_plan = true;
     return RB_OK;
@@ -781,6 +801,8 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
         drop_graph(t->gx_solve);
         t->gx_solve_rhs = 0;
         free_list(t, t->solve_bufs);
+        t->solve_planes = nullptr;
+        t->solve_planes_bytes = 0;
         t->built_rhs = 0;
         const int k = nrhs;
         if ((rc = alloc_n(t, t->solve_bufs, (size_t)k * nl * ab, &t->d_f))) return rc;
@@ -959,6 +981,31 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
 // out: where the leaf solutions go (t->sol when null).  inject: subtract the interface rows of
 // the residual (t->d_ri) from the children's outgoing data before each level's merge (the
 // correction sweeps of the mixed-precision refinement).
+// Operand planes of the solve batches that run on the tcgen05 kernel (RB_MIXED_SOLVE_ENGINE=tc5):
+// one workspace for them all (the sweep is one stream), grown on first use.
+static int ensure_solve_planes(rb_tree* t) {
+    const int L = t->P.L;
+    std::vector<GemmBatch*> mixed;
+    if (mixed_level(t, L)) mixed.push_back(&t->sL0);
+    for (int l = 1; l < L; ++l)
+        if (mixed_level(t, l))
+            for (GemmBatch* gb : {&t->sF12[l], &t->sF3[l], &t->sF4[l], &t->sF5[l], &t->sBY[l]}) mixed.push_back(gb);
+    size_t need = 0;
+    for (GemmBatch* gb : mixed) need = std::max(need, tc5_plane_bytes(*gb));
+    if (need > t->solve_planes_bytes) {
+        unsigned char* q = nullptr;
+        int rc = alloc_n(t, t->solve_bufs, need, &q);
+        if (rc) return rc;
+        t->solve_planes = q;
+        t->solve_planes_bytes = need;
+    }
+    for (GemmBatch* gb : mixed) {
+        gb->t5_planes = t->solve_planes;
+        gb->t5_plane_cap = t->solve_planes_bytes;
+    }
+    return RB_OK;
+}
+
 static int run_solve(rb_tree* t, int k, cudaStream_t s, const std::vector<cudaEvent_t>* wait = nullptr,
                      z* out = nullptr, bool inject = false) {
     const Plan& P = t->P;
@@ -966,6 +1013,7 @@ static int run_solve(rb_tree* t, int k, cudaStream_t s, const std::vector<cudaEv
     LeafGeom lg{P.leaf_a(), P.leaf_b(), P.leaf_nb(), P.leaf_n(), P.kb};
     int rc;
     const bool sweep_fp64 = mixed_solve_fp64();
+    if (!sweep_fp64 && t->prec == RB_PREC_MIXED && (rc = ensure_solve_planes(t))) return rc;
 #define RB_GEMM_S(batch, level, stream)                                                          \
     do {                                                                                         \
         if (sweep_fp64) RB_GEMM(batch, stream);                                                  \

@@ -118,6 +118,8 @@ struct rb_tree {
     std::vector<GemmBatch> sF12, sF3, sF4, sF5, sBY;
     GemmBatch sR1;                   // root: x_i = h_i + T_iN g_N (no K^-1 needed)
     std::vector<DevBuf> solve_bufs;
+    unsigned char* solve_planes = nullptr;   // tcgen05 operand planes of the solve (mixed, tc5 sweeps)
+    size_t solve_planes_bytes = 0;
 
     // timing: 0 off, 1 per stage, 2 per launch
     int timing = 0;
