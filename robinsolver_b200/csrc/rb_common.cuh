@@ -122,6 +122,9 @@ struct GemmBatch {
     // shared-memory stages hold them
     void* t5_planes = nullptr;
     size_t t5_plane_cap = 0;      // bytes at t5_planes; a launch that needs more is refused
+    // arithmetic of the tensor-core engine: 0 split TF32 ("TF32x3"), 1 int8 digit slices with
+    // exact integer accumulation (Ozaki scheme); -1: the process default (tc5_engine)
+    int t5_engine = -1;
     // FP64 engine (tile shape) chosen by an autotuner; -1: the launcher's own rule
     int engine = -1;
 };

@@ -49,9 +49,16 @@ constexpr int RB_TC5_TIMEOUT = 4;           // a tensor-core GEMM CTA gave up wa
 
 // ---- batched GEMM ---------------------------------------------------------------------------------
 cudaError_t launch_gemm_batch(const GemmBatch& b, cudaStream_t s);
-// The same batch on the tcgen05 tensor cores in split TF32 (rb_gemm_tc5.cu): ~1e-6 relative error,
-// for the mixed-precision levels.  status: device word for RB_TC5_TIMEOUT.
+// The same batch on the tcgen05 tensor cores (rb_gemm_tc5.cu), for the mixed-precision levels, in
+// one of two arithmetics (b.t5_engine): split TF32 with FP32 accumulation (~1e-7 of
+// max|A| max|B| k), or the default, int8 digit slices of row- and column-scaled operands with
+// exact int32 accumulation (~1e-10 of that scale).  status: device word for RB_TC5_TIMEOUT.
 cudaError_t launch_gemm_tc5(const GemmBatch& b, int* status, cudaStream_t s);
+constexpr int TC5_ENGINE_TF32X3 = 0;
+constexpr int TC5_ENGINE_INT8 = 1;
+// the engine a batch runs on: its own t5_engine, else the process default (RB_MIXED_ENGINE =
+// "tf32x3" or "int8", read once; int8 when unset)
+int tc5_engine(const GemmBatch& b);
 int tc5_tile_n(const GemmBatch& b);
 // Bytes of operand planes launch_gemm_tc5 needs for this batch (b.t5_planes).
 size_t tc5_plane_bytes(const GemmBatch& b);

@@ -4,7 +4,8 @@
 // pointers, plain strided views) on one engine, so that the tests can hold each engine against a
 // host product directly:
 //   engine 0: the FP64 launcher the FP64 path uses (tensor-core DMMA / DFMA tiles)
-//   engine 1: the tcgen05 split-TF32 kernel of the mixed-precision levels
+//   engine 1: the tcgen05 kernel of the mixed-precision levels in split TF32
+//   engine 2: the tcgen05 kernel in int8 digit slices (the mixed-precision default)
 // It allocates its descriptor array itself and synchronises; it returns 0, a negative RB_ERR_*
 // code for bad arguments or CUDA failures, or the device status word's bits (> 0) when a kernel
 // reported one.
@@ -53,12 +54,13 @@ static int test_zgemm(int engine, int m, int n, int k, const double* dA, long lo
         return RB_ERR_CUDA;
     }
     cudaError_t e = cudaSuccess;
-    if (engine == 1) {
+    if (engine == 1 || engine == 2) {
+        b.t5_engine = engine == 2 ? TC5_ENGINE_INT8 : TC5_ENGINE_TF32X3;
         const size_t pb = tc5_plane_bytes(b);
         if (pb) e = cudaMalloc(&b.t5_planes, pb);
         b.t5_plane_cap = pb;
     }
-    auto run = [&]() { return engine == 1 ? launch_gemm_tc5(b, d_status, 0) : launch_gemm_batch(b, 0); };
+    auto run = [&]() { return engine != 0 ? launch_gemm_tc5(b, d_status, 0) : launch_gemm_batch(b, 0); };
     int rc = RB_OK;
     if (e == cudaSuccess) e = cudaMemcpy(b.d_desc, h.data(), sizeof(GemmDesc) * count, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(d_status, 0, sizeof(int));

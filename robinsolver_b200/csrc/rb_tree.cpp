@@ -563,8 +563,26 @@ static bool mixed_level(const rb_tree* t, int l) {
     if (t->prec != RB_PREC_MIXED || l < 2) return false;
     return l == t->P.L || t->P.lv[l].m >= 128;
 }
+// Which factor stages of a mixed level run on the tcgen05 kernel: RB_MIXED_STAGES (read at every
+// launch) is a bit mask over K = nu^2 I - A2 A1 (1), B1 (2), Y1 (4), Y2 (8) and the parent map
+// (16); the default is all of them.  The solve's batches follow their level.
+static int mixed_stage_mask() {
+    const char* v = std::getenv("RB_MIXED_STAGES");
+    return v ? std::atoi(v) : 31;
+}
+static bool mixed_batch(const rb_tree* t, const GemmBatch& b, int l) {
+    if (!mixed_level(t, l)) return false;
+    if (l >= t->P.L) return true;
+    int bit = 0;
+    if (&b == &t->fK[l]) bit = 1;
+    else if (&b == &t->fM1[l]) bit = 2;
+    else if (&b == &t->fM2[l]) bit = 4;
+    else if (&b == &t->fM3[l]) bit = 8;
+    else if (&b == &t->fM4[l] || &b == &t->fM4F[l] || &b == &t->fM4N[l]) bit = 16;
+    return bit == 0 || (mixed_stage_mask() & bit) != 0;
+}
 static cudaError_t launch_gemm_level(rb_tree* t, const GemmBatch& b, int l, cudaStream_t s) {
-    return mixed_level(t, l) ? launch_gemm_tc5(b, t->d_status, s) : launch_gemm_batch(b, s);
+    return mixed_batch(t, b, l) ? launch_gemm_tc5(b, t->d_status, s) : launch_gemm_batch(b, s);
 }
 // The mixed solve applies its factor with the FP64 GEMMs: the sweeps' products are narrow (n =
 // the right-hand sides), where the tcgen05 tile is slower than the FP64 one (1024^2, L=12, 32
@@ -629,7 +647,7 @@ static int ensure_mixed_factor_plan(rb_tree* t) {
 }
 
 #define RB_GEMM_L(batch, level, stream)                                                          \
-    RB_TIMED(mixed_level(t, level) ? "zgemm_tc5" : gemm_stage_name(batch), (batch).flops,         \
+    RB_TIMED(mixed_batch(t, batch, level) ? "zgemm_tc5" : gemm_stage_name(batch), (batch).flops,  \
              launch_gemm_level(t, batch, level, stream))
 
 static double gj_flops(int m, int count) { return 8.0 * (double)m * m * m * count; }
