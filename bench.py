@@ -9,11 +9,15 @@ One step = the reference's hot path on one batch: robin_tree%factor of the 1024^
 (16x16 leaves, kb=200, seeded 100-bump potential with 0.002i*kb damping) followed by one batched
 solve of its 32 seeded plane-wave right-hand sides and get_solution.  ``value`` is right-hand
 sides per second with the factorization inside every step, so it moves with both factor time
-and solve throughput.  Both precisions run on the same inputs in the same run: the plain FP64
-path (the headline arm, ``value``: the faster of the two on this workload) and the mixed-precision
-path (``mixed``: RB_PREC_MIXED, split-TF32 tcgen05 GEMMs on the merge levels 2-6 and the solve's
-leaf GEMM, FP64 elsewhere, every solve refined to 1e-10 against the FP64 residual), with
-``mixed_vs_fp64`` their factor, solve and step ratios.  ``--precision mixed`` swaps the roles.
+and solve throughput.  Three arms run on the same inputs in the same run: the plain FP64 path
+(the headline arm, ``value``, the reference's precision), the mixed-precision path (``mixed``:
+RB_PREC_MIXED, the B1, Y1, Y2 and parent-map GEMMs of merge levels 2-4 on the tcgen05 tensor
+cores in int8 digit slices with exact integer accumulation, FP64 elsewhere including the top two
+levels, every solve refined to 1e-10 against the FP64 residual), and ``mixed_int8_top``, the
+same with the top two levels' GEMMs on the int8 engine too (RB_FLAG_MIXED_INT8_TOP; their
+inversions stay FP64), each with its factor, solve and step ratios against FP64
+(``mixed_vs_fp64``, ``mixed_int8_top_vs_fp64``).  ``--precision mixed`` makes the mixed arm the
+headline.
 
 * value:  device-resident inputs (rb_tree_factor_device / rb_tree_solve_device /
           rb_get_solution_device), CUDA events on the library's stream, max over ranks.
@@ -26,8 +30,8 @@ leaf GEMM, FP64 elsewhere, every solve refined to 1e-10 against the FP64 residua
 * roofline: per-launch CUDA events over a second pass of the same steps give the dominant
           kernel family's algorithmic flops / time, against the peak of the pipe it runs on: the
           complex128 cuBLAS GEMM measured in this run (FP64 kernels; MEASURED_PEAKS.json has no
-          FP64 entry) or MEASURED_PEAKS.json's bf16 rate / 2 (TF32) / 3 (split products) for the
-          tcgen05 kernel.
+          FP64 entry) or, for the tcgen05 kernel, MEASURED_PEAKS.json's bf16 rate x 2 (int8) / 15
+          (int8 operations per algorithmic flop of the digit-slice product; split TF32: / 2 / 3).
 * cpu_baseline / --impl reference: the reference's LAPACK/BLAS call sequence (oracle port, scipy
           OpenBLAS, all host threads) MEASURED on the whole workload: the full factor (every leaf
           and merge) and a few single-RHS solves (the reference solves one right-hand side per
@@ -416,11 +420,12 @@ class Arm:
     def __init__(self, rb, _lib, wl, precision, kv, d_k, d_f, d_g, nrhs):
         self.lib = _lib.lib
         self._lib = _lib
-        self.precision = precision
-        self.prec = _lib.RB_PREC_MIXED if precision == "mixed" else _lib.RB_PREC_FP64
+        # "mixed_int8_top": the mixed factor with its top two levels' GEMMs on the int8 engine too
+        self.precision = "mixed" if precision.startswith("mixed") else "fp64"
+        self.prec = _lib.RB_PREC_MIXED if self.precision == "mixed" else _lib.RB_PREC_FP64
         # RB_FLAG_ASYNC_FACTOR: the host factor call returns once enqueued, so that the e2e step's
         # right-hand-side upload overlaps the factor (the device-path calls are asynchronous anyway)
-        self.T = rb.robin_tree(async_factor=True)
+        self.T = rb.robin_tree(async_factor=True, mixed_int8_top=(precision == "mixed_int8_top"))
         self.T.bndry_params = wl.bndry_params
         op = rb.elliptic_operator(d=2, domain=wl.domain, k=wl.potential)
         opts = rb.solve_opts(h_tgt=wl.h_tgt, kb=wl.opts_kb)
@@ -498,10 +503,13 @@ def roofline_block(arm, torch, dev, steps, zpeak, bf16_peak):
     shares = {k: round(v[1] / tot, 4) for k, v in per.items()}
     dname, (dcnt, dms, dflops) = max(per.items(), key=lambda kv_: kv_[1][1])
     achieved = dflops / (dms * 1e-3) / 1e12 if dflops > 0 else None
-    # split TF32 on tcgen05: the dense TF32 rate is half the measured bf16 rate, and every complex
-    # multiply-add is 4 real ones x 3 split products: algorithmic 8mnk is a third of the executed
-    # 24mnk real tensor flops
-    tc5_peak = bf16_peak / 2.0 / 3.0 if bf16_peak else None
+    # the tcgen05 kernel's ceiling in algorithmic flops.  int8 digit slices (the default engine):
+    # the dense int8 rate is twice the measured bf16 rate, and a 128 x 48 complex tile takes 30
+    # int8 MMAs of 128 x 96 x 32 per 32-deep k-block, 23.6 M int8 operations for 1.57 M algorithmic
+    # flops (15 per flop).  Split TF32: the TF32 rate is half the bf16 rate, and every complex
+    # multiply-add is 4 real ones x 3 split products (3 per flop).
+    int8 = os.environ.get("RB_MIXED_ENGINE", "int8") != "tf32x3"
+    tc5_peak = (bf16_peak * 2.0 / 15.0 if int8 else bf16_peak / 2.0 / 3.0) if bf16_peak else None
     fams = {}
     for k, v in per.items():
         if v[2] > 0:
@@ -509,8 +517,11 @@ def roofline_block(arm, torch, dev, steps, zpeak, bf16_peak):
             fams[k] = {"launches": v[0], "ms": round(v[1], 3), "tflops": round(v[2] / (v[1] * 1e-3) / 1e12, 2),
                        "frac": round(v[2] / (v[1] * 1e-3) / 1e12 / pk, 3) if pk else None}
     if dname == "zgemm_tc5":
-        peak, pipe, src = tc5_peak, "tf32 (tcgen05, split x3)", \
-            "MEASURED_PEAKS.json bf16_tflops / 2 (dense TF32) / 3 (split products per complex term)"
+        peak, pipe, src = (tc5_peak, "int8 (tcgen05, 5 digit slices)",
+                           "MEASURED_PEAKS.json bf16_tflops x 2 (dense int8) / 15 (int8 operations per algorithmic "
+                           "flop)") if int8 else \
+            (tc5_peak, "tf32 (tcgen05, split x3)",
+             "MEASURED_PEAKS.json bf16_tflops / 2 (dense TF32) / 3 (split products per complex term)")
     else:
         peak, pipe, src = zpeak, "fp64", "complex128 cuBLAS GEMM 4096^3 measured in this run (no FP64 entry in " \
                                          "MEASURED_PEAKS.json)"
@@ -564,7 +575,9 @@ def our_arm(args):
     d_g = torch.from_numpy(G).to(dev)
     main = args.precision
     other = "fp64" if main == "mixed" else "mixed"
-    order = (main,) if args.single_arm else (main, other)
+    # the third arm: the mixed factor with the top two levels' GEMMs on the int8 engine as well
+    # (RB_FLAG_MIXED_INT8_TOP), beyond the configuration's FP64 top levels
+    order = (main,) if args.single_arm else (main, other, "mixed_int8_top")
     arms = {p: Arm(rb, _lib, wl, p, kv, d_k, d_f, d_g, nrhs) for p in order}
 
     # ---- timed regions: the headline precision, then the other one --------------------------------
@@ -587,11 +600,16 @@ def our_arm(args):
 
     # ---- accuracy: mixed vs FP64 GPU on every right-hand side, both vs the FP64 CPU solve ------------
     U = {p: arms[p].d_u.cpu().numpy() for p in arms}
-    both = len(arms) == 2
-    if both:
-        mix_vs_fp64 = [float(np.abs(U["mixed"][r] - U["fp64"][r]).max() / np.abs(U["fp64"][r]).max())
-                       for r in range(nrhs)]
-        it, rho, est, resid = arms["mixed"].T.refine_info()
+    both = len(arms) >= 2
+
+    def vs_fp64(p):
+        errs = [float(np.abs(U[p][r] - U["fp64"][r]).max() / np.abs(U["fp64"][r]).max()) for r in range(nrhs)]
+        it, rho, est, resid = arms[p].T.refine_info()
+        return {"step_speedup": res["fp64"]["total_ms"] / res[p]["total_ms"],
+                "factor_speedup": res["fp64"]["factor_ms"] / res[p]["factor_ms"],
+                "solve_speedup": res["fp64"]["solve_ms"] / res[p]["solve_ms"],
+                "max_rel_err_all_rhs": max(errs), "refine_corrections": it, "contraction": rho,
+                "estimated_error": est, "residual": resid}
 
     # ---- roofline of the headline precision ---------------------------------------------------------
     zpeak = zgemm_peak_tflops(torch, dev)
@@ -666,12 +684,12 @@ def our_arm(args):
         cpu = cpu_baseline_block(wl, nrhs)
 
     if rank == 0:
-        r0, r1 = res[main], res.get(other)
+        r0, r1, r2 = res[main], res.get(other), res.get("mixed_int8_top")
         out = {
             "metric": METRIC, "value": r0["value"], "unit": "RHS/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": r0["total_ms"] / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "complex128" if main == "fp64" else
-            "complex128 storage; tf32x3 tensor-core GEMMs on levels 2-6, fp64 elsewhere",
+            "complex128 storage; int8 digit-slice tensor-core GEMMs on levels 2-4, fp64 elsewhere",
             "data": "synthetic (seeded potential and plane waves, no dataset)",
             "config": config_dict(args.config, nrhs, main),
             "factor_ms": r0["factor_ms"], "solve_ms": r0["solve_ms"],
@@ -680,12 +698,13 @@ def our_arm(args):
             other: None if r1 is None else {
                 "value": r1["value"], "ms_per_step": r1["total_ms"] / args.steps, "factor_ms": r1["factor_ms"],
                 "solve_ms": r1["solve_ms"], "solves_per_s_resident": nrhs / (r1["solve_ms"] * 1e-3)},
-            "mixed_vs_fp64": None if not both else {
-                "step_speedup": res["fp64"]["total_ms"] / res["mixed"]["total_ms"],
-                "factor_speedup": res["fp64"]["factor_ms"] / res["mixed"]["factor_ms"],
-                "solve_speedup": res["fp64"]["solve_ms"] / res["mixed"]["solve_ms"],
-                "max_rel_err_all_rhs": max(mix_vs_fp64), "refine_corrections": it, "contraction": rho,
-                "estimated_error": est, "residual": resid},
+            "mixed_int8_top": None if not both else {
+                "value": r2["value"], "ms_per_step": r2["total_ms"] / args.steps, "factor_ms": r2["factor_ms"],
+                "solve_ms": r2["solve_ms"], "solves_per_s_resident": nrhs / (r2["solve_ms"] * 1e-3),
+                "what": "RB_FLAG_MIXED_INT8_TOP: the mixed factor with the top two merge levels' GEMMs on the "
+                        "int8 engine as well (their inversions FP64)"},
+            "mixed_vs_fp64": None if not both else vs_fp64("mixed"),
+            "mixed_int8_top_vs_fp64": None if not both else vs_fp64("mixed_int8_top"),
             "backward_error": bw, "forward_error": fwd,
             "roofline": roof, "cpu_baseline": cpu, "e2e": e2e,
             "gpu_launches": int(r0["launches"]), "clocks": clk,

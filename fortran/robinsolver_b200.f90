@@ -72,12 +72,14 @@ module robinsolver_b200
     end type
 
     ! Extensions of this library, kept out of solve_opts so that it stays the reference's type:
-    ! precision 'fp64' (RB_PREC_FP64) or 'mixed' (RB_PREC_MIXED: split-TF32 tensor-core GEMMs on
-    ! the lower merge levels, every solve refined against the FP64 residual to tol).
+    ! precision 'fp64' (RB_PREC_FP64) or 'mixed' (RB_PREC_MIXED: int8 tensor-core GEMMs on the
+    ! lower merge levels, every solve refined against the FP64 residual to tol); int8_top: the
+    ! mixed factor's top two levels on the tensor cores too (RB_FLAG_MIXED_INT8_TOP).
     type b200_opts
         character(len=5) :: precision = 'fp64'
         real(dp) :: tol = 1.0d-10
         integer :: max_iter = 8
+        logical :: int8_top = .false.
     end type
 
     type robin_tree
@@ -217,7 +219,7 @@ contains
                           real(T%bndry_params(1,2)), aimag(T%bndry_params(1,2)), &
                           real(T%bndry_params(2,2)), aimag(T%bndry_params(2,2))]
         g%ordering = opts%ordering
-        g%flags = merge(2, 0, opts%debug%txt_output)
+        g%flags = merge(2, 0, opts%debug%txt_output) + merge(32, 0, T%b200%int8_top)
         g%device_budget = 0
         call check(rb_tree_create(g, T%handle), c_null_ptr)
         call check(rb_tree_info(T%handle, info), T%handle)

@@ -80,6 +80,10 @@ extern "C" {
                                      root's own RtR map, which no solve reads, may still be
                                      computed behind it (rb_tree_get_rtr and the next factor
                                      wait for it).                                              */
+#define RB_FLAG_MIXED_INT8_TOP 32 /* RB_PREC_MIXED only: the top two merge levels' GEMMs also run on the
+                                     int8 tensor-core engine (~1e-11 of max|A| max|B| k); their
+                                     interface inversions stay FP64.  Without it those levels are FP64,
+                                     as the mixed-precision configuration prescribes.               */
 #define RB_FLAG_MERGE_DS      8   /* interface solve as the reference writes it, inv(D) and inv(S)
                                      (compute_RTR, robin_tree_module.f90:449-470), instead of the
                                      default single inversion of K = nu^2 I - (zeta I - T2_ii)(zeta I -

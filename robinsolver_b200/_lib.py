@@ -37,6 +37,7 @@ RB_FLAG_VERBOSE = 2
 RB_FLAG_NO_GRAPHS = 4
 RB_FLAG_MERGE_DS = 8
 RB_FLAG_ASYNC_FACTOR = 16
+RB_FLAG_MIXED_INT8_TOP = 32
 RB_FIELD_BUMP_POTENTIAL = 0
 RB_FIELD_POINT_SOURCE = 1
 RB_FIELD_PLANE_WAVE = 2

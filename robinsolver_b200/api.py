@@ -137,7 +137,7 @@ class robin_tree:
     """robin_tree (robin_tree_module.f90:55-77) backed by a device-resident factorization."""
 
     def __init__(self, device_budget: int = 0, skip_root_rtr: bool = False, merge_ds: bool = False,
-                 async_factor: bool = False, graphs: bool = True):
+                 async_factor: bool = False, graphs: bool = True, mixed_int8_top: bool = False):
         self.bndry_params = None
         self.nlvls = 0
         self.ell_op = None
@@ -152,6 +152,7 @@ class robin_tree:
         self._merge_ds = bool(merge_ds)     # the reference's inv(D), inv(S) interface solve
         self._async = bool(async_factor)    # factor returns when enqueued (RB_FLAG_ASYNC_FACTOR)
         self._graphs = bool(graphs)         # replay factor/solve as CUDA graphs (else RB_FLAG_NO_GRAPHS)
+        self._int8_top = bool(mixed_int8_top)   # mixed factor: top two levels' GEMMs on the int8 engine too
 
     # -- handle ----------------------------------------------------------------------------------
     def close(self):
@@ -178,6 +179,7 @@ class robin_tree:
                 (_lib.RB_FLAG_SKIP_ROOT_RTR if self._skip_root else 0) | \
                 (_lib.RB_FLAG_MERGE_DS if self._merge_ds else 0) | \
                 (_lib.RB_FLAG_ASYNC_FACTOR if self._async else 0) | \
+                (_lib.RB_FLAG_MIXED_INT8_TOP if self._int8_top else 0) | \
                 (0 if self._graphs else _lib.RB_FLAG_NO_GRAPHS)
         g = make_geom(L, ell_op, opts, self.bndry_params, flags, self._budget)
         h = _lib.C.c_void_p()

@@ -62,81 +62,98 @@ __device__ __forceinline__ void atomic_max_nonneg(double* p, double v) {
 
 }  // namespace
 
-// One CTA per (leaf, rhs).  d: the vector whose residual is taken ([rhs][leaf][n]); f: interior
-// rows ([rhs][leaf][ab]), groot: domain-boundary rows ([rhs][root_nb]), ri: interface rows
-// ([rhs][leaf][nb]), all updated in place (ri read as zero when first).  bclass[leaf*nb + r]:
-// >= 0 the root boundary position of a domain-boundary point, < 0 -1 - (leaf'*nb + r') of the
-// neighbour's row for the same point.  rnorm[rhs]: max |r| over every row, accumulated.
-__global__ void __launch_bounds__(128) fd_residual_kernel(RefineGeom g, const z* __restrict__ d, z* f, z* groot,
-                                                         z* ri, const z* __restrict__ kv, const double* __restrict__ hh,
-                                                         const int* __restrict__ bclass, int first, double* rnorm) {
+// One CTA per RES_LEAVES consecutive leaves of one right-hand side (blockIdx.y).  d: the vector
+// whose residual is taken ([rhs][leaf][n]); f: interior rows ([rhs][leaf][ab]), groot:
+// domain-boundary rows ([rhs][root_nb]), ri: interface rows ([rhs][leaf][nb]), all updated in
+// place (ri read as zero when first).  bclass[leaf*nb + r]: >= 0 the root boundary position of a
+// domain-boundary point, < 0 -1 - (leaf'*nb + r') of the neighbour's row for the same point.
+// rnorm[rhs]: max |r| over every row, accumulated with one atomic per CTA (one per warp and leaf
+// serialised half a million atomics on the L2 slices holding rnorm).
+constexpr int RES_LEAVES = 16;
+constexpr int RES_THREADS = 128;
+__global__ void __launch_bounds__(RES_THREADS) fd_residual_kernel(RefineGeom g, const z* __restrict__ d, z* f,
+                                                                 z* groot, z* ri, const z* __restrict__ kv,
+                                                                 const double* __restrict__ hh,
+                                                                 const int* __restrict__ bclass, int first,
+                                                                 double* rnorm) {
     extern __shared__ z ush[];
-    const int leaf = blockIdx.x, rhs = blockIdx.y;
+    __shared__ double wmax[RES_THREADS / 32];
+    const int rhs = blockIdx.y;
     const int a = g.a, b = g.b, nb = 2 * (a + b), ab = a * b, n = nb + ab;
-    const z* u = d + ((long long)rhs * g.nleaves + leaf) * n;
-    for (int e = threadIdx.x; e < n; e += blockDim.x) ush[e] = u[e];
-    __syncthreads();
-    const double hx = hh[2 * leaf], hy = hh[2 * leaf + 1];
     const z ikb = zmk(0.0, g.kb), mikb = zmk(0.0, -g.kb);
     double mx = 0.0;
-    for (int e = threadIdx.x; e < n; e += blockDim.x) {
-        if (e >= nb) {
-            const int q = e - nb;
-            const int gi = q % a + 1, gj = q / a + 1;
-            z acc = zmul(kv[(long long)leaf * ab + q], ush[e]);
-            // x then y, each the [w0, w1, w2] stencil of FD_matrix_row (fd_module.f90:150-181)
-            for (int dim = 0; dim < 2; ++dim) {
-                const int gg = dim == 0 ? gi : gj, len = dim == 0 ? a : b;
-                double w0 = 1.0, w1 = -2.0, w2 = 1.0;
-                if (gg == 1) { w0 = 8.0 / 3.0; w1 = -4.0; w2 = 4.0 / 3.0; }
-                else if (gg == len) { w0 = 4.0 / 3.0; w1 = -4.0; w2 = 8.0 / 3.0; }
-                const double h2 = dim == 0 ? hx * hx : hy * hy;
-                const int eu = dim == 0 ? leaf_lin(gi + 1, gj, a, b) : leaf_lin(gi, gj + 1, a, b);
-                const int ed = dim == 0 ? leaf_lin(gi - 1, gj, a, b) : leaf_lin(gi, gj - 1, a, b);
-                acc = zadd(acc, zscale(w1 / h2, ush[e]));
-                acc = zadd(acc, zscale(w2 / h2, ush[eu]));
-                acc = zadd(acc, zscale(w0 / h2, ush[ed]));
-            }
-            z* fp = f + ((long long)rhs * g.nleaves + leaf) * ab + q;
-            const z r = zsub(*fp, acc);
-            *fp = r;
-            mx = fmax(mx, fabs(r.x) + fabs(r.y));
-        } else {
-            int e1, e2, axis;
-            leaf_bnd(e, a, b, e1, e2, axis);
-            const double hn = axis == 0 ? hx : hy;
-            const z dn = dn_u(ush, e, e1, e2, hn);
-            const z gin = zadd(zmul(ikb, ush[e]), dn);
-            const int cls = bclass[(long long)leaf * nb + e];
-            z r;
-            if (cls >= 0) {
-                z* gp = groot + (long long)rhs * g.root_nb + cls;
-                r = zsub(*gp, gin);
-                *gp = r;
+    const int l0 = blockIdx.x * RES_LEAVES;
+    const int l1 = min(g.nleaves, l0 + RES_LEAVES);
+    for (int leaf = l0; leaf < l1; ++leaf) {
+        const z* u = d + ((long long)rhs * g.nleaves + leaf) * n;
+        __syncthreads();                       // the previous leaf's reads of ush are done
+        for (int e = threadIdx.x; e < n; e += blockDim.x) ush[e] = u[e];
+        __syncthreads();
+        const double hx = hh[2 * leaf], hy = hh[2 * leaf + 1];
+        for (int e = threadIdx.x; e < n; e += blockDim.x) {
+            if (e >= nb) {
+                const int q = e - nb;
+                const int gi = q % a + 1, gj = q / a + 1;
+                z acc = zmul(kv[(long long)leaf * ab + q], ush[e]);
+                // x then y, each the [w0, w1, w2] stencil of FD_matrix_row (fd_module.f90:150-181)
+                for (int dim = 0; dim < 2; ++dim) {
+                    const int gg = dim == 0 ? gi : gj, len = dim == 0 ? a : b;
+                    double w0 = 1.0, w1 = -2.0, w2 = 1.0;
+                    if (gg == 1) { w0 = 8.0 / 3.0; w1 = -4.0; w2 = 4.0 / 3.0; }
+                    else if (gg == len) { w0 = 4.0 / 3.0; w1 = -4.0; w2 = 8.0 / 3.0; }
+                    const double h2 = dim == 0 ? hx * hx : hy * hy;
+                    const int eu = dim == 0 ? leaf_lin(gi + 1, gj, a, b) : leaf_lin(gi, gj + 1, a, b);
+                    const int ed = dim == 0 ? leaf_lin(gi - 1, gj, a, b) : leaf_lin(gi, gj - 1, a, b);
+                    acc = zadd(acc, zscale(w1 / h2, ush[e]));
+                    acc = zadd(acc, zscale(w2 / h2, ush[eu]));
+                    acc = zadd(acc, zscale(w0 / h2, ush[ed]));
+                }
+                z* fp = f + ((long long)rhs * g.nleaves + leaf) * ab + q;
+                const z r = zsub(*fp, acc);
+                *fp = r;
+                mx = fmax(mx, fabs(r.x) + fabs(r.y));
             } else {
-                const int other = -1 - cls;
-                const int lj = other / nb, rj = other % nb;
-                const z* un = d + ((long long)rhs * g.nleaves + lj) * n;
-                int f1, f2, ax2;
-                leaf_bnd(rj, a, b, f1, f2, ax2);
-                const double hn2 = ax2 == 0 ? hh[2 * lj] : hh[2 * lj + 1];
-                z dn2 = zscale((8.0 / 3.0) / hn2, un[rj]);
-                dn2 = zadd(dn2, zscale(-3.0 / hn2, un[f1]));
-                dn2 = zadd(dn2, zscale((1.0 / 3.0) / hn2, un[f2]));
-                const z gin2 = zadd(zmul(ikb, un[rj]), dn2);
-                const z hout = zadd(zmul(mikb, ush[e]), dn);
-                // transmission row: h_out - zeta g_in - nu g_in' = 0
-                const z row = zsub(zsub(hout, zmul(g.zeta, gin)), zmul(g.nu, gin2));
-                z* rp = ri + ((long long)rhs * g.nleaves + leaf) * nb + e;
-                r = first ? zneg(row) : zsub(*rp, row);
-                *rp = r;
+                int e1, e2, axis;
+                leaf_bnd(e, a, b, e1, e2, axis);
+                const double hn = axis == 0 ? hx : hy;
+                const z dn = dn_u(ush, e, e1, e2, hn);
+                const z gin = zadd(zmul(ikb, ush[e]), dn);
+                const int cls = bclass[(long long)leaf * nb + e];
+                z r;
+                if (cls >= 0) {
+                    z* gp = groot + (long long)rhs * g.root_nb + cls;
+                    r = zsub(*gp, gin);
+                    *gp = r;
+                } else {
+                    const int other = -1 - cls;
+                    const int lj = other / nb, rj = other % nb;
+                    const z* un = d + ((long long)rhs * g.nleaves + lj) * n;
+                    int f1, f2, ax2;
+                    leaf_bnd(rj, a, b, f1, f2, ax2);
+                    const double hn2 = ax2 == 0 ? hh[2 * lj] : hh[2 * lj + 1];
+                    z dn2 = zscale((8.0 / 3.0) / hn2, un[rj]);
+                    dn2 = zadd(dn2, zscale(-3.0 / hn2, un[f1]));
+                    dn2 = zadd(dn2, zscale((1.0 / 3.0) / hn2, un[f2]));
+                    const z gin2 = zadd(zmul(ikb, un[rj]), dn2);
+                    const z hout = zadd(zmul(mikb, ush[e]), dn);
+                    // transmission row: h_out - zeta g_in - nu g_in' = 0
+                    const z row = zsub(zsub(hout, zmul(g.zeta, gin)), zmul(g.nu, gin2));
+                    z* rp = ri + ((long long)rhs * g.nleaves + leaf) * nb + e;
+                    r = first ? zneg(row) : zsub(*rp, row);
+                    *rp = r;
+                }
+                mx = fmax(mx, fabs(r.x) + fabs(r.y));
             }
-            mx = fmax(mx, fabs(r.x) + fabs(r.y));
         }
     }
-    // max over the CTA, then over leaves
+    // max over the CTA, then over CTAs
     for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-    if ((threadIdx.x & 31) == 0 && rnorm) atomic_max_nonneg(rnorm + rhs, mx);
+    if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5] = mx;
+    __syncthreads();
+    if (threadIdx.x == 0 && rnorm) {
+        for (int w = 1; w < RES_THREADS / 32; ++w) mx = fmax(mx, wmax[w]);
+        atomic_max_nonneg(rnorm + rhs, mx);
+    }
 }
 
 // hbuf (children of level l's nodes, [child][rhs column][nbc]) -= ri at the interface points:
@@ -190,7 +207,8 @@ cudaError_t fd_residual(const RefineGeom& g, int nrhs, const z* d, z* f, z* groo
         cudaError_t e = ensure_smem_attr(fd_residual_kernel, sh, attr);
         if (e != cudaSuccess) return e;
     }
-    fd_residual_kernel<<<dim3(g.nleaves, nrhs), 128, sh, s>>>(g, d, f, groot, ri, kv, hh, bclass, first ? 1 : 0, rnorm);
+    fd_residual_kernel<<<dim3((g.nleaves + RES_LEAVES - 1) / RES_LEAVES, nrhs), RES_THREADS, sh, s>>>(
+        g, d, f, groot, ri, kv, hh, bclass, first ? 1 : 0, rnorm);
     note_launch();
     return cudaGetLastError();
 }

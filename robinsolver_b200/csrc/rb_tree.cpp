@@ -559,16 +559,29 @@ static int ensure_factor_storage(rb_tree* t) {
 // kernel: below the top two levels, and only where the interface fills the 128-row MMA tile.
 // Level L stands for the solve's leaf GEMM h = Y(:, nb:) f, which streams every leaf's Y once
 // (HBM-bound): on the tensor cores in the mixed solve as well.
+// With the int8 engine (the default) the tensor-core products are as accurate as the refinement
+// needs from any of them, so a level goes to the tensor cores only where they are faster than the
+// FP64 tiles: interfaces of at least 256 points (1024^2, L=12: levels 2-4; at m = 128 the digit
+// passes and the 48-column tiles cost more than the FP64 products save).  Split TF32 keeps its
+// 128-point rule.
+// The top two merge levels (the root interface system) stay FP64, unless the tree was created
+// with RB_FLAG_MIXED_INT8_TOP (int8 engine only): then their GEMMs run on the int8 engine too,
+// and only their inversions stay FP64.
+static bool mixed_top_levels(const rb_tree* t) {
+    return t->mixed_int8_top && tc5_engine(GemmBatch{}) == TC5_ENGINE_INT8;
+}
 static bool mixed_level(const rb_tree* t, int l) {
-    if (t->prec != RB_PREC_MIXED || l < 2) return false;
-    return l == t->P.L || t->P.lv[l].m >= 128;
+    if (t->prec != RB_PREC_MIXED || (l < 2 && !mixed_top_levels(t))) return false;
+    const int mmin = tc5_engine(GemmBatch{}) == TC5_ENGINE_INT8 ? 256 : 128;
+    return l == t->P.L || t->P.lv[l].m >= mmin;
 }
 // Which factor stages of a mixed level run on the tcgen05 kernel: RB_MIXED_STAGES (read at every
 // launch) is a bit mask over K = nu^2 I - A2 A1 (1), B1 (2), Y1 (4), Y2 (8) and the parent map
-// (16); the default is all of them.  The solve's batches follow their level.
+// (16).  The default leaves K (m^3, the smallest product of a level) on the FP64 tiles, which are
+// as fast there; the int8 engine runs the rest.  The solve's batches follow their level.
 static int mixed_stage_mask() {
     const char* v = std::getenv("RB_MIXED_STAGES");
-    return v ? std::atoi(v) : 31;
+    return v ? std::atoi(v) : 30;
 }
 static bool mixed_batch(const rb_tree* t, const GemmBatch& b, int l) {
     if (!mixed_level(t, l)) return false;
@@ -1336,6 +1349,7 @@ int rb_tree_create(const rb_geom* geom, rb_tree** out) {
     t->skip_root = (geom->flags & RB_FLAG_SKIP_ROOT_RTR) != 0;
     t->graphs = (geom->flags & RB_FLAG_NO_GRAPHS) == 0;
     t->async_factor = (geom->flags & RB_FLAG_ASYNC_FACTOR) != 0;
+    t->mixed_int8_top = (geom->flags & RB_FLAG_MIXED_INT8_TOP) != 0;
     // refuse up front a problem the budget cannot hold (persistent factor storage only)
     if (t->budget > 0) {
         const Plan& Q = t->P;

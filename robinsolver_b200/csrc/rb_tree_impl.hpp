@@ -136,6 +136,7 @@ struct rb_tree {
     // the top two levels, the interface inverses, the leaves and the FD residual stay FP64, and
     // the solve refines every right-hand side against the FP64 residual to refine_tol
     int prec = RB_PREC_FP64;          // precision of the current factorization
+    bool mixed_int8_top = false;      // RB_FLAG_MIXED_INT8_TOP
     int gx_factor_prec = -1;          // precision the captured factor graph was recorded with
     double refine_tol = 1e-10;
     int refine_maxit = 8;
