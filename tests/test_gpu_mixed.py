@@ -96,3 +96,25 @@ def test_mixed_full_size_matches_fp64():
         assert rel_err(Um[r], Uf[r]) < 1e-10, (r, rel_err(Um[r], Uf[r]))
     Tf.close()
     Tm.close()
+
+
+def test_mixed_int8_top_levels():
+    """RB_FLAG_MIXED_INT8_TOP (512^2/L=10): the top two levels' GEMMs on the int8 engine as well
+    (their 512- and 256-point interfaces' inversions stay FP64); refined within 1e-10 of FP64 with
+    one correction, and the root level's map differs from the FP64 one within the engine's bar."""
+    wl = W.make_workload(2, N=512, L=10, nrhs=4)
+    Tf, op, opts = gpu_tree(wl)
+    Tf.factor(wl.L, op, opts)
+    Tm, op2, opts2 = gpu_tree(wl, mixed_int8_top=True)
+    Tm.factor(wl.L, op2, opts2, precision="mixed")
+    Uf = _solve(Tf, wl.rhs)
+    Um = _solve(Tm, wl.rhs)
+    for r in range(len(wl.rhs)):
+        assert rel_err(Um[r], Uf[r]) < 1e-10, (r, rel_err(Um[r], Uf[r]))
+    it, rho, est, res = Tm.refine_info()
+    assert it == 1 and rho < 1e-5, (it, rho)
+    for lvl in (1, 2):
+        d = rel_err(Tm.get_rtr(lvl, 0), Tf.get_rtr(lvl, 0))
+        assert 1e-15 < d < 1e-8, (lvl, d)
+    Tf.close()
+    Tm.close()
