@@ -4,6 +4,8 @@ against FP64.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--precision mixed|fp64]
     python bench.py --serve [--requests R]
+    python bench.py --forest | --three-d
+    python bench.py --gemm fp64|tf32x3|int8 [--gemm-shape m,n,k,count]   (one GEMM engine alone)
 
 One step = the reference's hot path on one batch: robin_tree%factor of the 1024^2, L=12 tree
 (16x16 leaves, kb=200, seeded 100-bump potential with 0.002i*kb damping) followed by one batched
@@ -93,6 +95,11 @@ def parse():
     ap.add_argument("--requests", type=int, default=4000, help="solve requests per offered load (--serve)")
     ap.add_argument("--forest", action="store_true",
                     help="batching bench: 64 trees of uneven sizes factored as one forest vs one at a time")
+    ap.add_argument("--gemm", default=None, choices=["fp64", "tf32x3", "int8"],
+                    help="one batched complex GEMM on one engine (the FP64 tiles, or the tcgen05 kernel in split "
+                         "TF32 or int8 digit slices): device time per launch and algorithmic TFLOP/s; "
+                         "--gemm-shape m,n,k,count")
+    ap.add_argument("--gemm-shape", default="2048,2048,512,4")
     ap.add_argument("--three-d", action="store_true",
                     help="3D bench: factor and 8-RHS solve of the unit cube at 16^3 (L=6) and 32^3 (L=9), "
                          "4^3 leaves, with the manufactured solution's error")
@@ -1036,10 +1043,44 @@ def three_d_arm(args):
     return 0
 
 
+def gemm_arm(args):
+    """One batched complex GEMM D_i = A_i B_i (column-major, random normal entries) on one engine,
+    timed with CUDA events over --steps launches after --warmup (rb_test_zgemm_timed, operand
+    split passes included), and its error against torch's complex128 product relative to
+    max|A| max|B| k."""
+    import ctypes
+
+    import torch
+
+    from robinsolver_b200 import _lib
+    m, n, k, cnt = (int(x) for x in args.gemm_shape.split(","))
+    engine = {"fp64": 0, "tf32x3": 1, "int8": 2}[args.gemm]
+    dev = torch.device("cuda", 0)
+    g = torch.Generator(device=dev).manual_seed(7)
+    A = torch.randn(cnt, k, m, dtype=torch.complex128, device=dev, generator=g)
+    B = torch.randn(cnt, n, k, dtype=torch.complex128, device=dev, generator=g)
+    C = torch.zeros(cnt, n, m, dtype=torch.complex128, device=dev)
+    ms = ctypes.c_double()
+    for reps in (max(args.warmup, 1), args.steps):
+        rc = _lib.lib.rb_test_zgemm_timed(engine, m, n, k, A.data_ptr(), m, m * k, B.data_ptr(), k, k * n,
+                                          C.data_ptr(), m, m * n, 1.0, 0.0, 0.0, 0.0, cnt, reps, ctypes.byref(ms))
+        if rc != 0:
+            raise RuntimeError(f"rb_test_zgemm_timed: {rc} {_lib.last_error(None)}")
+    ref = torch.matmul(A.transpose(1, 2), B.transpose(1, 2))
+    err = float((C.transpose(1, 2) - ref).abs().max() / (A.abs().max() * B.abs().max() * k))
+    flops = 8.0 * m * n * k * cnt
+    print(json.dumps({"gemm": args.gemm, "shape": {"m": m, "n": n, "k": k, "count": cnt}, "ms_per_launch": ms.value,
+                      "tflops_algorithmic": flops / (ms.value * 1e-3) / 1e12, "err_rel_scale": err,
+                      "launches_timed": args.steps}), flush=True)
+    return 0
+
+
 def main():
     args = parse()
     if args.three_d:
         return three_d_arm(args)
+    if args.gemm:
+        return gemm_arm(args)
     if args.serve:
         return serve_arm(args)
     if args.forest:
