@@ -624,7 +624,11 @@ __device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t da, uint64_t d
 }  // namespace
 
 // Row exponents of A: e = 1 + max frexp exponent over the row's k (re and im), so the scaled row
-// lies in (-1/2, 1/2).  Block = 32 rows x 8 k phases; grid = count * ceil(MT * 128 / 32).
+// lies in (-1/2, 1/2).  Block = 32 rows x 8 k phases over one range of OZ_SCALE_KC k (blockIdx.y);
+// grid = (count * ceil(MT * 128 / 32), ceil(max_k / OZ_SCALE_KC)).  The ranges meet in an atomic
+// max on ea, which the launcher fills with INT_MIN-like bytes first (a whole row per block left
+// most SMs idle, waiting on one long chain of loads each).
+constexpr int OZ_SCALE_KC = 64;
 __global__ void __launch_bounds__(256) oz_scale_a_kernel(const GemmDesc* __restrict__ descs, int MT, int* ea) {
     __shared__ int red[8][32];
     const int groups = MT * TC5_BM / 32;
@@ -632,12 +636,14 @@ __global__ void __launch_bounds__(256) oz_scale_a_kernel(const GemmDesc* __restr
     const int lane = threadIdx.x & 31, ph = threadIdx.x >> 5;
     const GemmDesc& g = descs[prob];
     const int i = grp * 32 + lane;
+    const int k0 = blockIdx.y * OZ_SCALE_KC, k1 = min(g.k, k0 + OZ_SCALE_KC);
+    if (k0 >= g.k && blockIdx.y > 0) return;          // uniform over the block
     int ex = -1022;
     if (i < g.m) {
         const ZView v = g.A;
         const long long ro = vrow(v, i);
 #pragma unroll 4
-        for (int k = ph; k < g.k; k += 8) {
+        for (int k = k0 + ph; k < k1; k += 8) {
             const z x = v.p[ro + (long long)vcol(v, k) * v.ld];
             ex = max(ex, max(oz_exponent(x.x), oz_exponent(x.y)));
         }
@@ -647,7 +653,7 @@ __global__ void __launch_bounds__(256) oz_scale_a_kernel(const GemmDesc* __restr
     if (ph == 0) {
 #pragma unroll
         for (int q = 1; q < 8; ++q) ex = max(ex, red[q][lane]);
-        ea[(long long)prob * MT * TC5_BM + i] = ex + 1;
+        atomicMax(ea + (long long)prob * MT * TC5_BM + i, ex + 1);
     }
 }
 
@@ -676,7 +682,7 @@ __global__ void __launch_bounds__(256) oz_scale_b_kernel(const GemmDesc* __restr
 // halves), else a B block (problem, nt, kb: 48 columns x 32 k).  Digit plane p of a block holds
 // chunk c (16 k) of row r at ((p * 2 + c) * ROWS + r) * 16 bytes; a B plane's rows are -Bi of the
 // 48 columns, then Br, then Bi.
-__global__ void __launch_bounds__(256) oz_split_kernel(const GemmDesc* __restrict__ descs, int MT, int NT, int KBN,
+__global__ void __launch_bounds__(256, 4) oz_split_kernel(const GemmDesc* __restrict__ descs, int MT, int NT, int KBN,
                                                        long long nA, unsigned char* __restrict__ planes,
                                                        long long a_bytes, const int* __restrict__ ea,
                                                        const int* __restrict__ fb) {
@@ -991,7 +997,11 @@ static cudaError_t launch_oz(const GemmBatch& b, int* status, cudaStream_t s) {
         const long long nA = (long long)b.count * og.MT * og.KBN;
         const long long nB = (long long)b.count * og.NT * og.KBN;
         if (ga > 0x7FFFFFFFLL || gb > 0x7FFFFFFFLL || nA + nB > 0x7FFFFFFFLL) return cudaErrorInvalidValue;
-        oz_scale_a_kernel<<<(unsigned)ga, 256, 0, s>>>(b.d_desc, og.MT, ea);
+        e = cudaMemsetAsync(ea, 0x80, (size_t)(og.fb_off - og.ea_off), s);     // every int far below -1022
+        if (e != cudaSuccess) return e;
+        const unsigned gk = (unsigned)((b.max_k + OZ_SCALE_KC - 1) / OZ_SCALE_KC);
+        if (gk > 65535u) return cudaErrorInvalidValue;
+        oz_scale_a_kernel<<<dim3((unsigned)ga, gk), 256, 0, s>>>(b.d_desc, og.MT, ea);
         note_launch();
         oz_scale_b_kernel<<<(unsigned)gb, 256, 0, s>>>(b.d_desc, og.NT, fb);
         note_launch();
