@@ -177,7 +177,9 @@ int rb_tree_factor(rb_tree* tree, const double* k_centres, int precision);
 int rb_tree_factor_device(rb_tree* tree, const double* d_k_centres, int precision, int sync);
 
 /* robin_tree%solve(rhs) (robin_tree_module.f90:198-233) for `nrhs` right-hand sides at once:
- *  f_centres: nrhs * nleaves*a*b complex, RHS-major, each at RB_POINTS_SOURCE;
+ *  f_centres: nrhs * nleaves*a*b complex, RHS-major, each at RB_POINTS_SOURCE; NULL when every
+ *             interior source is zero (e.g. plane waves fed through g): the library zeroes its
+ *             source array on the device instead of copying one, and solves as for zeros;
  *  g_faces:   nrhs * root_nb complex, RHS-major, each at RB_POINTS_BOUNDARY.
  * Every call applies its own boundary data (the reference applies boundary data only on the
  * first solve of a process, robin_tree_module.f90:1014-1029).  Blocks until done; sets
@@ -192,6 +194,16 @@ int rb_tree_solve_device(rb_tree* tree, int nrhs, const double* d_f_centres,
  *  u:     nleaves * leaf_n complex (host), leaves in DFS order, each in lin2fgrid order;
  *  boxes: nleaves * 6 doubles (host, may be NULL), each leaf's box(1:2,1:3) column-major. */
 int rb_get_solution(const rb_tree* tree, int irhs, double* u, double* boxes);
+
+/* rb_get_solution without waiting for the copy (beyond the reference, whose get_solution returns
+ * filled arrays): enqueues the device -> host copy of right-hand side irhs's solution into u on a
+ * stream of its own, behind the solve that wrote it, and returns; boxes (may be NULL) are filled
+ * at once.  u must stay valid and untouched until rb_tree_sync(tree) returns; with pinned host
+ * memory the copy runs beside later work, e.g. the next factorization.  A later solve waits on the
+ * device for these copies before it overwrites the solution. */
+int rb_get_solution_async(const rb_tree* tree, int irhs, double* u, double* boxes);
+/* Waits until every copy rb_get_solution_async enqueued for this handle has landed. */
+int rb_tree_sync(const rb_tree* tree);
 
 /* All right-hand sides' solutions into device memory: nrhs * nleaves * leaf_n complex,
  * RHS-major.  Asynchronous on the handle's stream when `sync` is 0. */

@@ -46,7 +46,8 @@ RB_FIELD_PLANE_WAVE = 2
 EXPORTS = [
     "rb_tree_create", "rb_tree_destroy", "rb_last_error", "rb_tree_info", "rb_tree_sample_points",
     "rb_tree_factor", "rb_tree_factor_device", "rb_tree_solve", "rb_tree_solve_device",
-    "rb_get_solution", "rb_get_solution_device", "rb_tree_times", "rb_tree_stream",
+    "rb_get_solution", "rb_get_solution_device", "rb_get_solution_async", "rb_tree_sync", "rb_tree_times",
+    "rb_tree_stream",
     "rb_tree_set_timing", "rb_tree_stage_times", "rb_tree_clear_stage_times", "rb_tree_level_shape", "rb_tree_get_rtr", "rb_tree_launch_counts",
     "rb_leaf_rtr_noalloc",
     "rb_tree_sample_device", "rb_check_solution", "rb_check_solution_device", "rb_tree_save", "rb_tree_load",
@@ -131,6 +132,8 @@ def _load():
         "rb_tree_solve_device": (C.c_int, [P, C.c_int, P, P, C.c_int]),
         "rb_get_solution": (C.c_int, [P, C.c_int, D, D]),
         "rb_get_solution_device": (C.c_int, [P, P, C.c_int]),
+        "rb_get_solution_async": (C.c_int, [P, C.c_int, D, D]),
+        "rb_tree_sync": (C.c_int, [P]),
         "rb_tree_times": (C.c_int, [P, D, D]),
         "rb_tree_stream": (P, [P]),
         "rb_tree_set_timing": (C.c_int, [P, C.c_int]),

@@ -289,13 +289,18 @@ class robin_tree:
         F, G = self.sample_rhs(rhs_list)
         self.solve_samples(F, G)
 
-    def solve_samples(self, F: np.ndarray, G: np.ndarray):
-        F = np.ascontiguousarray(F, dtype=np.complex128)
+    def solve_samples(self, F, G: np.ndarray):
+        """Solve with sampled sources F (None: every interior source is zero, nothing is
+        uploaded for it) and boundary data G."""
         G = np.ascontiguousarray(G, dtype=np.complex128)
-        nr = F.shape[0]
-        if F.size != nr * self._info.n_interior or G.size != nr * self._info.root_nb:
+        nr = G.shape[0]
+        if F is not None:
+            F = np.ascontiguousarray(F, dtype=np.complex128)
+            if F.size != nr * self._info.n_interior:
+                raise RobinSolverError(_lib.RB_ERR_INVALID, "right-hand side sample count mismatch")
+        if G.size != nr * self._info.root_nb:
             raise RobinSolverError(_lib.RB_ERR_INVALID, "right-hand side sample count mismatch")
-        _check(lib.rb_tree_solve(self._h, nr, _lib.dptr(F), _lib.dptr(G)), self._h)
+        _check(lib.rb_tree_solve(self._h, nr, None if F is None else _lib.dptr(F), _lib.dptr(G)), self._h)
         self._info = self.info()
         self._update_times()
 

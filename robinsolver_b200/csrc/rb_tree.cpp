@@ -829,6 +829,7 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
     const int L = P.L, nl = P.nleaves(), ab = P.leaf_interior(), nb = P.leaf_nb(), n = P.leaf_n();
     int rc;
     if (nrhs > t->cap_rhs) {
+        if (t->d2h_pending) RB_CK(cudaStreamSynchronize(t->stream5));   // no read-back may still use sol
         drop_graph(t->gx_solve);
         t->gx_solve_rhs = 0;
         free_list(t, t->solve_bufs);
@@ -1037,6 +1038,17 @@ static int ensure_solve_planes(rb_tree* t) {
     return RB_OK;
 }
 
+// the solution buffer is about to be written on stream s: wait (on the device) for the read-backs
+// rb_get_solution_async enqueued from it.  Inside a stream capture the wait is not recorded: a
+// graphed solve waits before its graph is launched (solve_common).
+static int wait_readback(rb_tree* t, cudaStream_t s) {
+    if (!t->d2h_pending) return RB_OK;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    RB_CK(cudaStreamIsCapturing(s, &cs));
+    if (cs == cudaStreamCaptureStatusNone) RB_CK(cudaStreamWaitEvent(s, t->ev_d2h, 0));
+    return RB_OK;
+}
+
 static int run_solve(rb_tree* t, int k, cudaStream_t s, const std::vector<cudaEvent_t>* wait = nullptr,
                      z* out = nullptr, bool inject = false) {
     const Plan& P = t->P;
@@ -1096,6 +1108,7 @@ static int run_solve(rb_tree* t, int k, cudaStream_t s, const std::vector<cudaEv
     }
     if ((rc = timer_end(t))) return rc;
     if ((rc = timer_begin(t, "leaf_recover"))) return rc;
+    if ((!out || out == t->sol) && (rc = wait_readback(t, s))) return rc;
     if (P.d == 2) {
         RB_TIMED("leaf_solve", 0.0, leaf_block_solve(lg, nl, k, t->d_h, t->d_f, t->gbuf[L], t->leaf_sinv,
                                                      out ? out : t->sol, s));
@@ -1394,6 +1407,11 @@ int rb_tree_destroy(rb_tree* t) {
     if (t->stream3) cudaStreamSynchronize(t->stream3);
     if (t->ev_copy) cudaEventDestroy(t->ev_copy);
     if (t->h_status) cudaFreeHost(t->h_status);
+    if (t->stream5) {
+        cudaStreamSynchronize(t->stream5);
+        cudaStreamDestroy(t->stream5);
+    }
+    if (t->ev_d2h) cudaEventDestroy(t->ev_d2h);
     if (t->stream3) cudaStreamDestroy(t->stream3);
     if (t->stream2) cudaStreamDestroy(t->stream2);
     if (t->stream4) cudaStreamDestroy(t->stream4);
@@ -1661,7 +1679,7 @@ static int solve_common(rb_tree* t, int nrhs, const double* f, const double* g, 
     if (!t) return RB_ERR_INVALID;
     if (!t->factored) return fail(t, RB_ERR_NOT_FACTORED, "Error: Robin Tree must be factored first.");
     if (nrhs <= 0) return fail(t, RB_ERR_INVALID, "rb_tree_solve: nrhs must be positive");
-    if (!f || !g) return fail(t, RB_ERR_INVALID, "rb_tree_solve: null right-hand side");
+    if (!g) return fail(t, RB_ERR_INVALID, "rb_tree_solve: null boundary data");
     int rc = ensure_solve_storage(t, nrhs);
     if (rc) return rc;
     const Plan& P = t->P;
@@ -1684,7 +1702,8 @@ static int solve_common(rb_tree* t, int nrhs, const double* f, const double* g, 
         RB_CK(cudaEventRecord(t->ev_copy, t->stream));          // device inputs are ordered there
         RB_CK(cudaStreamWaitEvent(ss, t->ev_copy, 0));
         RB_CK(cudaStreamWaitEvent(ss, t->ev[3], 0));            // the last read-back is done
-        RB_CK(cudaMemcpyAsync(t->d_f, f, nrhs * nint * sizeof(z), kind, ss));
+        RB_CK(f ? cudaMemcpyAsync(t->d_f, f, nrhs * nint * sizeof(z), kind, ss)
+                  : cudaMemsetAsync(t->d_f, 0, nrhs * nint * sizeof(z), ss));
         RB_CK(cudaMemcpyAsync(t->gbuf[0], g, nrhs * nroot * sizeof(z), kind, ss));
         RB_CK(cudaEventRecord(t->ev[2], ss));
         if (overlap && (rc = launch_factor(t, &t->ev_lvl))) return rc;
@@ -1726,7 +1745,8 @@ static int solve_common(rb_tree* t, int nrhs, const double* f, const double* g, 
         // competing with the solve's last levels.
         RB_CK(cudaEventRecord(t->ev_copy, t->stream));       // device inputs are ordered there
         RB_CK(cudaStreamWaitEvent(t->stream3, t->ev_copy, 0));
-        RB_CK(cudaMemcpyAsync(t->d_f, f, nrhs * nint * sizeof(z), kind, t->stream3));
+        RB_CK(f ? cudaMemcpyAsync(t->d_f, f, nrhs * nint * sizeof(z), kind, t->stream3)
+                  : cudaMemsetAsync(t->d_f, 0, nrhs * nint * sizeof(z), t->stream3));
         RB_CK(cudaMemcpyAsync(t->gbuf[0], g, nrhs * nroot * sizeof(z), kind, t->stream3));
         const std::function<int()> enqueue_solve = [&]() -> int {
             const long long l0 = launch_count();
@@ -1753,14 +1773,17 @@ static int solve_common(rb_tree* t, int nrhs, const double* f, const double* g, 
             // host right-hand sides go up on the copy stream, beside a factor that may still run on
             // the main stream; the copy waits until the last solve has read its buffers
             RB_CK(cudaStreamWaitEvent(t->stream3, t->ev[3], 0));
-            RB_CK(cudaMemcpyAsync(t->d_f, f, nrhs * nint * sizeof(z), kind, t->stream3));
+            RB_CK(f ? cudaMemcpyAsync(t->d_f, f, nrhs * nint * sizeof(z), kind, t->stream3)
+                  : cudaMemsetAsync(t->d_f, 0, nrhs * nint * sizeof(z), t->stream3));
             RB_CK(cudaMemcpyAsync(t->gbuf[0], g, nrhs * nroot * sizeof(z), kind, t->stream3));
             RB_CK(cudaEventRecord(t->ev_copy, t->stream3));
             RB_CK(cudaStreamWaitEvent(t->stream, t->ev_copy, 0));
         } else {
-            RB_CK(cudaMemcpyAsync(t->d_f, f, nrhs * nint * sizeof(z), kind, t->stream));
+            RB_CK(f ? cudaMemcpyAsync(t->d_f, f, nrhs * nint * sizeof(z), kind, t->stream)
+                  : cudaMemsetAsync(t->d_f, 0, nrhs * nint * sizeof(z), t->stream));
             RB_CK(cudaMemcpyAsync(t->gbuf[0], g, nrhs * nroot * sizeof(z), kind, t->stream));
         }
+        if ((rc = wait_readback(t, t->stream))) return rc;
         RB_CK(cudaEventRecord(t->ev[2], t->stream));
         const long long l0 = launch_count();
         if (t->gx_solve_rhs != nrhs) {     // the solve sequence depends on the RHS count
@@ -1818,6 +1841,42 @@ int rb_get_solution(const rb_tree* tc, int irhs, double* u, double* boxes) {
                 boxes[6 * i + 2 * j + 1] = lf.hi[3 * i + j];
             }
     }
+    return RB_OK;
+}
+
+int rb_get_solution_async(const rb_tree* tc, int irhs, double* u, double* boxes) {
+    rb_tree* t = const_cast<rb_tree*>(tc);
+    if (!t || !u) return RB_ERR_INVALID;
+    if (int rc = (t->factor_deferred || t->nrhs == 0) ? settle_factor(t) : settle_solution(t)) return rc;
+    if (!t->factored) return fail(t, RB_ERR_NOT_FACTORED, "Error in GET_SOLUTION: Robin Tree not factored.");
+    if (irhs < 0 || irhs >= t->nrhs) return fail(t, RB_ERR_NO_SOLUTION, "get_solution: no solution for this right-hand side");
+    if (!t->stream5) {
+        int lo = 0, hi = 0;
+        RB_CK(cudaDeviceGetStreamPriorityRange(&lo, &hi));
+        RB_CK(cudaStreamCreateWithPriority(&t->stream5, cudaStreamNonBlocking, lo));
+    }
+    if (!t->ev_d2h) RB_CK(cudaEventCreateWithFlags(&t->ev_d2h, cudaEventDisableTiming));
+    const Plan& P = t->P;
+    const size_t per = (size_t)P.nleaves() * P.leaf_n();
+    RB_CK(cudaStreamWaitEvent(t->stream5, t->ev[3], 0));        // the solve that wrote the solution
+    RB_CK(cudaMemcpyAsync(u, t->sol + (size_t)irhs * per, per * sizeof(z), cudaMemcpyDeviceToHost, t->stream5));
+    RB_CK(cudaEventRecord(t->ev_d2h, t->stream5));
+    t->d2h_pending = true;
+    if (boxes) {
+        const PlanLevel& lf = P.lv[P.L];
+        for (int i = 0; i < lf.nnodes; ++i)
+            for (int j = 0; j < 3; ++j) {
+                boxes[6 * i + 2 * j] = lf.lo[3 * i + j];
+                boxes[6 * i + 2 * j + 1] = lf.hi[3 * i + j];
+            }
+    }
+    return RB_OK;
+}
+
+int rb_tree_sync(const rb_tree* tc) {
+    rb_tree* t = const_cast<rb_tree*>(tc);
+    if (!t) return RB_ERR_INVALID;
+    if (t->stream5) RB_CK(cudaStreamSynchronize(t->stream5));
     return RB_OK;
 }
 

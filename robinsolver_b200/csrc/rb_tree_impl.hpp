@@ -42,6 +42,11 @@ struct rb_tree {
     cudaStream_t stream = nullptr;
     cudaStream_t stream2 = nullptr;      // runs one merge GEMM per level beside the level's inversion
     cudaStream_t stream3 = nullptr;      // host -> device copies of the inputs, beside running work
+    // rb_get_solution_async: device -> host copies of solutions on their own stream, behind the solve
+    // that wrote them; the next solve waits for ev_d2h before it writes the solution buffer
+    cudaStream_t stream5 = nullptr;
+    cudaEvent_t ev_d2h = nullptr;
+    bool d2h_pending = false;
     cudaEvent_t ev_copy = nullptr;
     // RB_FLAG_ASYNC_FACTOR: rb_tree_factor returns once the factor is enqueued; its completion,
     // time and status are taken by the next call that needs them (settle_factor)

@@ -81,3 +81,49 @@ def test_save_and_load_give_the_same_solver(tmp_path):
     assert np.array_equal(T.get_rtr(1, 0), Tl.get_rtr(1, 0))
     T.close()
     Tl.close()
+
+
+def test_async_readback_equals_sync_and_orders_with_the_next_solve():
+    """rb_get_solution_async + rb_tree_sync give the same bytes as rb_get_solution, and a solve
+    issued right after the asynchronous read-back (other right-hand sides) does not overwrite the
+    solution before the copy has landed."""
+    import ctypes
+
+    import torch
+
+    from robinsolver_b200 import _lib
+    wl = W.make_workload(2, N=256, L=6, nrhs=4)
+    T, op, opts = gpu_tree(wl)
+    T.factor(wl.L, op, opts)
+    rhs = gpu_rhs(wl.rhs)
+    T.solve(rhs)
+    ref = [T.solution_array(r) for r in range(4)]
+    inf = T.info()
+    bufs = [torch.zeros((inf.nleaves, inf.leaf_n), dtype=torch.complex128).pin_memory() for _ in range(4)]
+    ptr = [ctypes.cast(b.data_ptr(), ctypes.POINTER(ctypes.c_double)) for b in bufs]
+    lib = _lib.lib
+    for r in range(4):
+        assert lib.rb_get_solution_async(T.handle, r, ptr[r], None) == 0, _lib.last_error(T.handle)
+    T.solve(rhs[::-1])              # writes the solution buffer: must wait for the copies above
+    assert lib.rb_tree_sync(T.handle) == 0
+    for r in range(4):
+        assert np.array_equal(bufs[r].numpy(), ref[r]), r
+    # and the new solve is the reversed set
+    assert np.array_equal(T.solution_array(0), ref[3])
+    T.close()
+
+
+def test_null_sources_solve_as_zeros():
+    """rb_tree_solve with f_centres = NULL (every interior source zero) gives the bytes of a solve
+    with an uploaded array of zeros, FP64 and mixed precision."""
+    wl = W.make_workload(2, N=256, L=6, nrhs=3)
+    for prec in ("fp64", "mixed"):
+        T, op, opts = gpu_tree(wl)
+        T.factor(wl.L, op, opts, precision=prec)
+        F, G = T.sample_rhs(gpu_rhs(wl.rhs))
+        T.solve_samples(np.zeros_like(F), G)
+        ref = [T.solution_array(r) for r in range(3)]
+        T.solve_samples(None, G)
+        for r in range(3):
+            assert np.array_equal(T.solution_array(r), ref[r]), (prec, r)
+        T.close()
