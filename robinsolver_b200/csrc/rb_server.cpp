@@ -213,8 +213,27 @@ static void run_solve_batch(rb_server* s, TreeSlot& slot, std::vector<ReqPtr>& b
         if (rc) break;
         tot += r->nrhs;
     }
+    // the batch is padded with zero right-hand sides up to a power of two (at most max_batch_rhs):
+    // a tree then solves at most a handful of distinct RHS counts, whose launch plans and graphs
+    // it keeps, instead of building one for nearly every batch.  Every right-hand side is solved
+    // independently, so the padding changes no result.
+    int padded = tot;
+    if (!rc && tot > 0) {
+        padded = 1;
+        while (padded < tot) padded *= 2;
+        padded = std::min(padded, std::max(tot, s->opts.max_batch_rhs));
+        if (padded > tot) {
+            cudaError_t e = cudaMemsetAsync(slot.f_stage + 2 * (size_t)tot * nint, 0, (size_t)(padded - tot) * nint * 16, st);
+            if (e == cudaSuccess)
+                e = cudaMemsetAsync(slot.g_stage + 2 * (size_t)tot * nb, 0, (size_t)(padded - tot) * nb * 16, st);
+            if (e != cudaSuccess) {
+                rc = RB_ERR_CUDA;
+                msg = cuda_msg("batch padding failed", e);
+            }
+        }
+    }
     if (!rc) {
-        rc = rb_tree_solve_device(slot.t, tot, slot.f_stage, slot.g_stage, 0);
+        rc = rb_tree_solve_device(slot.t, padded, slot.f_stage, slot.g_stage, 0);
         if (rc) msg = rb_last_error(slot.t);
     }
     if (!rc) {

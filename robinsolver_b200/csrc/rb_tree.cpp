@@ -824,6 +824,27 @@ static int run_factor(rb_tree* t, const z* dk, const std::vector<cudaEvent_t>* r
 }
 
 // ---------------------------------------------------------------------------------------------------
+// cached solve plans (SolveSet): at most kMaxSolveSets besides the current one
+constexpr size_t kMaxSolveSets = 8;
+static void free_solve_set(rb_tree* t, SolveSet& c) {
+    drop_graph(c.gx);
+    free_list(t, c.bufs);
+}
+static void drop_solve_sets(rb_tree* t) {
+    for (auto& c : t->solve_sets) free_solve_set(t, c);
+    t->solve_sets.clear();
+}
+// frees the least recently used plans until at most `keep` remain
+static void evict_solve_sets(rb_tree* t, size_t keep) {
+    while (t->solve_sets.size() > keep) {
+        size_t lru = 0;
+        for (size_t i = 1; i < t->solve_sets.size(); ++i)
+            if (t->solve_sets[i].used < t->solve_sets[lru].used) lru = i;
+        free_solve_set(t, t->solve_sets[lru]);
+        t->solve_sets.erase(t->solve_sets.begin() + (long)lru);
+    }
+}
+
 static int ensure_solve_storage(rb_tree* t, int nrhs) {
     const Plan& P = t->P;
     const int L = P.L, nl = P.nleaves(), ab = P.leaf_interior(), nb = P.leaf_nb(), n = P.leaf_n();
@@ -832,6 +853,8 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
         if (t->d2h_pending) RB_CK(cudaStreamSynchronize(t->stream5));   // no read-back may still use sol
         drop_graph(t->gx_solve);
         t->gx_solve_rhs = 0;
+        drop_solve_sets(t);                          // every cached plan points into the old buffers
+        free_list(t, t->solve_desc_bufs);
         free_list(t, t->solve_bufs);
         t->solve_planes = nullptr;
         t->solve_planes_bytes = 0;
@@ -853,9 +876,43 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
         t->cap_rhs = k;
     }
     if (t->built_rhs == nrhs) return RB_OK;
-    drop_graph(t->gx_solve);
+    // keep the current count's plan, and take the requested count's from the cache if it is there
+    if (t->built_rhs > 0) {
+        SolveSet cur;
+        cur.nrhs = t->built_rhs;
+        cur.sL0 = t->sL0; cur.sLg = t->sLg; cur.sLf = t->sLf; cur.sR1 = t->sR1;
+        cur.sF12 = t->sF12; cur.sF3 = t->sF3; cur.sF4 = t->sF4; cur.sF5 = t->sF5; cur.sBY = t->sBY;
+        cur.bufs = std::move(t->solve_desc_bufs);
+        t->solve_desc_bufs.clear();
+        cur.gx = t->gx_solve_rhs == t->built_rhs ? t->gx_solve : nullptr;
+        if (!cur.gx) drop_graph(t->gx_solve);
+        cur.gx_launches = t->gx_solve_launches;
+        cur.runs = cur.gx ? t->solve_runs : 0;
+        cur.used = ++t->solve_clock;
+        t->gx_solve = nullptr;
+        t->solve_sets.push_back(std::move(cur));
+    } else {
+        drop_graph(t->gx_solve);
+    }
+    t->built_rhs = 0;
     t->gx_solve_rhs = 0;
-    // descriptor batches for this RHS count (allocated in solve_bufs too)
+    for (size_t i = 0; i < t->solve_sets.size(); ++i) {
+        if (t->solve_sets[i].nrhs != nrhs) continue;
+        SolveSet& c = t->solve_sets[i];
+        t->sL0 = c.sL0; t->sLg = c.sLg; t->sLf = c.sLf; t->sR1 = c.sR1;
+        t->sF12 = c.sF12; t->sF3 = c.sF3; t->sF4 = c.sF4; t->sF5 = c.sF5; t->sBY = c.sBY;
+        t->solve_desc_bufs = std::move(c.bufs);
+        t->gx_solve = c.gx;
+        t->gx_solve_launches = c.gx_launches;
+        t->solve_runs = c.runs;
+        t->gx_solve_rhs = nrhs;
+        t->solve_sets.erase(t->solve_sets.begin() + (long)i);
+        t->built_rhs = nrhs;
+        return RB_OK;
+    }
+    evict_solve_sets(t, kMaxSolveSets - 1);
+    t->solve_runs = 0;
+    // descriptor batches for this RHS count (their arrays in solve_desc_bufs)
     const int k = nrhs;
     const z one = zmk(1.0, 0.0), mone = zmk(-1.0, 0.0), mnu = zneg(t->nu);
     const z rnu = zrcp(t->nu), mrnu = zneg(rnu);
@@ -864,7 +921,7 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
         v.push_back(gdesc(nb, k, ab, zview(t->leaf_Y + (long long)i * nb * n + (long long)nb * nb, nb),
                           zview(t->d_f + (long long)i * ab, (long long)nl * ab),
                           zout(t->hbuf[L] + (long long)i * nb * k, nb), one));
-    if ((rc = upload_gemm(t, t->solve_bufs, v, t->sL0))) return rc;
+    if ((rc = upload_gemm(t, t->solve_desc_bufs, v, t->sL0))) return rc;
     t->sLg = GemmBatch();
     t->sLf = GemmBatch();
     if (P.d == 3) {
@@ -882,8 +939,8 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
             gf.beta = one;
             vf.push_back(gf);
         }
-        if ((rc = upload_gemm(t, t->solve_bufs, vg, t->sLg))) return rc;
-        if ((rc = upload_gemm(t, t->solve_bufs, vf, t->sLf))) return rc;
+        if ((rc = upload_gemm(t, t->solve_desc_bufs, vg, t->sLg))) return rc;
+        if ((rc = upload_gemm(t, t->solve_desc_bufs, vf, t->sLf))) return rc;
     }
     t->sF12.assign(L, GemmBatch()); t->sF3.assign(L, GemmBatch()); t->sF4.assign(L, GemmBatch());
     t->sF5.assign(L, GemmBatch()); t->sBY.assign(L, GemmBatch());
@@ -972,12 +1029,12 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
                 by.push_back(gy1); by.push_back(gy2);
             }
         }
-        if ((rc = upload_gemm(t, t->solve_bufs, f12, t->sF12[l]))) return rc;
-        if ((rc = upload_gemm(t, t->solve_bufs, f3, t->sF3[l]))) return rc;
-        if ((rc = upload_gemm(t, t->solve_bufs, f4, t->sF4[l]))) return rc;
-        if ((rc = upload_gemm(t, t->solve_bufs, f5, t->sF5[l]))) return rc;
-        if ((rc = upload_gemm(t, t->solve_bufs, by, t->sBY[l]))) return rc;
-        if (l == 0 && (rc = upload_gemm(t, t->solve_bufs, rx, t->sR1))) return rc;
+        if ((rc = upload_gemm(t, t->solve_desc_bufs, f12, t->sF12[l]))) return rc;
+        if ((rc = upload_gemm(t, t->solve_desc_bufs, f3, t->sF3[l]))) return rc;
+        if ((rc = upload_gemm(t, t->solve_desc_bufs, f4, t->sF4[l]))) return rc;
+        if ((rc = upload_gemm(t, t->solve_desc_bufs, f5, t->sF5[l]))) return rc;
+        if ((rc = upload_gemm(t, t->solve_desc_bufs, by, t->sBY[l]))) return rc;
+        if (l == 0 && (rc = upload_gemm(t, t->solve_desc_bufs, rx, t->sR1))) return rc;
     }
     t->sL0.fixed_order = true;
     t->sR1.fixed_order = true;
@@ -998,12 +1055,13 @@ static int ensure_solve_storage(rb_tree* t, int nrhs) {
         }
         if (wmax > 0) {
             z* ws = nullptr;
-            if ((rc = alloc_n(t, t->solve_bufs, (size_t)wmax, &ws))) return rc;
+            if ((rc = alloc_n(t, t->solve_desc_bufs, (size_t)wmax, &ws))) return rc;
             for (GemmBatch* gb : all)
                 if (gb->ksplit > 1 || gb->t5_ksplit > 1) gb->work = ws;
         }
     }
     t->built_rhs = nrhs;
+    t->gx_solve_rhs = nrhs;
     return RB_OK;
 }
 
@@ -1389,6 +1447,8 @@ int rb_tree_destroy(rb_tree* t) {
     timers_collect(t);
     drop_graph(t->gx_factor);
     drop_graph(t->gx_solve);
+    drop_solve_sets(t);
+    free_list(t, t->solve_desc_bufs);
     free_list(t, t->solve_bufs);
     free_list(t, t->refine_bufs);
     free_list(t, t->mixed_bufs);

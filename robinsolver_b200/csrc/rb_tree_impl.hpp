@@ -24,6 +24,21 @@ struct GJBatch {
     int m = 0;
 };
 
+// The solve's launch plan for one RHS count: its descriptor batches, their device arrays (and
+// split-K workspace), and its captured graph.  A tree keeps a few of them, so that solves whose
+// RHS counts change from call to call (a serving loop's batches) reuse them instead of uploading
+// descriptors and capturing a graph again.
+struct SolveSet {
+    int nrhs = 0;
+    GemmBatch sL0, sLg, sLf, sR1;
+    std::vector<GemmBatch> sF12, sF3, sF4, sF5, sBY;
+    std::vector<DevBuf> bufs;
+    cudaGraphExec_t gx = nullptr;
+    long long gx_launches = 0;
+    int runs = 0;
+    unsigned long long used = 0;
+};
+
 struct StageTimer {
     const char* name;
     double flops;
@@ -123,6 +138,9 @@ struct rb_tree {
     std::vector<GemmBatch> sF12, sF3, sF4, sF5, sBY;
     GemmBatch sR1;                   // root: x_i = h_i + T_iN g_N (no K^-1 needed)
     std::vector<DevBuf> solve_bufs;
+    std::vector<DevBuf> solve_desc_bufs;     // the current RHS count's descriptor arrays and workspace
+    std::vector<SolveSet> solve_sets;        // other RHS counts' plans, least recently used evicted
+    unsigned long long solve_clock = 0;
     unsigned char* solve_planes = nullptr;   // tcgen05 operand planes of the solve (mixed, tc5 sweeps)
     size_t solve_planes_bytes = 0;
 

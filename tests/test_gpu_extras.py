@@ -127,3 +127,25 @@ def test_null_sources_solve_as_zeros():
         for r in range(3):
             assert np.array_equal(T.solution_array(r), ref[r]), (prec, r)
         T.close()
+
+
+def test_changing_rhs_counts_reuse_cached_solve_plans():
+    """Solves whose RHS counts change from call to call (a serving loop's batches) switch between
+    cached launch plans and graphs: every solution equals the first solve of that count, bit for
+    bit, across switches, and more counts than the cache holds still solve correctly."""
+    wl = W.make_workload(2, N=256, L=6, nrhs=12)
+    T, op, opts = gpu_tree(wl)
+    T.factor(wl.L, op, opts)
+    rhs = gpu_rhs(wl.rhs)
+    first = {}
+    for c in [3, 5, 3, 7, 5, 3, 7, 7, 1, 2, 4, 6, 8, 9, 10, 11, 12, 3, 5]:
+        T.solve(rhs[:c])
+        U = [T.solution_array(r) for r in range(c)]
+        if c not in first:
+            first[c] = U
+        for r in range(c):
+            assert np.array_equal(U[r], first[c][r]), (c, r)
+    # batches are independent of their size: the first RHS agrees across counts
+    for c in first:
+        assert np.array_equal(first[c][0], first[1][0]), c
+    T.close()
