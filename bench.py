@@ -42,7 +42,7 @@ headline.
           and merge) and a few single-RHS solves (the reference solves one right-hand side per
           call); RHS/s = nrhs / (factor + nrhs x mean solve).  The reference arm cuts that one
           pass into K consecutive measured steps.
-* --serve: the serving loop (rb_server_*): 8 resident trees of BASELINE's serving set, a
+* --serve: the serving loop (rb_server_*): 8 resident trees (grids 256^2..1024^2, kb 50..200), a
           Poisson stream of device-sampled point-source / plane-wave solve requests (1-64 RHS)
           with 20 refactors, at 0.5x and 0.9x of the measured saturated rate; p50/p99 latency
           from arrival to solution in host memory, mixed and FP64 servers.

@@ -8,7 +8,8 @@
 //     concurrently on the device;
 //   * continuous batching: the solve requests queued for a tree when its worker becomes free are
 //     merged, up to max_batch_rhs right-hand sides, into ONE batched up/down sweep; requests that
-//     arrive meanwhile form the next batch.  A factor request is a barrier in its tree's queue:
+//     arrive meanwhile form the next batch.  A batch is padded with zero right-hand sides to a
+//     power of two, so that each tree reuses a few cached launch plans (one per RHS count).  A factor request is a barrier in its tree's queue:
 //     solves submitted before it use the old factorization, solves after it the new one;
 //   * admission by device memory: a tree's first factorization reserves its estimated footprint
 //     (factor storage, solve buffers of a full batch, input staging) against the server's budget

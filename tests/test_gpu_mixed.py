@@ -5,7 +5,7 @@ factor with FP64 GEMMs and are refined against the FP64 residual of the global F
 GPU).
 
 Bars: every refined solution within 1e-10 relative (max norm) of the FP64 GPU solution of the
-same problem, as BASELINE's precision configuration asks; the merged maps of a tensor-core level
+same problem (the mixed-precision configuration's bar); the merged maps of a tensor-core level
 within 1e-8 of the FP64 ones (the digit slices keep ~35 bits) but not equal to them (the
 tensor-core path did run); the refinement contracts by at least 1e-5 per correction.
 """
