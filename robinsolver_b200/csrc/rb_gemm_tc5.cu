@@ -24,7 +24,7 @@
 //  2. zgemm_tc5_kernel, one CTA per 128 x BN output tile, 8 warps:
 //       warp 0   one lane streams the k-blocks of A and B into a ring of shared-memory stages with
 //                two 1-D bulk copies each (cp.async.bulk, completion counted in bytes on the
-//                stage's mbarrier; no multicast);
+//                stage's mbarrier; each CTA copies only for itself);
 //       warp 1   allocates 2*BN tensor-memory columns; one lane issues the stage's MMAs once its
 //                bytes have landed and releases the stage with tcgen05.commit;
 //       all 8   the epilogue: tcgen05.ld of the accumulators (warp w reads lanes 32 (w % 4) ..
